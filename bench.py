@@ -1,0 +1,361 @@
+"""Benchmark: Mrays/s of the 1080p PBR mesh scene (config 1) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Workload (one step = one frame): 1920x1080 viewport = 1921x1081 QCAA grid of primary rays,
+trace.depth 4, one displaced icosphere of 1,310,720 triangles in 8 instances (4 Cook-Torrance,
+2 glass, 2 mirror), two 1024^2 textures with 9-level mip chains, 2 emissive quads.  Seeded
+synthetic data (scenes.config1); the BLAS is built on the device (LBVH30) once, before timing.
+
+value      primary rays of all ranks / (max over ranks of the device time of K renders), inputs
+           resident, outputs to device buffers; L2 flushed (256 MiB write) before every step,
+           outside the timed events
+e2e        the same through st_render_scene with host buffers: each step uploads the primitive
+           records (H2D) and reads back the float grid and the u8 frame (D2H)
+roofline   the trace kernel: algorithmic bytes per frame (device event counters on the reference
+           traversal, bytes per event as defined in DESIGN.md) / its CUDA-event time, against the
+           measured HBM copy bandwidth
+cpu_baseline / --impl reference
+           the reference's own renderer (oracle/_ref, compiled from the reference sources) on the
+           same scene bytes, all host threads, over a bounded sample of rows
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from slimtracin_b200 import scenes, structs as S  # noqa: E402
+
+WIDTH, HEIGHT, DEPTH = 1920, 1080, 4
+METRIC = "Mrays/s at 1080p PBR mesh scene; p50/p99 latency, served vs per-frame launch"
+# bytes per event of the algorithmic traffic model (reference traversal, counted on the device)
+BYTES = {"aabb_tests": 32, "triangle_tests": 64, "primitive_tests": 72, "leaf_id_reads": 4,
+         "shaded_hits": 84 + 64, "texel_fetches": 12, "primary_rays": 24}
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def build_scene(seed_offset=0):
+    sd, cam = scenes.config1(seed_offset=seed_offset)
+    return sd, cam
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(s[1]) for s in self.samples if len(s) >= 9 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) >= 9 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            if len(s) >= 9:
+                for k, n in enumerate(names):
+                    if s[5 + k].lower() == "active":
+                        reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def cpu_reference_rows(sd, cam, rows, threads):
+    """Time the reference's renderer (oracle/_ref) on `rows` rows spread evenly over the frame."""
+    import oracle
+    ref = oracle.reference()
+    d = sd.copy()
+    sc, keep = d.to_ctypes()
+    fr = scenes.Frame(WIDTH, HEIGHT, cam, depth=DEPTH)
+    ref.ref_update_scene_ssb(C.byref(sc), C.byref(fr.viewport))
+    ref.ref_begin_drawing(C.byref(fr.viewport))
+    step = max(1, fr.grid_h // rows)
+    first = step // 2
+    t = time.perf_counter()
+    ref.ref_render_rows(C.byref(sc), C.byref(fr.viewport), threads, first, step, rows)
+    dt = time.perf_counter() - t
+    return rows * fr.grid_w, dt
+
+
+def calibrated_reference(sd, cam, threads, budget_s):
+    """Pick a row count whose reference render takes about budget_s seconds."""
+    rays, dt = cpu_reference_rows(sd, cam, max(threads, 8), threads)
+    per_row = dt / max(threads, 8)
+    rows = int(max(threads, min(1081, budget_s / max(per_row, 1e-6))))
+    return rows
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    import oracle
+    if not oracle.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libslimref.so is not built"}))
+        return 0
+    threads = os.cpu_count() or 1
+    sd, cam = build_scene()
+    blas_on_device(sd)
+    import tests.helpers as H
+    H.tlas_sah(sd, "ref")
+    rows = calibrated_reference(sd, cam, threads, 6.0)
+    for _ in range(args.warmup):
+        cpu_reference_rows(sd, cam, max(threads, 8), threads)
+    times, rays = [], 0
+    for _ in range(args.steps):
+        r, dt = cpu_reference_rows(sd, cam, rows, threads)
+        times.append(dt)
+        rays += r
+    total = sum(times)
+    value = rays / total / 1e6
+    grid = (WIDTH + 1) * (HEIGHT + 1)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * grid / (value * 1e6),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded config1 scene bytes, identical to the device arm)",
+            "config": {"workload": "config1 1080p PBR mesh scene, depth 4, 1.31M-triangle BLAS x 8 instances",
+                       "width": WIDTH, "height": HEIGHT, "depth": DEPTH, "rays_per_frame": grid},
+            "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": "reference",
+                             "sample": f"{rows} of {HEIGHT + 1} QCAA rows per step, rows spread evenly; "
+                                       f"reference rayTrace (raytracer.h:81) per pixel, {threads} threads"},
+            "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def blas_on_device(sd):
+    from slimtracin_b200 import api
+    r = api.Renderer(device=int(os.environ.get("LOCAL_RANK", 0)))
+    try:
+        for md in sd.meshes:
+            r.build_blas(md, api.ST_BVH_LBVH30)
+    finally:
+        r.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    from slimtracin_b200 import api, build
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    build.build()
+
+    # ---- scene (seeded; every rank renders its own replica) -----------------------------------
+    sd, cam = build_scene()
+    r = api.Renderer(device=local)
+    for md in sd.meshes:
+        r.build_blas(md, api.ST_BVH_LBVH30)
+    r.upload(0, sd, tlas=None)
+    r.build_tlas(0, sd, api.ST_BVH_LBVH30)
+    frame = scenes.Frame(WIDTH, HEIGHT, cam, depth=DEPTH)
+    grid = frame.rays
+
+    stream = torch.cuda.ExternalStream(r.stream)
+    out_float = torch.empty(grid * 24, dtype=torch.uint8, device="cuda")
+    out_u8 = torch.empty(WIDTH * HEIGHT * 4, dtype=torch.uint8, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    # ---- work counters (instrumented kernel, untimed) -----------------------------------------
+    ctr_frame = scenes.Frame(WIDTH, HEIGHT, cam, depth=DEPTH)
+    opt = r.render(0, sd, ctr_frame, count_work=True, skip_float_copy=True)
+    counters = api.counters_dict(opt)
+    bytes_alg = sum(BYTES[k] * counters[k] for k in BYTES)
+
+    def step():
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        return r.render_device(0, sd, frame, out_float.data_ptr(), out_u8.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    trace_ms = []
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                evs[k][0].record(stream)
+            o = r.render_device(0, sd, frame, out_float.data_ptr(), out_u8.data_ptr())
+            with torch.cuda.stream(stream):
+                evs[k][1].record(stream)
+            trace_ms.append(o.trace_ms)
+        torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    ms_per_step = total_ms / args.steps
+    value = world * grid / (ms_per_step / 1e3) / 1e6
+
+    # ---- end to end through st_render_scene with pinned host buffers ----------------------------
+    pinned_float = torch.empty(grid * 24, dtype=torch.uint8, pin_memory=True)
+    pinned_u8 = torch.empty(WIDTH * HEIGHT * 4, dtype=torch.uint8, pin_memory=True)
+    e2e_frame = scenes.Frame(WIDTH, HEIGHT, cam, depth=DEPTH)
+    e2e_frame.grid.float_pixels = pinned_float.data_ptr()
+    e2e_frame.grid.pixels = pinned_u8.data_ptr()
+    prims_pinned = torch.from_numpy(sd.primitives.view(np.uint8).copy()).pin_memory()
+    prim_view = prims_pinned.numpy().view(S.PRIMITIVE_DT)
+    sc, keep = sd.to_ctypes()
+    sc.primitives = prims_pinned.data_ptr()
+    L = api.lib()
+
+    def e2e_step():
+        st = L.st_upload_primitives(r.ctx, 0, C.byref(sc))
+        st |= L.st_render_scene(r.ctx, 0, C.byref(sc), C.byref(e2e_frame.viewport))
+        assert st == 0, st
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    with torch.cuda.stream(stream):
+        e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * grid * args.steps / (e2e_ms / 1e3) / 1e6
+    h2d = len(prim_view) * S.PRIMITIVE_DT.itemsize
+    d2h = grid * 24 + WIDTH * HEIGHT * 4
+
+    # ---- roofline of the trace kernel -----------------------------------------------------------
+    trace_avg_ms = sum(trace_ms) / len(trace_ms)
+    peaks = measured_peaks()
+    peak = peaks["hbm_gbs"] if peaks and "hbm_gbs" in peaks else 6650.0
+    achieved = bytes_alg / (trace_avg_ms / 1e3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "trace_kernel_config1_traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            try:
+                import oracle
+                if oracle.reference_available():
+                    threads = os.cpu_count() or 1
+                    ref_sd = sd.copy()
+                    ref_sd.meshes = sd.meshes
+                    import tests.helpers as H
+                    H.tlas_sah(ref_sd, "ref")
+                    rows = calibrated_reference(ref_sd, cam, threads, 15.0)
+                    rays, dt = cpu_reference_rows(ref_sd, cam, rows, threads)
+                    cpu = {"value": rays / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "reference",
+                           "sample": f"{rows} of {HEIGHT + 1} QCAA rows spread evenly, same scene bytes, "
+                                     f"{dt:.1f} s on {threads} host threads"}
+            except Exception as ex:  # the baseline is reported, never required
+                cpu = {"value": None, "unit": "Mrays/s", "cores": os.cpu_count(), "kind": "reference",
+                       "sample": f"failed: {ex}"}
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded config1 scene: displaced icosphere, Perlin textures; no dataset)",
+            "config": {"workload": "config1 1080p PBR mesh scene, depth 4, 1.31M-triangle BLAS x 8 instances",
+                       "width": WIDTH, "height": HEIGHT, "depth": DEPTH, "rays_per_frame": grid,
+                       "triangles": sd.meshes[0].triangle_count, "instances": 8, "parallelism": f"replicas x{world}",
+                       "l2": "flushed before every step (256 MiB write, outside the timed events)",
+                       "blas": "LBVH30 on device", "tlas": "LBVH30 on device"},
+            "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "api": "st_upload_primitives + st_render_scene, pinned host buffers"},
+            "gpu_launches": 4 * args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "trace_kernel", "kernel_ms": trace_avg_ms,
+                         "bytes_alg_per_launch": bytes_alg,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6.65 TB/s"},
+            "counters": counters,
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    r.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

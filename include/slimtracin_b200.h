@@ -1,0 +1,152 @@
+/*
+ * slimtracin_b200.h — C ABI of libslimtracin_b200, the B200 (sm_100a) tracing path of SlimTracin.
+ *
+ * The library replaces the reference's per-frame render and its BVH updates:
+ *   renderScene        render/raytracer.h:302   -> st_render_scene / st_render_ex
+ *   updateSceneBVH     acceleration_structures/builder_top_down.h:366 -> st_update_scene_bvh
+ *   updateMeshBVH      acceleration_structures/builder_top_down.h:272 -> st_update_mesh_bvh
+ *   allocateDeviceScene, upload*   core/init.h:36-126 -> st_allocate_device_scene, st_upload_*
+ *
+ * Conventions (they differ from the reference on purpose, see each function):
+ *   - every entry point returns an int status, ST_OK == 0; nothing calls exit();
+ *   - the library owns all device memory; host structs are read-only inputs unless a function says
+ *     it writes them; output buffers are caller-allocated;
+ *   - one st_ctx is used by one host thread at a time.
+ */
+#ifndef SLIMTRACIN_B200_H
+#define SLIMTRACIN_B200_H
+
+#include "slimtracin_types.h"
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define ST_API __attribute__((visibility("default")))
+#else
+#define ST_API
+#endif
+
+typedef struct st_ctx st_ctx;
+
+enum st_status {
+    ST_OK = 0,
+    ST_ERR_INVALID_ARG = 1,     /* a null pointer, a bad slot, a size outside the stated limits */
+    ST_ERR_NO_DEVICE = 2,       /* no CUDA device, or the device is not sm_100 */
+    ST_ERR_CUDA = 3,            /* a CUDA runtime call failed; st_last_cuda_error() has the text */
+    ST_ERR_OUT_OF_MEMORY = 4,   /* cudaMalloc failed */
+    ST_ERR_BUDGET = 5,          /* the request would exceed the context's device-memory budget */
+    ST_ERR_STACK_OVERFLOW = 6,  /* a traversal stack overflowed (the kernel stops that ray) */
+    ST_ERR_TIMEOUT = 7,         /* a bounded device-side wait gave up */
+    ST_ERR_NOT_RESIDENT = 8,    /* the scene slot holds no uploaded scene */
+    ST_ERR_BAD_SCENE = 9,       /* the scene data is inconsistent (e.g. a leaf id out of range) */
+    ST_ERR_QUEUE_FULL = 10,     /* the serving queue has no free slot */
+    ST_ERR_NOT_READY = 11,      /* st_poll: the request is still running */
+    ST_ERR_CANCELLED = 12       /* st_poll: the request was cancelled before it ran */
+};
+
+/* TLAS/BLAS build modes for st_update_scene_bvh / st_update_mesh_bvh. */
+enum st_bvh_mode {
+    ST_BVH_LBVH30 = 1,      /* 30-bit Morton LBVH: device radix sort, Karras topology, leaf collapse */
+    ST_BVH_BINNED_SAH = 2,  /* top-down binned SAH on the device */
+    ST_BVH_REFIT = 3        /* keep the resident topology, recompute every AABB bottom-up */
+};
+
+typedef struct st_config {
+    int device;                 /* CUDA device ordinal */
+    uint64_t memory_budget;     /* bytes of device memory the context may hold; 0 -> 120 GB */
+    int max_scenes;             /* resident scene slots; 0 -> 16 */
+    uint32_t flags;             /* reserved, 0 */
+} st_config;
+
+/* Outputs and knobs of one render, beyond what the reference's Viewport carries.
+ * All output pointers are optional.  When `device_outputs` is non-zero they are device pointers and
+ * no host copy happens inside the call. */
+typedef struct st_render_options {
+    void *stream;               /* cudaStream_t to launch on; NULL -> the context's stream */
+    int device_outputs;         /* 1: the out_* pointers below are device pointers */
+    FloatPixel *out_float;      /* (W+1)x(H+1) QCAA grid; NULL -> viewport->frame_buffer->float_pixels */
+    Pixel *out_u8;              /* W x H resolved BGRA; NULL -> viewport->frame_buffer->pixels */
+    uint32_t *out_prim_id;      /* (W+1)x(H+1) primary-hit primitive id, 0xFFFFFFFF on a miss */
+    int skip_float_copy;        /* 1: do not copy the float grid to the host (u8 only) */
+    int count_work;             /* 1: fill `counters` (a slower instrumented kernel) */
+    uint64_t counters[16];      /* out: see enum st_counter */
+    float trace_ms;             /* out: CUDA-event time of the trace kernel on the launch stream */
+    float total_ms;             /* out: CUDA-event time of the whole render on the launch stream */
+} st_render_options;
+
+enum st_counter {
+    ST_CNT_PRIMARY_RAYS = 0,
+    ST_CNT_SHADOW_RAYS = 1,     /* point-light shadow rays (any-hit TLAS walks) */
+    ST_CNT_BOUNCE_RAYS = 2,     /* reflection/refraction rays (closest-hit TLAS walks) */
+    ST_CNT_AABB_TESTS = 3,      /* TLAS + BLAS node AABB tests */
+    ST_CNT_TRIANGLE_TESTS = 4,
+    ST_CNT_PRIMITIVE_TESTS = 5, /* implicit-primitive intersection tests */
+    ST_CNT_LEAF_ID_READS = 6,
+    ST_CNT_SHADED_HITS = 7,
+    ST_CNT_TEXEL_FETCHES = 8,
+    ST_CNT_MESH_ENTRIES = 9,    /* BLAS traversals started */
+    ST_CNT_COUNT = 10
+};
+
+/* ---- context ---------------------------------------------------------------------------------- */
+ST_API int  st_init(st_ctx **ctx, const st_config *cfg);
+ST_API void st_shutdown(st_ctx *ctx);
+ST_API const char *st_strerror(int status);
+ST_API const char *st_last_cuda_error(st_ctx *ctx);
+ST_API void *st_get_stream(st_ctx *ctx);                       /* the context's cudaStream_t */
+ST_API uint64_t st_device_bytes_in_use(st_ctx *ctx);
+/* Size of a contract struct ("Primitive") or offset of a field ("Primitive.rotation") as this
+ * library was compiled; -1 if the name is not in include/slimtracin_layout.h. */
+ST_API long st_layout_query(const char *name);
+
+/* ---- residency: core/init.h:36-126 -------------------------------------------------------------- */
+/* allocateDeviceScene (core/init.h:36): reserve device arenas for `scene` in `slot`. */
+ST_API int st_allocate_device_scene(st_ctx *ctx, int slot, const Scene *scene);
+/* uploadScene (core/init.h:85): lights, primitives, materials, textures (+ mip chains). */
+ST_API int st_upload_scene(st_ctx *ctx, int slot, const Scene *scene);
+/* uploadPrimitives (core/init.h:74). */
+ST_API int st_upload_primitives(st_ctx *ctx, int slot, const Scene *scene);
+/* uploadMaterials (core/init.h:77). */
+ST_API int st_upload_materials(st_ctx *ctx, int slot, const Scene *scene);
+/* uploadLights (core/init.h:80). */
+ST_API int st_upload_lights(st_ctx *ctx, int slot, const Scene *scene);
+/* uploadSceneBVH (core/init.h:106): the host-built TLAS (scene->bvh) as-is. */
+ST_API int st_upload_scene_bvh(st_ctx *ctx, int slot, const Scene *scene);
+/* uploadMeshBVHs (core/init.h:111): every mesh's BLAS nodes and BVH-ordered Triangles as-is. */
+ST_API int st_upload_mesh_bvhs(st_ctx *ctx, int slot, const Scene *scene);
+/* Primitives whose transform changed since the last upload: re-upload only those records and mark
+ * the TLAS dirty (serving path; the reference re-uploads the whole array, core/init.h:74). */
+ST_API int st_update_primitives(st_ctx *ctx, int slot, const Primitive *primitives,
+                         const uint32_t *ids, uint32_t count);
+ST_API int st_free_scene(st_ctx *ctx, int slot);
+
+/* ---- BVH builds: render/acceleration_structures/builder_top_down.h ---------------------------- */
+/* updateSceneBVH (builder_top_down.h:366): build the TLAS of the resident primitives on the device.
+ * mode: ST_BVH_LBVH30 | ST_BVH_BINNED_SAH | ST_BVH_REFIT.  When scene->bvh.nodes and
+ * scene->bvh.leaf_ids are non-null the result is also copied there (node_count, height set). */
+ST_API int st_update_scene_bvh(st_ctx *ctx, int slot, Scene *scene, int mode);
+/* updateMeshBVH (builder_top_down.h:272): build the BLAS of `mesh` on the device and write the
+ * reference's outputs into the caller's arrays: mesh->bvh.nodes (capacity 2*triangle_count),
+ * mesh->bvh.leaf_ids, mesh->bvh.node_count/height and the BVH-ordered mesh->triangles. */
+ST_API int st_update_mesh_bvh(st_ctx *ctx, Mesh *mesh, int mode);
+
+/* ---- render: render/raytracer.h:302 ------------------------------------------------------------ */
+/* renderScene (raytracer.h:302) + the QCAA resolve of drawViewportToWindowContent (viewport.h:12).
+ * Renders the scene resident in `slot` from viewport->camera into viewport->frame_buffer:
+ * float_pixels ((W+1)x(H+1), as renderScene leaves them after beginDrawing) and, when
+ * frame_buffer->pixels is non-null, the resolved W x H BGRA pixels.  `scene` supplies the per-frame
+ * values the reference passes by value to its kernel (counts, ambient light); the arrays come from
+ * the device copy.  viewport->trace.depth is the bounce count. */
+ST_API int st_render_scene(st_ctx *ctx, int slot, const Scene *scene, Viewport *viewport);
+/* st_render_scene with explicit outputs, stream, counters and timings. */
+ST_API int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *viewport,
+                 st_render_options *options);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SLIMTRACIN_B200_H */

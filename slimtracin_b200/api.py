@@ -1,0 +1,190 @@
+"""ctypes binding of libslimtracin_b200 (include/slimtracin_b200.h) and a thin Python host over it.
+
+The binding is the same one a SlimTracin host written in C links against; `Renderer` mirrors the
+reference's per-frame sequence (core/init.h:36-126 uploads, builder_top_down.h:366 updateSceneBVH,
+raytracer.h:302 renderScene) on reference structs built by `scenes`.  There is no CPU path: every
+call goes to the CUDA library, and importing fails loudly when it is not built.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import structs as S
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libslimtracin_b200.so")
+
+ST_OK = 0
+ST_BVH_LBVH30, ST_BVH_BINNED_SAH, ST_BVH_REFIT = 1, 2, 3
+COUNTER_NAMES = ["primary_rays", "shadow_rays", "bounce_rays", "aabb_tests", "triangle_tests",
+                 "primitive_tests", "leaf_id_reads", "shaded_hits", "texel_fetches", "mesh_entries"]
+
+
+class st_config(C.Structure):
+    _fields_ = [("device", C.c_int), ("memory_budget", C.c_uint64), ("max_scenes", C.c_int),
+                ("flags", C.c_uint32)]
+
+
+class st_render_options(C.Structure):
+    _fields_ = [("stream", C.c_void_p), ("device_outputs", C.c_int), ("out_float", C.c_void_p),
+                ("out_u8", C.c_void_p), ("out_prim_id", C.c_void_p), ("skip_float_copy", C.c_int),
+                ("count_work", C.c_int), ("counters", C.c_uint64 * 16), ("trace_ms", C.c_float),
+                ("total_ms", C.c_float)]
+
+
+class STError(RuntimeError):
+    def __init__(self, status, what, detail=""):
+        self.status = status
+        super().__init__(f"{what}: status {status} ({lib().st_strerror(status).decode()}) {detail}".strip())
+
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library; raise if it is missing (there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is not built; run `python -m slimtracin_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        vp, i, u32, u64 = C.c_void_p, C.c_int, C.c_uint32, C.c_uint64
+        sig = {
+            "st_init": (i, [C.POINTER(vp), C.POINTER(st_config)]),
+            "st_shutdown": (None, [vp]),
+            "st_strerror": (C.c_char_p, [i]),
+            "st_last_cuda_error": (C.c_char_p, [vp]),
+            "st_get_stream": (vp, [vp]),
+            "st_device_bytes_in_use": (u64, [vp]),
+            "st_layout_query": (C.c_long, [C.c_char_p]),
+            "st_allocate_device_scene": (i, [vp, i, vp]),
+            "st_upload_scene": (i, [vp, i, vp]),
+            "st_upload_primitives": (i, [vp, i, vp]),
+            "st_upload_materials": (i, [vp, i, vp]),
+            "st_upload_lights": (i, [vp, i, vp]),
+            "st_upload_scene_bvh": (i, [vp, i, vp]),
+            "st_upload_mesh_bvhs": (i, [vp, i, vp]),
+            "st_update_primitives": (i, [vp, i, vp, vp, u32]),
+            "st_free_scene": (i, [vp, i]),
+            "st_update_scene_bvh": (i, [vp, i, vp, i]),
+            "st_update_mesh_bvh": (i, [vp, vp, i]),
+            "st_render_scene": (i, [vp, i, vp, vp]),
+            "st_render_ex": (i, [vp, i, vp, vp, C.POINTER(st_render_options)]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def declared_functions(header=os.path.join(os.path.dirname(HERE), "include", "slimtracin_b200.h")):
+    """Names of the functions the public header declares."""
+    import re
+    text = open(header).read()
+    return sorted(set(re.findall(r"ST_API[^;(]*?\b(st_[a-z_0-9]+)\s*\(", text)))
+
+
+class Renderer:
+    """One library context on one GPU."""
+
+    def __init__(self, device=0, memory_budget=0, max_scenes=16):
+        self.L = lib()
+        self.ctx = C.c_void_p()
+        cfg = st_config(device, memory_budget, max_scenes, 0)
+        self._check(self.L.st_init(C.byref(self.ctx), C.byref(cfg)), "st_init")
+        self._keep = {}
+
+    def _check(self, status, what):
+        if status != ST_OK:
+            detail = ""
+            if getattr(self, "ctx", None) and self.ctx:
+                detail = self.L.st_last_cuda_error(self.ctx).decode()
+            raise STError(status, what, detail)
+
+    def close(self):
+        if self.ctx:
+            self.L.st_shutdown(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self):
+        return self.L.st_get_stream(self.ctx)
+
+    # -- residency ---------------------------------------------------------------------------------
+    def upload(self, slot, sd, tlas="host"):
+        """Upload a SceneData: scene arrays, mesh BLASes (as built) and the TLAS.
+        tlas: "host" (sd.tlas_* as given), "lbvh" (build on the device) or None."""
+        sc, keep = sd.to_ctypes()
+        self._keep[slot] = (sc, keep, sd)
+        self._check(self.L.st_upload_scene(self.ctx, slot, C.byref(sc)), "st_upload_scene")
+        if sd.meshes:
+            self._check(self.L.st_upload_mesh_bvhs(self.ctx, slot, C.byref(sc)), "st_upload_mesh_bvhs")
+        if tlas == "host":
+            self._check(self.L.st_upload_scene_bvh(self.ctx, slot, C.byref(sc)), "st_upload_scene_bvh")
+        elif tlas == "lbvh":
+            self.build_tlas(slot, sd, ST_BVH_LBVH30)
+        return sc
+
+    def build_tlas(self, slot, sd, mode=ST_BVH_LBVH30):
+        sc, keep = sd.to_ctypes()
+        self._check(self.L.st_update_scene_bvh(self.ctx, slot, C.byref(sc), mode), "st_update_scene_bvh")
+        sd.read_back_tlas(sc)
+        return sd
+
+    def build_blas(self, md, mode=ST_BVH_LBVH30):
+        """Build a MeshData's BLAS on the device (updateMeshBVH); fills md.nodes/leaf_ids/triangles."""
+        keep = []
+        md.allocate_bvh()
+        m = md.to_ctypes(keep)
+        self._check(self.L.st_update_mesh_bvh(self.ctx, C.byref(m), mode), "st_update_mesh_bvh")
+        md.read_back(m)
+        return md
+
+    def update_primitives(self, slot, prims, ids):
+        prims = np.ascontiguousarray(prims, dtype=S.PRIMITIVE_DT)
+        ids = np.ascontiguousarray(ids, dtype=np.uint32)
+        self._check(self.L.st_update_primitives(self.ctx, slot, prims.ctypes.data, ids.ctypes.data, len(ids)),
+                    "st_update_primitives")
+
+    def free(self, slot):
+        self._check(self.L.st_free_scene(self.ctx, slot), "st_free_scene")
+        self._keep.pop(slot, None)
+
+    # -- render --------------------------------------------------------------------------------------
+    def render(self, slot, sd, frame, prim_ids=None, count_work=False, skip_float_copy=False):
+        """st_render_ex into the frame's host buffers; returns the options struct (timings,
+        counters)."""
+        sc, keep = sd.to_ctypes()
+        opt = st_render_options()
+        if prim_ids is not None:
+            opt.out_prim_id = prim_ids.ctypes.data
+        opt.count_work = int(count_work)
+        opt.skip_float_copy = int(skip_float_copy)
+        self._check(self.L.st_render_ex(self.ctx, slot, C.byref(sc), C.byref(frame.viewport), C.byref(opt)),
+                    "st_render_ex")
+        return opt
+
+    def render_device(self, slot, sd, frame, out_float_ptr, out_u8_ptr=None, stream=None):
+        """st_render_ex with device-resident outputs (no host copies inside the call)."""
+        sc, keep = sd.to_ctypes()
+        opt = st_render_options()
+        opt.device_outputs = 1
+        opt.out_float = out_float_ptr
+        opt.out_u8 = out_u8_ptr
+        opt.stream = stream
+        self._check(self.L.st_render_ex(self.ctx, slot, C.byref(sc), C.byref(frame.viewport), C.byref(opt)),
+                    "st_render_ex")
+        return opt
+
+
+def counters_dict(opt):
+    return {k: int(opt.counters[i]) for i, k in enumerate(COUNTER_NAMES)}

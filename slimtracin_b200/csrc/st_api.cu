@@ -1,0 +1,745 @@
+// st_api.cu — the C ABI of libslimtracin_b200 (include/slimtracin_b200.h): context, scene residency,
+// BVH builds and the render entry points.
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include "slimtracin_b200.h"
+#include "slimtracin_layout.h"
+#include "st_kernels.h"
+
+using namespace st;
+
+namespace {
+
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct SceneSlot {
+    bool allocated = false;
+    u32t n_prims = 0, n_materials = 0, n_lights = 0, n_meshes = 0, n_textures = 0;
+    u32t cap_prims = 0, cap_materials = 0, cap_lights = 0, cap_tris = 0, cap_meshes = 0, cap_mips = 0;
+    size_t cap_quads = 0;
+    DevBuf prims_raw, prims, materials, lights;
+    DevBuf tlas_nodes, tlas_leaf_ids, tlas_pairs, tlas_aabbs, tlas_scratch;
+    u32t tlas_node_count = 0, tlas_height = 0;
+    bool tlas_valid = false;
+    BVHNode tlas_root{};
+    DevBuf meshes, mesh_pairs, tri_hot, tri_full;
+    std::vector<MeshDev> mesh_host;
+    bool meshes_valid = false;
+    DevBuf textures, mips, quads;
+    DevBuf emissive, occluders;
+    u32t n_emissive = 0, n_occluders = 0;
+    vec3 ambient{};
+    bool lights_present = false;
+    std::vector<Primitive> prims_host;    // host copy for the emissive/occluder lists
+    std::vector<Material> materials_host;
+};
+
+}  // namespace
+
+struct st_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint64_t budget = 0, in_use = 0;
+    std::vector<SceneSlot> slots;
+    DevBuf ssb, dirs, out_float, out_u8, prim_ids, status, counters;
+    LbvhScratch lbvh;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    std::string cuda_error;
+};
+
+namespace {
+
+int fail_cuda(st_ctx *ctx, cudaError_t e) {
+    ctx->cuda_error = cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? ST_ERR_OUT_OF_MEMORY : ST_ERR_CUDA;
+}
+int ST_CUDA_SYNC(st_ctx *ctx) {
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? ST_OK : fail_cuda(ctx, e);
+}
+#define ST_CUDA(call)                                     \
+    do {                                                  \
+        cudaError_t e_ = (call);                          \
+        if (e_ != cudaSuccess) return fail_cuda(ctx, e_); \
+    } while (0)
+
+void release(st_ctx *ctx, DevBuf &b) {
+    if (b.ptr) {
+        cudaFree(b.ptr);
+        ctx->in_use -= b.bytes;
+    }
+    b = DevBuf();
+}
+// Grow `b` to at least `bytes` (contents are not kept).  Refuses past the context's budget.
+int reserve(st_ctx *ctx, DevBuf &b, size_t bytes) {
+    if (bytes <= b.bytes && b.ptr) return ST_OK;
+    if (bytes == 0) bytes = 16;
+    size_t add = bytes - (b.ptr ? b.bytes : 0);
+    if (ctx->in_use + add > ctx->budget) return ST_ERR_BUDGET;
+    release(ctx, b);
+    cudaError_t e = cudaMalloc(&b.ptr, bytes);
+    if (e != cudaSuccess) return fail_cuda(ctx, e);
+    b.bytes = bytes;
+    ctx->in_use += bytes;
+    return ST_OK;
+}
+#define ST_TRY(x)                    \
+    do {                             \
+        int s_ = (x);                \
+        if (s_ != ST_OK) return s_;  \
+    } while (0)
+
+template <class T> T *P(DevBuf &b) { return static_cast<T *>(b.ptr); }
+
+SceneSlot *slot_of(st_ctx *ctx, int slot) {
+    if (!ctx || slot < 0 || slot >= (int)ctx->slots.size()) return nullptr;
+    return &ctx->slots[slot];
+}
+
+u32t total_triangles(const Scene *s) {
+    u32t t = 0;
+    for (u32t i = 0; i < s->settings.meshes; i++) t += s->meshes[i].triangle_count;
+    return t;
+}
+
+int allocate(st_ctx *ctx, SceneSlot &S, const Scene *scene) {
+    const u32t np = scene->settings.primitives, nm = scene->settings.materials, nl = scene->settings.lights;
+    const u32t nt = scene->meshes ? total_triangles(scene) : 0;
+    const u32t nmesh = scene->meshes ? scene->settings.meshes : 0;
+    u32t nmip = 0;
+    size_t nquad = 0;
+    for (u32t t = 0; scene->textures && t < scene->settings.textures; t++) {
+        nmip += scene->textures[t].mip_count;
+        for (u32t m = 0; m < scene->textures[t].mip_count; m++)
+            nquad += (size_t)(scene->textures[t].mips[m].width + 1) * (scene->textures[t].mips[m].height + 1);
+    }
+    ST_TRY(reserve(ctx, S.prims_raw, sizeof(Primitive) * np));
+    ST_TRY(reserve(ctx, S.prims, sizeof(PrimDev) * np));
+    ST_TRY(reserve(ctx, S.materials, sizeof(Material) * std::max(nm, 1u)));
+    ST_TRY(reserve(ctx, S.lights, sizeof(Light) * std::max(nl, 1u)));
+    ST_TRY(reserve(ctx, S.tlas_nodes, sizeof(BVHNode) * 2 * std::max(np, 1u)));
+    ST_TRY(reserve(ctx, S.tlas_leaf_ids, sizeof(u32t) * std::max(np, 1u)));
+    ST_TRY(reserve(ctx, S.tlas_pairs, sizeof(NodePair) * std::max(np, 1u)));
+    ST_TRY(reserve(ctx, S.tlas_aabbs, sizeof(float) * 6 * std::max(np, 1u)));
+    ST_TRY(reserve(ctx, S.tlas_scratch, (sizeof(u32t) * 2 + sizeof(unsigned) * 6) * 2 * std::max(np, 1u)));
+    ST_TRY(reserve(ctx, S.meshes, sizeof(MeshDev) * std::max(nmesh, 1u)));
+    ST_TRY(reserve(ctx, S.mesh_pairs, sizeof(NodePair) * std::max(nt, 1u)));
+    ST_TRY(reserve(ctx, S.tri_hot, sizeof(TriHot) * std::max(nt, 1u)));
+    ST_TRY(reserve(ctx, S.tri_full, sizeof(Triangle) * std::max(nt, 1u)));
+    ST_TRY(reserve(ctx, S.textures, sizeof(TexDev) * std::max(scene->settings.textures, 1u)));
+    ST_TRY(reserve(ctx, S.mips, sizeof(MipDev) * std::max(nmip, 1u)));
+    ST_TRY(reserve(ctx, S.quads, sizeof(TexelQuad) * std::max(nquad, (size_t)1)));
+    ST_TRY(reserve(ctx, S.emissive, sizeof(u32t) * std::max(np, 1u)));
+    ST_TRY(reserve(ctx, S.occluders, sizeof(u32t) * std::max(np, 1u)));
+    S.cap_prims = np;
+    S.cap_materials = nm;
+    S.cap_lights = nl;
+    S.cap_tris = nt;
+    S.cap_meshes = nmesh;
+    S.cap_mips = nmip;
+    S.cap_quads = nquad;
+    S.allocated = true;
+    return ST_OK;
+}
+
+bool fits(const SceneSlot &S, const Scene *scene) {
+    if (!S.allocated) return false;
+    if (scene->settings.primitives > S.cap_prims || scene->settings.materials > S.cap_materials ||
+        scene->settings.lights > S.cap_lights)
+        return false;
+    if (scene->meshes && (scene->settings.meshes > S.cap_meshes || total_triangles(scene) > S.cap_tris)) return false;
+    return true;
+}
+
+int ensure(st_ctx *ctx, SceneSlot &S, const Scene *scene) {
+    if (fits(S, scene)) return ST_OK;
+    return allocate(ctx, S, scene);
+}
+
+// emissive quads (closest_hit/surface.h:46-49,172-178) and the sphere/quad occluders of the
+// analytic area-light shadow (surface.h:84-114), both in primitive index order
+int refresh_lists(st_ctx *ctx, SceneSlot &S) {
+    std::vector<u32t> em, oc;
+    for (u32t i = 0; i < S.prims_host.size(); i++) {
+        const Primitive &p = S.prims_host[i];
+        if (p.type == PrimitiveType_Quad && p.material_id < S.materials_host.size() &&
+            (S.materials_host[p.material_id].is & EMISSIVE))
+            em.push_back(i);
+        if (p.type == PrimitiveType_Sphere || p.type == PrimitiveType_Quad) oc.push_back(i);
+    }
+    S.n_emissive = (u32t)em.size();
+    S.n_occluders = (u32t)oc.size();
+    if (!em.empty()) ST_CUDA(cudaMemcpyAsync(S.emissive.ptr, em.data(), em.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+    if (!oc.empty()) ST_CUDA(cudaMemcpyAsync(S.occluders.ptr, oc.data(), oc.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+    return ST_CUDA_SYNC(ctx);
+}
+
+}  // namespace
+
+// ================================================================================================
+extern "C" {
+
+const char *st_strerror(int s) {
+    switch (s) {
+        case ST_OK: return "ok";
+        case ST_ERR_INVALID_ARG: return "invalid argument";
+        case ST_ERR_NO_DEVICE: return "no usable CUDA device (sm_100 required)";
+        case ST_ERR_CUDA: return "CUDA runtime error";
+        case ST_ERR_OUT_OF_MEMORY: return "device allocation failed";
+        case ST_ERR_BUDGET: return "device-memory budget exceeded";
+        case ST_ERR_STACK_OVERFLOW: return "traversal stack overflow";
+        case ST_ERR_TIMEOUT: return "device-side wait timed out";
+        case ST_ERR_NOT_RESIDENT: return "scene slot is not resident";
+        case ST_ERR_BAD_SCENE: return "inconsistent scene data";
+        case ST_ERR_QUEUE_FULL: return "request queue full";
+        case ST_ERR_NOT_READY: return "request not finished";
+        case ST_ERR_CANCELLED: return "request cancelled";
+        default: return "unknown status";
+    }
+}
+
+long st_layout_query(const char *name) {
+    if (!name) return -1;
+#define ST_Q_S(T) if (!strcmp(name, #T)) return (long)sizeof(T);
+#define ST_Q_F(T, F) if (!strcmp(name, #T "." #F)) return (long)offsetof(T, F);
+    ST_LAYOUT_LIST(ST_Q_S, ST_Q_F)
+#undef ST_Q_S
+#undef ST_Q_F
+    return -1;
+}
+
+int st_init(st_ctx **out, const st_config *cfg) {
+    if (!out) return ST_ERR_INVALID_ARG;
+    *out = nullptr;
+    int device = cfg ? cfg->device : 0;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) return ST_ERR_NO_DEVICE;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) return ST_ERR_NO_DEVICE;
+    st_ctx *ctx = new st_ctx();
+    ctx->device = device;
+    ctx->budget = (cfg && cfg->memory_budget) ? cfg->memory_budget : (uint64_t)120 << 30;
+    ctx->slots.resize((cfg && cfg->max_scenes > 0) ? cfg->max_scenes : 16);
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&ctx->ev[i]);
+    if (e != cudaSuccess) {
+        delete ctx;
+        return ST_ERR_CUDA;
+    }
+    int s = reserve(ctx, ctx->status, 16);
+    if (s == ST_OK) s = reserve(ctx, ctx->counters, sizeof(unsigned long long) * 16);
+    if (s != ST_OK) {
+        st_shutdown(ctx);
+        return s;
+    }
+    *out = ctx;
+    return ST_OK;
+}
+
+void st_shutdown(st_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (int i = 0; i < (int)ctx->slots.size(); i++) st_free_scene(ctx, i);
+    for (DevBuf *b : {&ctx->ssb, &ctx->dirs, &ctx->out_float, &ctx->out_u8, &ctx->prim_ids, &ctx->status, &ctx->counters})
+        release(ctx, *b);
+    lbvh_release(ctx->lbvh);
+    for (auto &e : ctx->ev) if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char *st_last_cuda_error(st_ctx *ctx) { return ctx ? ctx->cuda_error.c_str() : ""; }
+void *st_get_stream(st_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+uint64_t st_device_bytes_in_use(st_ctx *ctx) { return ctx ? ctx->in_use : 0; }
+
+int st_free_scene(st_ctx *ctx, int slot) {
+    SceneSlot *S = slot_of(ctx, slot);
+    if (!S) return ST_ERR_INVALID_ARG;
+    for (DevBuf *b : {&S->prims_raw, &S->prims, &S->materials, &S->lights, &S->tlas_nodes, &S->tlas_leaf_ids,
+                      &S->tlas_pairs, &S->tlas_aabbs, &S->tlas_scratch, &S->meshes, &S->mesh_pairs, &S->tri_hot,
+                      &S->tri_full, &S->textures, &S->mips, &S->quads, &S->emissive, &S->occluders})
+        release(ctx, *b);
+    *S = SceneSlot();
+    return ST_OK;
+}
+
+int st_allocate_device_scene(st_ctx *ctx, int slot, const Scene *scene) {
+    SceneSlot *S = slot_of(ctx, slot);
+    if (!S || !scene) return ST_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    return allocate(ctx, *S, scene);
+}
+
+int st_upload_primitives(st_ctx *ctx, int slot, const Scene *scene) {
+    SceneSlot *S = slot_of(ctx, slot);
+    if (!S || !scene || (scene->settings.primitives && !scene->primitives)) return ST_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    ST_TRY(ensure(ctx, *S, scene));
+    const u32t n = scene->settings.primitives;
+    for (u32t i = 0; i < n; i++) {
+        const Primitive &p = scene->primitives[i];
+        if (p.type == PrimitiveType_Mesh && (!scene->meshes || p.id >= scene->settings.meshes)) return ST_ERR_BAD_SCENE;
+        if (p.material_id >= scene->settings.materials) return ST_ERR_BAD_SCENE;
+    }
+    S->n_prims = n;
+    S->prims_host.assign(scene->primitives, scene->primitives + n);
+    if (n) {
+        ST_CUDA(cudaMemcpyAsync(S->prims_raw.ptr, scene->primitives, sizeof(Primitive) * n, cudaMemcpyHostToDevice, ctx->stream));
+        launch_make_primdev(P<Primitive>(S->prims_raw), n, P<PrimDev>(S->prims), ctx->stream);
+    }
+    return refresh_lists(ctx, *S);
+}
+
+int st_upload_materials(st_ctx *ctx, int slot, const Scene *scene) {
+    SceneSlot *S = slot_of(ctx, slot);
+    if (!S || !scene || (scene->settings.materials && !scene->materials)) return ST_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    ST_TRY(ensure(ctx, *S, scene));
+    const u32t n = scene->settings.materials;
+    for (u32t i = 0; i < n; i++) {
+        const Material &m = scene->materials[i];
+        if (m.texture_count && m.use) {
+            for (u32t k = 0; k < m.texture_count && k < 2; k++)
+                if (m.texture_ids[k] >= scene->settings.textures || !scene->textures) return ST_ERR_BAD_SCENE;
+        }
+    }
+    S->n_materials = n;
+    S->materials_host.assign(scene->materials, scene->materials + n);
+    if (n) ST_CUDA(cudaMemcpyAsync(S->materials.ptr, scene->materials, sizeof(Material) * n, cudaMemcpyHostToDevice, ctx->stream));
+    return refresh_lists(ctx, *S);
+}
+
+int st_upload_lights(st_ctx *ctx, int slot, const Scene *scene) {
+    SceneSlot *S = slot_of(ctx, slot);
+    if (!S || !scene || (scene->settings.lights && !scene->lights)) return ST_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    ST_TRY(ensure(ctx, *S, scene));
+    S->n_lights = scene->settings.lights;
+    S->lights_present = scene->lights != nullptr;
+    if (S->n_lights)
+        ST_CUDA(cudaMemcpyAsync(S->lights.ptr, scene->lights, sizeof(Light) * S->n_lights, cudaMemcpyHostToDevice, ctx->stream));
+    return ST_CUDA_SYNC(ctx);
+}
+
+static int upload_textures(st_ctx *ctx, SceneSlot &S, const Scene *scene) {
+    std::vector<TexDev> tex;
+    std::vector<MipDev> mips;
+    size_t quad_off = 0;
+    S.n_textures = scene->textures ? scene->settings.textures : 0;
+    for (u32t t = 0; t < S.n_textures; t++) {
+        const Texture &T = scene->textures[t];
+        if (!T.mip_count || !T.mips) return ST_ERR_BAD_SCENE;
+        TexDev d;
+        d.width = T.width;
+        d.height = T.height;
+        d.mip_count = T.mip_count;
+        d.wrap = T.wrap;
+        d.mipmap = T.mipmap;
+        d.pad = 0;
+        d.mip_offset = (u32t)mips.size();
+        tex.push_back(d);
+        for (u32t m = 0; m < T.mip_count; m++) {
+            const TextureMip &M = T.mips[m];
+            size_t nq = (size_t)(M.width + 1) * (M.height + 1);
+            if (quad_off + nq > S.cap_quads) return ST_ERR_BAD_SCENE;
+            MipDev md;
+            md.width = M.width;
+            md.height = M.height;
+            md.quad_offset = (u32t)quad_off;
+            mips.push_back(md);
+            ST_CUDA(cudaMemcpyAsync(P<TexelQuad>(S.quads) + quad_off, M.texel_quads, sizeof(TexelQuad) * nq,
+                                    cudaMemcpyHostToDevice, ctx->stream));
+            quad_off += nq;
+        }
+    }
+    if (!tex.empty()) ST_CUDA(cudaMemcpyAsync(S.textures.ptr, tex.data(), sizeof(TexDev) * tex.size(), cudaMemcpyHostToDevice, ctx->stream));
+    if (!mips.empty()) ST_CUDA(cudaMemcpyAsync(S.mips.ptr, mips.data(), sizeof(MipDev) * mips.size(), cudaMemcpyHostToDevice, ctx->stream));
+    return ST_CUDA_SYNC(ctx);
+}
+
+int st_upload_scene(st_ctx *ctx, int slot, const Scene *scene) {
+    SceneSlot *S = slot_of(ctx, slot);
+    if (!S || !scene) return ST_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    if (!fits(*S, scene)) ST_TRY(allocate(ctx, *S, scene));
+    S->ambient = scene->ambient_light.color;
+    ST_TRY(st_upload_lights(ctx, slot, scene));
+    ST_TRY(st_upload_materials(ctx, slot, scene));
+    ST_TRY(st_upload_primitives(ctx, slot, scene));
+    return upload_textures(ctx, *S, scene);
+}
+
+// A reference-layout BVH is safe to walk when, starting from the root, every internal node's
+// children pair lies inside the array and is reached exactly once (no cycles, no sharing), every
+// leaf range lies inside the item array, and the height leaves stack room.
+static bool check_bvh(const BVHNode *nodes, u32t count, u32t items, u32t height) {
+    if (!count || height + 2 > (u32t)kStack) return false;
+    if (nodes[0].child_count) return (uint64_t)nodes[0].first_child_id + nodes[0].child_count <= items;
+    std::vector<uint8_t> seen(count, 0);
+    std::vector<u32t> stack;
+    stack.push_back(0);
+    seen[0] = 1;
+    while (!stack.empty()) {
+        const BVHNode &n = nodes[stack.back()];
+        stack.pop_back();
+        if (n.child_count) {
+            if ((uint64_t)n.first_child_id + n.child_count > items) return false;
+            continue;
+        }
+        const u32t f = n.first_child_id;
+        if (!(f & 1u) || (uint64_t)f + 1 >= count || seen[f] || seen[f + 1]) return false;
+        seen[f] = seen[f + 1] = 1;
+        stack.push_back(f);
+        stack.push_back(f + 1);
+    }
+    return true;
+}
+
+static int finish_tlas(st_ctx *ctx, SceneSlot &S) {
+    if (S.tlas_node_count > 1)
+        launch_make_pairs(P<BVHNode>(S.tlas_nodes), S.tlas_node_count, P<NodePair>(S.tlas_pairs), ctx->stream);
+    ST_CUDA(cudaMemcpyAsync(&S.tlas_root, S.tlas_nodes.ptr, sizeof(BVHNode), cudaMemcpyDeviceToHost, ctx->stream));
+    ST_TRY(ST_CUDA_SYNC(ctx));
+    S.tlas_valid = true;
+    return ST_OK;
+}
+
+int st_upload_scene_bvh(st_ctx *ctx, int slot, const Scene *scene) {
+    SceneSlot *S = slot_of(ctx, slot);
+    if (!S || !scene || !scene->bvh.nodes || !scene->bvh.leaf_ids) return ST_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    ST_TRY(ensure(ctx, *S, scene));
+    const u32t n = scene->settings.primitives;
+    if (!check_bvh(scene->bvh.nodes, scene->bvh.node_count, n, scene->bvh.height)) return ST_ERR_BAD_SCENE;
+    for (u32t i = 0; i < n; i++) if (scene->bvh.leaf_ids[i] >= n) return ST_ERR_BAD_SCENE;
+    S->tlas_node_count = scene->bvh.node_count;
+    S->tlas_height = scene->bvh.height;
+    ST_CUDA(cudaMemcpyAsync(S->tlas_nodes.ptr, scene->bvh.nodes, sizeof(BVHNode) * S->tlas_node_count, cudaMemcpyHostToDevice, ctx->stream));
+    ST_CUDA(cudaMemcpyAsync(S->tlas_leaf_ids.ptr, scene->bvh.leaf_ids, sizeof(u32t) * n, cudaMemcpyHostToDevice, ctx->stream));
+    return finish_tlas(ctx, *S);
+}
+
+int st_upload_mesh_bvhs(st_ctx *ctx, int slot, const Scene *scene) {
+    SceneSlot *S = slot_of(ctx, slot);
+    if (!S || !scene || (scene->settings.meshes && !scene->meshes)) return ST_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    ST_TRY(ensure(ctx, *S, scene));
+    S->mesh_host.clear();
+    u32t tri_off = 0, pair_off = 0;
+    for (u32t m = 0; m < scene->settings.meshes; m++) {
+        const Mesh &M = scene->meshes[m];
+        if (!M.triangles || !M.bvh.nodes || !check_bvh(M.bvh.nodes, M.bvh.node_count, M.triangle_count, M.bvh.height))
+            return ST_ERR_BAD_SCENE;
+        MeshDev d;
+        memset(&d, 0, sizeof(d));
+        d.pair_offset = pair_off;
+        d.tri_offset = tri_off;
+        d.triangle_count = M.triangle_count;
+        d.root_count = M.bvh.nodes[0].child_count;
+        d.root_first = M.bvh.nodes[0].first_child_id;
+        d.normals_count = M.normals_count;
+        d.uvs_count = M.uvs_count;
+        d.height = M.bvh.height;
+        memcpy(d.aabb, &M.bvh.nodes[0].aabb, sizeof(d.aabb));
+        memcpy(d.mesh_aabb, &M.aabb, sizeof(d.mesh_aabb));
+        S->mesh_host.push_back(d);
+        ST_CUDA(cudaMemcpyAsync(P<Triangle>(S->tri_full) + tri_off, M.triangles, sizeof(Triangle) * M.triangle_count,
+                                cudaMemcpyHostToDevice, ctx->stream));
+        launch_make_trihot(P<Triangle>(S->tri_full) + tri_off, M.triangle_count, P<TriHot>(S->tri_hot) + tri_off, ctx->stream);
+        if (M.bvh.node_count > 1) {
+            // stage the nodes through the TLAS AABB scratch-free path: a temporary device copy
+            BVHNode *tmp = nullptr;
+            ST_CUDA(cudaMallocAsync((void **)&tmp, sizeof(BVHNode) * M.bvh.node_count, ctx->stream));
+            ST_CUDA(cudaMemcpyAsync(tmp, M.bvh.nodes, sizeof(BVHNode) * M.bvh.node_count, cudaMemcpyHostToDevice, ctx->stream));
+            launch_make_pairs(tmp, M.bvh.node_count, P<NodePair>(S->mesh_pairs) + pair_off, ctx->stream);
+            ST_CUDA(cudaFreeAsync(tmp, ctx->stream));
+        }
+        tri_off += M.triangle_count;
+        pair_off += M.bvh.node_count > 1 ? (M.bvh.node_count - 1) / 2 : 0;
+    }
+    S->n_meshes = (u32t)S->mesh_host.size();
+    if (S->n_meshes)
+        ST_CUDA(cudaMemcpyAsync(S->meshes.ptr, S->mesh_host.data(), sizeof(MeshDev) * S->n_meshes, cudaMemcpyHostToDevice, ctx->stream));
+    S->meshes_valid = true;
+    return ST_CUDA_SYNC(ctx);
+}
+
+int st_update_primitives(st_ctx *ctx, int slot, const Primitive *primitives, const uint32_t *ids, uint32_t count) {
+    SceneSlot *S = slot_of(ctx, slot);
+    if (!S || !S->allocated || (count && (!primitives || !ids))) return ST_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    for (uint32_t k = 0; k < count; k++) {
+        if (ids[k] >= S->n_prims) return ST_ERR_INVALID_ARG;
+        S->prims_host[ids[k]] = primitives[k];
+        ST_CUDA(cudaMemcpyAsync(P<Primitive>(S->prims_raw) + ids[k], primitives + k, sizeof(Primitive), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    if (count) launch_make_primdev(P<Primitive>(S->prims_raw), S->n_prims, P<PrimDev>(S->prims), ctx->stream);
+    return ST_CUDA_SYNC(ctx);
+}
+
+int st_update_scene_bvh(st_ctx *ctx, int slot, Scene *scene, int mode) {
+    SceneSlot *S = slot_of(ctx, slot);
+    if (!S || !S->allocated) return ST_ERR_NOT_RESIDENT;
+    cudaSetDevice(ctx->device);
+    const u32t n = S->n_prims;
+    if (!n) return ST_ERR_BAD_SCENE;
+    for (u32t i = 0; i < n; i++)
+        if (S->prims_host[i].type == PrimitiveType_Mesh && (!S->meshes_valid || S->prims_host[i].id >= S->n_meshes))
+            return ST_ERR_NOT_RESIDENT;
+    if (mode == ST_BVH_LBVH30) {
+        if (lbvh_reserve(ctx->lbvh, n) != cudaSuccess) return ST_ERR_OUT_OF_MEMORY;
+        launch_prim_aabbs(P<Primitive>(S->prims_raw), P<MeshDev>(S->meshes), n, ctx->lbvh.aabbs, ctx->stream);
+        u32t info[2];
+        cudaError_t e = lbvh_build(ctx->lbvh, n, MAX_OBJS_PER_SCENE_BVH_NODE, P<BVHNode>(S->tlas_nodes),
+                                   P<u32t>(S->tlas_leaf_ids), info, ctx->stream);
+        if (e != cudaSuccess) return fail_cuda(ctx, e);
+        S->tlas_node_count = info[0];
+        S->tlas_height = info[1];
+        if (S->tlas_height + 2 > (u32t)kStack) return ST_ERR_BAD_SCENE;
+    } else if (mode == ST_BVH_REFIT) {
+        if (!S->tlas_valid) return ST_ERR_NOT_RESIDENT;
+        launch_prim_aabbs(P<Primitive>(S->prims_raw), P<MeshDev>(S->meshes), n, P<float>(S->tlas_aabbs), ctx->stream);
+        u32t *par = P<u32t>(S->tlas_scratch);
+        u32t *arr = par + 2 * n;
+        unsigned *box = reinterpret_cast<unsigned *>(arr + 2 * n);
+        cudaError_t e = refit_bvh(P<BVHNode>(S->tlas_nodes), S->tlas_node_count, P<u32t>(S->tlas_leaf_ids),
+                                  P<float>(S->tlas_aabbs), par, arr, box, ctx->stream);
+        if (e != cudaSuccess) return fail_cuda(ctx, e);
+    } else {
+        return ST_ERR_INVALID_ARG;
+    }
+    // the walk trusts every index it reads: check the device-built array before first use
+    std::vector<BVHNode> host(S->tlas_node_count);
+    std::vector<u32t> ids(n);
+    ST_CUDA(cudaMemcpyAsync(host.data(), S->tlas_nodes.ptr, sizeof(BVHNode) * host.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    ST_CUDA(cudaMemcpyAsync(ids.data(), S->tlas_leaf_ids.ptr, sizeof(u32t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    ST_TRY(ST_CUDA_SYNC(ctx));
+    if (!check_bvh(host.data(), S->tlas_node_count, n, S->tlas_height)) return ST_ERR_BAD_SCENE;
+    for (u32t i = 0; i < n; i++) if (ids[i] >= n) return ST_ERR_BAD_SCENE;
+    ST_TRY(finish_tlas(ctx, *S));
+    if (scene && scene->bvh.nodes && scene->bvh.leaf_ids) {
+        ST_CUDA(cudaMemcpyAsync(scene->bvh.nodes, S->tlas_nodes.ptr, sizeof(BVHNode) * S->tlas_node_count, cudaMemcpyDeviceToHost, ctx->stream));
+        ST_CUDA(cudaMemcpyAsync(scene->bvh.leaf_ids, S->tlas_leaf_ids.ptr, sizeof(u32t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        ST_TRY(ST_CUDA_SYNC(ctx));
+        scene->bvh.node_count = S->tlas_node_count;
+        scene->bvh.height = S->tlas_height;
+    }
+    return ST_OK;
+}
+
+int st_update_mesh_bvh(st_ctx *ctx, Mesh *mesh, int mode) {
+    if (!ctx || !mesh || !mesh->vertex_positions || !mesh->vertex_position_indices || !mesh->vertex_normals ||
+        !mesh->vertex_normal_indices || !mesh->triangles || !mesh->bvh.nodes || !mesh->bvh.leaf_ids)
+        return ST_ERR_INVALID_ARG;
+    if (mode != ST_BVH_LBVH30) return ST_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    const u32t n = mesh->triangle_count;
+    if (!n) return ST_ERR_BAD_SCENE;
+    for (u32t i = 0; i < 3 * n; i++) {
+        if (((const uint32_t *)mesh->vertex_position_indices)[i] >= mesh->vertex_count) return ST_ERR_BAD_SCENE;
+        if (((const uint32_t *)mesh->vertex_normal_indices)[i] >= mesh->normals_count) return ST_ERR_BAD_SCENE;
+        if (mesh->uvs_count && ((const uint32_t *)mesh->vertex_uvs_indices)[i] >= mesh->uvs_count) return ST_ERR_BAD_SCENE;
+    }
+    if (lbvh_reserve(ctx->lbvh, n) != cudaSuccess) return ST_ERR_OUT_OF_MEMORY;
+    cudaStream_t st = ctx->stream;
+    size_t bytes = sizeof(vec3) * (mesh->vertex_count + mesh->normals_count) + sizeof(vec2) * (mesh->uvs_count + 1) +
+                   sizeof(uint32_t) * 9 * (size_t)n + sizeof(BVHNode) * 2 * (size_t)n + sizeof(u32t) * 2 * (size_t)n +
+                   sizeof(Triangle) * (size_t)n + 256 * 8;
+    if (ctx->in_use + bytes > ctx->budget) return ST_ERR_BUDGET;
+    char *base = nullptr;
+    ST_CUDA(cudaMallocAsync((void **)&base, bytes, st));
+    char *cur = base;
+    auto take = [&](size_t b) { char *p = cur; cur += (b + 255) & ~(size_t)255; return p; };
+    vec3 *pos = (vec3 *)take(sizeof(vec3) * mesh->vertex_count);
+    vec3 *nrm = (vec3 *)take(sizeof(vec3) * mesh->normals_count);
+    vec2 *uv = (vec2 *)take(sizeof(vec2) * (mesh->uvs_count + 1));
+    uint32_t *pidx = (uint32_t *)take(sizeof(uint32_t) * 3 * n);
+    uint32_t *nidx = (uint32_t *)take(sizeof(uint32_t) * 3 * n);
+    uint32_t *uidx = (uint32_t *)take(sizeof(uint32_t) * 3 * n);
+    BVHNode *nodes = (BVHNode *)take(sizeof(BVHNode) * 2 * n);
+    u32t *order = (u32t *)take(sizeof(u32t) * n);
+    u32t *inverse = (u32t *)take(sizeof(u32t) * n);
+    Triangle *tris = (Triangle *)take(sizeof(Triangle) * n);
+    cudaMemcpyAsync(pos, mesh->vertex_positions, sizeof(vec3) * mesh->vertex_count, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(nrm, mesh->vertex_normals, sizeof(vec3) * mesh->normals_count, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(pidx, mesh->vertex_position_indices, sizeof(uint32_t) * 3 * n, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(nidx, mesh->vertex_normal_indices, sizeof(uint32_t) * 3 * n, cudaMemcpyHostToDevice, st);
+    if (mesh->uvs_count) {
+        cudaMemcpyAsync(uv, mesh->vertex_uvs, sizeof(vec2) * mesh->uvs_count, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(uidx, mesh->vertex_uvs_indices, sizeof(uint32_t) * 3 * n, cudaMemcpyHostToDevice, st);
+    }
+    launch_tri_aabbs(pos, pidx, n, ctx->lbvh.aabbs, st);
+    u32t info[2];
+    cudaError_t e = lbvh_build(ctx->lbvh, n, MAX_TRIANGLES_PER_MESH_BVH_NODE, nodes, order, info, st);
+    if (e == cudaSuccess) {
+        launch_tri_records(pos, nrm, uv, pidx, nidx, uidx, mesh->uvs_count ? 1 : 0, order, n, tris, inverse, st);
+        cudaMemcpyAsync(mesh->bvh.nodes, nodes, sizeof(BVHNode) * info[0], cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(mesh->bvh.leaf_ids, inverse, sizeof(u32t) * n, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(mesh->triangles, tris, sizeof(Triangle) * n, cudaMemcpyDeviceToHost, st);
+        cudaFreeAsync(base, st);
+        e = cudaStreamSynchronize(st);
+    } else {
+        cudaFreeAsync(base, st);
+        cudaStreamSynchronize(st);
+    }
+    if (e != cudaSuccess) return fail_cuda(ctx, e);
+    mesh->bvh.node_count = info[0];
+    mesh->bvh.height = info[1];
+    return ST_OK;
+}
+
+// ---- render ------------------------------------------------------------------------------------
+static int make_view(const Viewport *vp, ViewDev &v) {
+    if (!vp || !vp->camera || !vp->frame_buffer) return ST_ERR_INVALID_ARG;
+    const Camera &cam = *vp->camera;
+    const Dimensions &d = vp->frame_buffer->dimensions;
+    if (d.width < 2 || d.height < 2) return ST_ERR_INVALID_ARG;
+    v.cam_pos = {cam.transform.position.x, cam.transform.position.y, cam.transform.position.z};
+    v.cam_rot_inv.axis = {cam.transform.rotation_inverted.axis.x, cam.transform.rotation_inverted.axis.y,
+                          cam.transform.rotation_inverted.axis.z};
+    v.cam_rot_inv.w = cam.transform.rotation_inverted.amount;
+    memcpy(v.cam_rot_matrix_inv, &cam.transform.rotation_matrix_inverted, sizeof(v.cam_rot_matrix_inv));
+    v.focal_length = cam.focal_length;
+    const ProjectionPlane &pp = vp->projection_plane;
+    v.pp_start = {pp.start.x, pp.start.y, pp.start.z};
+    v.pp_right = {pp.right.x, pp.right.y, pp.right.z};
+    v.pp_down = {pp.down.x, pp.down.y, pp.down.z};
+    v.cone_angle = pp.cone_angle;
+    v.grid_w = d.width;
+    v.grid_h = d.height;
+    v.f_width = d.f_width;
+    v.f_height = d.f_height;
+    v.h_width = d.h_width;
+    v.h_height = d.h_height;
+    v.width_over_height = d.width_over_height;
+    v.height_over_width = d.height_over_width;
+    v.mode = vp->settings.render_mode;
+    v.depth = vp->trace.depth;
+    v.primary_tlas = 0;
+    return ST_OK;
+}
+
+static SceneDev scene_view(SceneSlot &S, const Scene *scene) {
+    SceneDev d;
+    d.prims = P<PrimDev>(S.prims);
+    d.prims_raw = P<Primitive>(S.prims_raw);
+    d.n_prims = S.n_prims;
+    d.materials = P<Material>(S.materials);
+    const bool lights = scene ? (scene->lights != nullptr && scene->settings.lights) : S.lights_present;
+    d.lights = lights ? P<Light>(S.lights) : nullptr;
+    d.n_lights = lights ? S.n_lights : 0;
+    d.ambient = scene ? scene->ambient_light.color : S.ambient;
+    d.tlas_pairs = P<NodePair>(S.tlas_pairs);
+    d.tlas_leaf_ids = P<u32t>(S.tlas_leaf_ids);
+    d.tlas_root_count = S.tlas_root.child_count;
+    d.tlas_root_first = S.tlas_root.first_child_id;
+    memcpy(d.tlas_root_aabb, &S.tlas_root.aabb, sizeof(d.tlas_root_aabb));
+    d.meshes = P<MeshDev>(S.meshes);
+    d.mesh_pairs = P<NodePair>(S.mesh_pairs);
+    d.tri_hot = P<TriHot>(S.tri_hot);
+    d.tri_full = P<Triangle>(S.tri_full);
+    d.textures = P<TexDev>(S.textures);
+    d.mips = P<MipDev>(S.mips);
+    d.quads = P<TexelQuad>(S.quads);
+    d.emissive_quads = P<u32t>(S.emissive);
+    d.n_emissive = S.n_emissive;
+    d.occluders = P<u32t>(S.occluders);
+    d.n_occluders = S.n_occluders;
+    return d;
+}
+
+int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *viewport, st_render_options *o) {
+    SceneSlot *S = slot_of(ctx, slot);
+    if (!S || !viewport) return ST_ERR_INVALID_ARG;
+    if (!S->allocated || !S->tlas_valid || !S->n_prims) return ST_ERR_NOT_RESIDENT;
+    for (const Primitive &p : S->prims_host)
+        if (p.type == PrimitiveType_Mesh && !S->meshes_valid) return ST_ERR_NOT_RESIDENT;
+    cudaSetDevice(ctx->device);
+    ViewDev v;
+    ST_TRY(make_view(viewport, v));
+    v.primary_tlas = S->n_prims > 64 ? 1 : 0;
+    st_render_options defaults;
+    memset(&defaults, 0, sizeof(defaults));
+    if (!o) o = &defaults;
+    cudaStream_t st = o->stream ? (cudaStream_t)o->stream : ctx->stream;
+    const size_t grid = (size_t)v.grid_w * v.grid_h;
+    const u32t W = v.grid_w - 1, H = v.grid_h - 1;
+    ST_TRY(reserve(ctx, ctx->ssb, sizeof(int4) * std::max(S->n_prims, 1u)));
+    ST_TRY(reserve(ctx, ctx->dirs, sizeof(float) * 3 * grid));
+    FloatPixel *host_float = o->out_float ? o->out_float : viewport->frame_buffer->float_pixels;
+    Pixel *host_u8 = o->out_u8 ? o->out_u8 : viewport->frame_buffer->pixels;
+    FloatPixel *dev_float;
+    uint32_t *dev_u8 = nullptr;
+    u32t *dev_ids = nullptr;
+    if (o->device_outputs) {
+        dev_float = o->out_float;
+        dev_u8 = reinterpret_cast<uint32_t *>(o->out_u8);
+        dev_ids = o->out_prim_id;
+        if (!dev_float) {
+            ST_TRY(reserve(ctx, ctx->out_float, sizeof(FloatPixel) * grid));
+            dev_float = P<FloatPixel>(ctx->out_float);
+        }
+    } else {
+        ST_TRY(reserve(ctx, ctx->out_float, sizeof(FloatPixel) * grid));
+        dev_float = P<FloatPixel>(ctx->out_float);
+        if (host_u8) {
+            ST_TRY(reserve(ctx, ctx->out_u8, sizeof(uint32_t) * (size_t)W * H));
+            dev_u8 = P<uint32_t>(ctx->out_u8);
+        }
+        if (o->out_prim_id) {
+            ST_TRY(reserve(ctx, ctx->prim_ids, sizeof(u32t) * grid));
+            dev_ids = P<u32t>(ctx->prim_ids);
+        }
+    }
+    SceneDev sd = scene_view(*S, scene);
+    ST_CUDA(cudaMemsetAsync(ctx->status.ptr, 0, 16, st));
+    if (o->count_work) ST_CUDA(cudaMemsetAsync(ctx->counters.ptr, 0, sizeof(unsigned long long) * 16, st));
+    ST_CUDA(cudaEventRecord(ctx->ev[0], st));
+    launch_ssb(sd, v, P<int4>(ctx->ssb), st);
+    launch_ray_rows(v, P<float>(ctx->dirs), st);
+    ST_CUDA(cudaEventRecord(ctx->ev[1], st));
+    launch_trace(sd, v, P<int4>(ctx->ssb), P<float>(ctx->dirs), dev_float, dev_ids, P<unsigned>(ctx->status),
+                 P<unsigned long long>(ctx->counters), o->count_work != 0, st);
+    ST_CUDA(cudaGetLastError());
+    ST_CUDA(cudaEventRecord(ctx->ev[2], st));
+    if (dev_u8) launch_resolve(dev_float, v.grid_w, W, H, dev_u8, st);
+    ST_CUDA(cudaEventRecord(ctx->ev[3], st));
+    if (!o->device_outputs) {
+        if (host_float && !o->skip_float_copy)
+            ST_CUDA(cudaMemcpyAsync(host_float, dev_float, sizeof(FloatPixel) * grid, cudaMemcpyDeviceToHost, st));
+        if (host_u8 && dev_u8)
+            ST_CUDA(cudaMemcpyAsync(host_u8, dev_u8, sizeof(uint32_t) * (size_t)W * H, cudaMemcpyDeviceToHost, st));
+        if (o->out_prim_id)
+            ST_CUDA(cudaMemcpyAsync(o->out_prim_id, dev_ids, sizeof(u32t) * grid, cudaMemcpyDeviceToHost, st));
+    }
+    unsigned status[4] = {0, 0, 0, 0};
+    ST_CUDA(cudaMemcpyAsync(status, ctx->status.ptr, 16, cudaMemcpyDeviceToHost, st));
+    if (o->count_work) {
+        unsigned long long c[16];
+        ST_CUDA(cudaMemcpyAsync(c, ctx->counters.ptr, sizeof(c), cudaMemcpyDeviceToHost, st));
+        ST_CUDA(cudaStreamSynchronize(st));
+        for (int k = 0; k < 16; k++) o->counters[k] = k < C_COUNT ? c[k] : 0;
+    }
+    ST_CUDA(cudaStreamSynchronize(st));
+    cudaEventElapsedTime(&o->trace_ms, ctx->ev[1], ctx->ev[2]);
+    cudaEventElapsedTime(&o->total_ms, ctx->ev[0], ctx->ev[3]);
+    if (status[0] & S_STACK_OVERFLOW) return ST_ERR_STACK_OVERFLOW;
+    return ST_OK;
+}
+
+int st_render_scene(st_ctx *ctx, int slot, const Scene *scene, Viewport *viewport) {
+    if (!viewport || !viewport->frame_buffer) return ST_ERR_INVALID_ARG;
+    st_render_options o;
+    memset(&o, 0, sizeof(o));
+    return st_render_ex(ctx, slot, scene, viewport, &o);
+}
+
+}  // extern "C"

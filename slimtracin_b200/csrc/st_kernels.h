@@ -1,0 +1,72 @@
+// st_kernels.h — host-visible kernel launchers and the per-view parameter block.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "st_device.cuh"
+
+namespace st {
+
+// One view: what rayTrace / renderSceneOnCPU read from the Viewport and its Camera
+// (raytracer.h:136-170) and what computeSSB reads from the frame buffer's Dimensions (SSB.h:5).
+struct ViewDev {
+    v3 cam_pos;
+    q4 cam_rot_inv;                 // camera->transform.rotation_inverted
+    float cam_rot_matrix_inv[9];    // camera->transform.rotation_matrix_inverted (SSB.h:143)
+    float focal_length;
+    v3 pp_start, pp_right, pp_down; // viewport->projection_plane
+    float cone_angle;
+    u32t grid_w, grid_h;            // QCAA grid (W+1)x(H+1)
+    float f_width, f_height, h_width, h_height, width_over_height, height_over_width;
+    int mode;                       // enum RenderMode
+    u32t depth;                     // trace.depth (bounces)
+    int primary_tlas;               // 1: primary rays walk the TLAS (with the SSB cull); 0: brute force
+};
+
+void launch_ssb(const SceneDev &S, const ViewDev &v, int4 *ssb, cudaStream_t st);
+void launch_ray_rows(const ViewDev &v, float *dirs, cudaStream_t st);
+void launch_trace(const SceneDev &S, const ViewDev &v, const int4 *ssb, const float *dirs, FloatPixel *out,
+                  u32t *prim_ids, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st);
+void launch_resolve(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out, cudaStream_t st);
+
+// ---- BVH builds (st_bvh.cu) ----
+// Device scratch the LBVH build needs for n items (allocated once per context and grown).
+struct LbvhScratch {
+    u32t capacity = 0;
+    float *aabbs = nullptr;          // 6 floats per item (world boxes)
+    unsigned *bounds = nullptr;      // 6 ordered-bit words: scene min.xyz, max.xyz
+    u32t *codes = nullptr, *codes_alt = nullptr;
+    u32t *order = nullptr, *order_alt = nullptr;
+    u32t *hist = nullptr;            // 256 * blocks
+    u32t *first = nullptr, *last = nullptr, *lchild = nullptr, *rchild = nullptr, *parent = nullptr;
+    u32t *leaf_parent = nullptr, *rank = nullptr, *flags = nullptr;
+    unsigned *kbox = nullptr;        // 6 ordered-bit words per internal node
+    u32t *info = nullptr;            // node_count, height
+};
+
+cudaError_t lbvh_reserve(LbvhScratch &s, u32t n);
+void lbvh_release(LbvhScratch &s);
+// Items' world boxes -> Morton codes -> stable radix sort -> Karras tree -> leaf collapse ->
+// reference-layout BVHNode array (1 + 2*kept nodes) + leaf order.  Synchronous w.r.t. `st`.
+// out_nodes must hold 2n nodes; out_order n ids.  info (host) receives node_count, height.
+cudaError_t lbvh_build(LbvhScratch &s, u32t n, u32t max_leaf, BVHNode *out_nodes, u32t *out_order,
+                       u32t info[2], cudaStream_t st);
+// World boxes of primitives as updateSceneBVH computes them (builder_top_down.h:370-377).
+void launch_prim_aabbs(const Primitive *prims, const MeshDev *meshes, u32t n, float *aabbs, cudaStream_t st);
+// Triangle boxes with the reference's EPS padding (builder_top_down.h:283-318).
+void launch_tri_aabbs(const vec3 *pos, const uint32_t *idx, u32t n, float *aabbs, cudaStream_t st);
+// The Triangle record of updateMeshBVH (builder_top_down.h:330-363) for every leaf-ordered slot.
+void launch_tri_records(const vec3 *pos, const vec3 *nrm, const vec2 *uv, const uint32_t *pidx, const uint32_t *nidx,
+                        const uint32_t *uidx, int has_uvs, const u32t *order, u32t n, Triangle *out,
+                        u32t *inverse, cudaStream_t st);
+// Refit: recompute every node box of a reference-layout BVH whose items' boxes are `aabbs`
+// (leaf ranges index `leaf_ids`), bottom-up.
+cudaError_t refit_bvh(BVHNode *nodes, u32t node_count, const u32t *leaf_ids, const float *aabbs,
+                      u32t *scratch_parent, u32t *scratch_flags, unsigned *scratch_box, cudaStream_t st);
+// Reference-layout BVHNode array -> child-pair array (pair k = nodes 1+2k, 2+2k).
+void launch_make_pairs(const BVHNode *nodes, u32t node_count, NodePair *pairs, cudaStream_t st);
+// Triangle -> TriHot
+void launch_make_trihot(const Triangle *tris, u32t n, TriHot *hot, cudaStream_t st);
+// Primitive -> PrimDev
+void launch_make_primdev(const Primitive *prims, u32t n, PrimDev *out, cudaStream_t st);
+
+}  // namespace st

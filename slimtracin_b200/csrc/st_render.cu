@@ -1,0 +1,704 @@
+// st_render.cu — the per-frame kernels: screen-space bounds, ray-direction rows, the trace+shade
+// megakernel and the QCAA resolve.
+#include <cstdio>
+#include "st_trace.cuh"
+#include "st_kernels.h"
+
+namespace st {
+
+// ---- triangles and the BLAS walk: intersection/mesh.h ----------------------------------------
+template <bool CNT>
+__device__ bool hit_triangles(TState<CNT> &t, const SceneDev &S, u32t base, u32t n, bool any_hit) {   // mesh.h:5
+    const RayD &ray = t.local;
+    Hit &hit = t.current;
+    Hit &closest = t.mesh_closest;
+    bool found = false;
+    for (u32t i = 0; i < n; i++) {
+        const TriHot T = S.tri_hot[base + i];
+        t.count(C_TRI);
+        v3 pos = V(T.p.x, T.p.y, T.p.z), nrm = V(T.p.w, T.q.x, T.q.y);
+        if (hit_plane(pos, nrm, ray.origin, ray.direction, hit) && hit.distance < closest.distance) {
+            const float m[9] = {T.q.z, T.q.w, T.r.x, T.r.y, T.r.z, T.r.w, T.s.x, T.s.y, T.s.z};
+            v3 UV = vmat3(hit.position - pos, m);
+            if (UV.x < 0 || UV.y < 0 || (UV.x + UV.y) > 1) continue;
+            closest.NdotV = hit.NdotV;
+            closest.normal = hit.normal;
+            closest.u = UV.x;
+            closest.v = UV.y;
+            closest.object_id = i;
+            closest.from_behind = hit.from_behind;
+            closest.distance = hit.distance;
+            closest.position = hit.position;
+            const float2 areas = __ldg(reinterpret_cast<const float2 *>(&S.tri_full[base + i].area_of_parallelogram));
+            closest.area = areas.x;
+            closest.uv_area = areas.y;
+            found = true;
+            if (any_hit) break;
+        }
+    }
+    return found;
+}
+
+__device__ __forceinline__ NodePair load_pair(const NodePair *p) {
+    NodePair r;
+    const float4 *f = reinterpret_cast<const float4 *>(p);
+    r.a = __ldg(f);
+    r.b = __ldg(f + 1);
+    r.c = __ldg(f + 2);
+    r.d = __ldg(reinterpret_cast<const uint4 *>(f + 3));
+    return r;
+}
+
+template <bool CNT>
+__device__ bool trace_mesh(TState<CNT> &t, const SceneDev &S, const MeshDev &M, bool any_hit) {   // mesh.h:38
+    const RayD &ray = t.local;
+    Hit &closest = t.mesh_closest;
+    float ld, rd;
+    t.count(C_MESH);
+    t.count(C_AABB);
+    if (!hit_aabb(V(M.aabb[0], M.aabb[1], M.aabb[2]), V(M.aabb[3], M.aabb[4], M.aabb[5]), ray, closest.distance, ld))
+        return false;
+    if (M.root_count) return hit_triangles(t, S, M.tri_offset, M.triangle_count, any_hit);
+    const NodePair *pairs = S.mesh_pairs + M.pair_offset;
+    u32t pair = (M.root_first - 1) >> 1;
+    u32t sp = 0;
+    bool found = false;
+    for (;;) {
+        const NodePair P = load_pair(pairs + pair);
+        t.count(C_AABB, 2);
+        bool hl = hit_aabb(V(P.a.x, P.a.y, P.a.z), V(P.a.w, P.b.x, P.b.y), ray, closest.distance, ld);
+        bool hr = hit_aabb(V(P.b.z, P.b.w, P.c.x), V(P.c.y, P.c.z, P.c.w), ray, closest.distance, rd);
+        bool lgo = hl, rgo = hr;
+        if (hl && P.d.y) {
+            if (hit_triangles(t, S, M.tri_offset + P.d.x, P.d.y, any_hit)) {
+                closest.object_id += P.d.x;
+                found = true;
+                if (any_hit) break;
+            }
+            lgo = false;
+        }
+        if (hr && P.d.w) {
+            if (hit_triangles(t, S, M.tri_offset + P.d.z, P.d.w, any_hit)) {
+                closest.object_id += P.d.z;
+                found = true;
+                if (any_hit) break;
+            }
+            rgo = false;
+        }
+        if (lgo) {
+            u32t near_pair = P.d.x, far_pair = P.d.z;
+            if (rgo) {
+                if (!any_hit && ld > rd) { near_pair = P.d.z; far_pair = P.d.x; }
+                if (sp >= kStack) { t.status |= S_STACK_OVERFLOW; return false; }
+                t.stack[sp++] = far_pair;
+            }
+            pair = near_pair;
+        } else if (rgo) {
+            pair = P.d.z;
+        } else {
+            if (sp == 0) break;
+            pair = t.stack[--sp];
+        }
+    }
+    return found;
+}
+
+// ---- hitPrimitives intersection/primitives.h:9 ----------------------------------------------------
+// ids == nullptr: the candidates are primitives first..first+count-1 in index order.
+template <bool CNT>
+__device__ bool hit_primitives(TState<CNT> &t, const SceneDev &S, const RayD &ray, const u32t *ids, u32t first,
+                               u32t count, bool any_hit, const int4 *ssb, int x, int y, float cone_angle) {
+    Hit &hit = t.current, &closest = t.closest;
+    bool found = false;
+    u32t hid = 0;
+    for (u32t i = 0; i < count; i++) {
+        t.count(C_LEAF);
+        const u32t pid = ids ? __ldg(ids + first + i) : first + i;
+        if (ssb) {  // primary rays: IS_VISIBLE and the screen-space rect, folded into one rect per view
+            const int4 b = __ldg(ssb + pid);
+            if (x < b.x || x >= b.z || y < b.y || y >= b.w) continue;
+        }
+        const PrimDev P = S.prims[pid];
+        const unsigned flags = prim_flags(P);
+        if (any_hit && !(flags & IS_SHADOWING)) continue;
+        t.count(C_PRIM);
+        to_object(ray.origin, ray.direction, P, t.local.origin, t.local.direction);
+        t.local.origin = vsfma(t.local.direction, kTraceOffset, t.local.origin);
+        bool cur;
+        switch (prim_type(P)) {
+            case PrimitiveType_Quad: cur = hit_quad(hit, t.local.origin, t.local.direction, flags); break;
+            case PrimitiveType_Box: cur = hit_box(hit, t.local.origin, t.local.direction, flags); break;
+            case PrimitiveType_Sphere: cur = hit_sphere(hit, t.local.origin, t.local.direction, flags); break;
+            case PrimitiveType_Tetrahedron: cur = hit_tetra(hit, t.local.origin, t.local.direction, flags); break;
+            case PrimitiveType_Mesh: {
+                t.local.rcp = rcp(t.local.direction);
+                t.mesh_closest.distance = closest.distance == INFINITY ? INFINITY :
+                    len(pos_to_object(closest.position, P) - t.local.origin);
+                pre_prep(t.local);
+                const MeshDev M = S.meshes[__float_as_uint(P.scale_id.w)];
+                cur = trace_mesh(t, S, M, any_hit);
+                if (cur) hit = t.mesh_closest;
+            } break;
+            default: continue;
+        }
+        if (cur) {
+            hit.position = pos_to_world(hit.position, P);
+            hit.distance_squared = sqlen(hit.position - ray.origin);
+            if (hit.distance_squared < closest.distance_squared) {
+                closest = hit;
+                hid = pid;
+                closest.object_type = prim_type(P);
+                closest.material_id = prim_material(P);
+                found = true;
+                if (any_hit) break;
+            }
+        }
+    }
+    if (found) {
+        const PrimDev HP = S.prims[hid];
+        if (closest.object_type == PrimitiveType_Mesh) {
+            const MeshDev M = S.meshes[__float_as_uint(HP.scale_id.w)];
+            if (M.normals_count | M.uvs_count) {
+                const Triangle &T = S.tri_full[M.tri_offset + closest.object_id];
+                float u = closest.u, v = closest.v;
+                float w = 1 - u - v;
+                if (M.uvs_count) {
+                    closest.u = T.uvs[2].x * u + (T.uvs[1].x * v + T.uvs[0].x * w);
+                    closest.v = T.uvs[2].y * u + (T.uvs[1].y * v + T.uvs[0].y * w);
+                }
+                if (M.normals_count) {
+                    const vec3 *vn = T.vertex_normals;
+                    closest.normal.x = vn[2].x * u + (vn[1].x * v + vn[0].x * w);
+                    closest.normal.y = vn[2].y * u + (vn[1].y * v + vn[0].y * w);
+                    closest.normal.z = vn[2].z * u + (vn[1].z * v + vn[0].z * w);
+                    closest.normal = norm(closest.normal);
+                }
+            }
+        }
+        closest.object_id = hid;
+        closest.normal = norm(dir_to_world(closest.normal, HP));
+        closest.distance = sqrtf(closest.distance_squared);
+        closest.cone_width = 2.0f * cone_angle * closest.distance;
+        v3 rs = qrot(V(HP.scale_id.x, HP.scale_id.y, HP.scale_id.z), prim_rot(HP));
+        closest.area *= dot(one_minus(closest.normal), rs);
+    }
+    return found;
+}
+
+// ---- traceScene shaders/trace.h:8 (TLAS walk); with ssb != null it also serves primary rays ----
+template <bool CNT>
+__device__ bool trace_scene(TState<CNT> &t, const SceneDev &S, RayD &ray, bool any_hit, const int4 *ssb, int x,
+                            int y, float cone_angle, bool prepped) {
+    if (!prepped) {
+        ray.rcp = rcp(ray.direction);
+        pre_prep(ray);
+    }
+    float ld, rd;
+    t.count(C_AABB);
+    if (!hit_aabb(V(S.tlas_root_aabb[0], S.tlas_root_aabb[1], S.tlas_root_aabb[2]),
+                  V(S.tlas_root_aabb[3], S.tlas_root_aabb[4], S.tlas_root_aabb[5]), ray, t.closest.distance, ld))
+        return false;
+    if (S.tlas_root_count)
+        return hit_primitives(t, S, ray, S.tlas_leaf_ids, 0, S.n_prims, any_hit, ssb, x, y, cone_angle);
+    u32t pair = (S.tlas_root_first - 1) >> 1;
+    u32t sp = 0;
+    bool found = false;
+    for (;;) {
+        const NodePair P = load_pair(S.tlas_pairs + pair);
+        t.count(C_AABB, 2);
+        bool hl = hit_aabb(V(P.a.x, P.a.y, P.a.z), V(P.a.w, P.b.x, P.b.y), ray, t.closest.distance, ld);
+        bool hr = hit_aabb(V(P.b.z, P.b.w, P.c.x), V(P.c.y, P.c.z, P.c.w), ray, t.closest.distance, rd);
+        bool lgo = hl, rgo = hr;
+        if (hl && P.d.y) {
+            if (hit_primitives(t, S, ray, S.tlas_leaf_ids, P.d.x, P.d.y, any_hit, ssb, x, y, cone_angle)) {
+                found = true;
+                if (any_hit) break;
+            }
+            lgo = false;
+        }
+        if (hr && P.d.w) {
+            if (hit_primitives(t, S, ray, S.tlas_leaf_ids, P.d.z, P.d.w, any_hit, ssb, x, y, cone_angle)) {
+                found = true;
+                if (any_hit) break;
+            }
+            rgo = false;
+        }
+        if (lgo) {
+            u32t near_pair = P.d.x, far_pair = P.d.z;
+            if (rgo) {
+                if (!any_hit && ld > rd) { near_pair = P.d.z; far_pair = P.d.x; }
+                if (sp >= kStack) { t.status |= S_STACK_OVERFLOW; return found; }
+                t.stack[sp++] = far_pair;
+            }
+            pair = near_pair;
+        } else if (rgo) {
+            pair = P.d.z;
+        } else {
+            if (sp == 0) break;
+            pair = t.stack[--sp];
+        }
+    }
+    return found;
+}
+
+// ---- closest_hit/surface.h, lights.h ------------------------------------------------------------
+template <bool CNT>
+__device__ v3 shade_from_lights(TState<CNT> &t, const SceneDev &S, Shaded &s, RayD &ray, v3 color) {   // surface.h:9
+    Hit &hit = t.closest;
+    for (u32t i = 0; i < S.n_lights; i++) {
+        const Light &light = S.lights[i];
+        hit.position = from(light.position_or_direction);
+        s.light_direction = hit.position - s.position;
+        hit.distance_squared = sqlen(s.light_direction);
+        hit.distance = sqrtf(hit.distance_squared);
+        s.light_direction = vscale(s.light_direction, 1.0f / hit.distance);
+        float NdotL = dot(s.normal, s.light_direction);
+        if (NdotL <= 0) continue;
+        float li = light.intensity / hit.distance_squared;
+        ray.origin = s.position;
+        ray.direction = s.light_direction;
+        t.count(C_SHADOW);
+        if (trace_scene(t, S, ray, true, nullptr, 0, 0, 0.0f, false)) continue;       // inShadow trace.h:85
+        color = vvfma(shade_point(s, NdotL), vscale(from(light.color), li), color);
+    }
+    return color;
+}
+
+template <bool CNT>
+__device__ bool shade_from_emissive_quads(TState<CNT> &t, const SceneDev &S, Shaded &s, RayD &ray, v3 &color) {  // surface.h:37
+    Hit &hit = t.current;
+    bool found = false;
+    for (u32t e = 0; e < S.n_emissive; e++) {
+        const u32t qi = S.emissive_quads[e];
+        const PrimDev Q = S.prims[qi];
+        const Primitive &quad = S.prims_raw[qi];
+        const Material &em = S.materials[prim_material(Q)];
+        v3 Ro, Rd;
+        to_object(s.viewing_origin, s.viewing_direction, Q, Ro, Rd);
+        if (hit_quad(hit, Ro, Rd, prim_flags(Q))) {
+            hit.position = pos_to_world(hit.position, Q);
+            hit.distance_squared = sqlen(hit.position - s.viewing_origin);
+            if (hit.distance_squared < t.closest.distance_squared) {
+                hit.object_id = qi;
+                hit.object_type = PrimitiveType_Quad;
+                hit.material_id = prim_material(Q);
+                t.closest = hit;
+                found = true;
+            }
+        }
+        v3 qn = qrot(V(0, 1, 0), prim_rot(Q));
+        v3 qpos = V(Q.pos_bits.x, Q.pos_bits.y, Q.pos_bits.z);
+        s.light_direction = ray.direction = qpos - s.position;
+        if (dot(qn, s.light_direction) >= 0) continue;
+        float ei = dot(s.normal, area_light_vector(quad, s.position, s.quad_vertices));
+        if (ei > 0) {
+            bool skip = true;
+            for (int j = 0; j < 4; j++)
+                if (dot(s.normal, s.quad_vertices[j] - s.position) >= 0) { skip = false; break; }
+            if (skip) continue;
+            float shaded_light = 1;
+            if (qi != s.prim_index) {
+                for (u32t k = 0; k < S.n_occluders; k++) {
+                    const u32t oi = S.occluders[k];
+                    const PrimDev O = S.prims[oi];
+                    if (oi == qi || dot(qn, V(O.pos_bits.x, O.pos_bits.y, O.pos_bits.z) - qpos) <= 0) continue;
+                    v3 oRo, oRd;
+                    to_object(s.position, s.light_direction, O, oRo, oRd);
+                    oRo = vsfma(oRd, kTraceOffset, oRo);
+                    float d = 1;
+                    if (prim_type(O) == PrimitiveType_Sphere) {
+                        if (hit_sphere(hit, oRo, oRd, prim_flags(O)))
+                            d -= (1.0f - sqrtf(hit.distance_squared)) / (hit.distance * ei * 3);
+                    } else {
+                        if (hit_quad(hit, oRo, oRd, prim_flags(O))) {
+                            hit.position.y = 0;
+                            hit.position.x = hit.position.x < 0 ? -hit.position.x : hit.position.x;
+                            hit.position.z = hit.position.z < 0 ? -hit.position.z : hit.position.z;
+                            if (hit.position.x > hit.position.z) {
+                                hit.position.y = hit.position.z;
+                                hit.position.z = hit.position.x;
+                                hit.position.x = hit.position.y;
+                                hit.position.y = 0;
+                            }
+                            d -= (1.0f - hit.position.z) / (hit.distance * ei);
+                        }
+                    }
+                    if (d < shaded_light) shaded_light = d;
+                }
+            }
+            if (shaded_light > 0) {
+                float NdotL = dot01(s.normal, s.light_direction);
+                if (NdotL) color = vvfma(shade_point(s, NdotL), vscale(from(em.emission), ei * shaded_light), color);
+            }
+        }
+    }
+    if (found) t.closest.distance = sqrtf(t.closest.distance_squared);
+    return found;
+}
+
+__device__ __forceinline__ float volume_density(const SphereHitD &h) {   // lights.h:7
+    float t1 = h.t_near > 0 ? h.t_near : 0;
+    float t2 = h.t_far < h.furthest ? h.t_far : h.furthest;
+    return (h.c * t1 - h.b * t1 * t1 + t1 * t1 * t1 / 3.0f - (
+            h.c * t2 - h.b * t2 * t2 + t2 * t2 * t2 / 3.0f)) * (3.0f / 4.0f);
+}
+template <bool CNT>
+__device__ bool shade_lights(TState<CNT> &t, const SceneDev &S, v3 Ro, v3 Rd, float max_distance, v3 &color) {  // lights.h:17
+    bool hit_light = false;
+    SphereHitD &sh = t.sphere;
+    sh.closest_distance = INFINITY;
+    for (u32t i = 0; i < S.n_lights; i++) {
+        const Light &light = S.lights[i];
+        float size = light.intensity * (1.0f / 16.0f);
+        float oor = 8.0f / size;
+        sh.furthest = max_distance * oor;
+        if (hit_sphere_simple(Ro, Rd, from(light.position_or_direction), oor, sh)) {
+            float distance = sh.t_far - size * 8;
+            float density = powf(volume_density(sh), 8) * 8;
+            if (distance < sh.closest_distance) sh.closest_distance = distance;
+            color = vsfma(from(light.color), density, color);
+            hit_light = true;
+        }
+    }
+    return hit_light;
+}
+
+template <bool CNT>
+__device__ __forceinline__ void apply_textures(TState<CNT> &t, const SceneDev &S, Shaded &s, Hit &hit, const Material &M,
+                                               float &du, float &dv, bool first) {
+    s.u = hit.u * M.uv_repeat.x;
+    s.v = hit.v * M.uv_repeat.y;
+    hit.uv_area /= M.uv_repeat.x / M.uv_repeat.y;
+    float d = duv_ray_cone(hit.NdotV, hit.cone_width, hit.area, hit.uv_area);
+    du = d;
+    if (first) dv = d;              // surface.h:162 sets u and v; the bounce path (:230) only u
+    if (M.use & ALBEDO_MAP) s.albedo = sample_texture(t, S, M.texture_ids[0], s.u, s.v, du, dv);
+    if ((M.use & NORMAL_MAP) && M.texture_count > 1) {
+        q4 rot = normal_rotation(sample_normal(t, S, M.texture_ids[1], s.u, s.v, du, dv));
+        hit.normal = qrot(hit.normal, rot);
+    }
+}
+
+template <bool CNT>
+__device__ v3 shade_surface(TState<CNT> &t, const SceneDev &S, RayD &ray, bool &lights_shaded) {   // surface.h:146
+    Hit &hit = t.closest;
+    v3 color = splat(0);
+    const Material *M = S.materials + hit.material_id;
+    t.count(C_SHADE);
+    if (M->is & EMISSIVE) return hit.from_behind ? color : from(M->emission);
+    float du = 0, dv = 0;
+    Shaded s;
+    s.viewing_origin = ray.origin;
+    s.viewing_direction = ray.direction;
+    s.prim_index = hit.object_id;
+    s.material = M;
+    s.albedo = from(M->albedo);
+    s.reflected_direction = splat(0);
+    if (M->use && M->texture_count) apply_textures(t, S, s, hit, *M, du, dv, true);
+    float NdotRd = 0, ior, max_distance = hit.distance;
+    v3 throughput = splat(1);
+    u32t depth = t.depth;
+    while (depth) {
+        s.position = ray.origin = hit.position;
+        s.normal = hit.from_behind ? neg(hit.normal) : hit.normal;
+        ior = hit.from_behind ? s.material->n2_over_n1 : s.material->n1_over_n2;
+        bool is_ref = (M->is & REFLECTIVE) || (M->is & REFRACTIVE);
+        if (is_ref || M->brdf == BRDF_Phong) {
+            NdotRd = -clamp01(-dot(s.normal, s.viewing_direction));      // invDotVec3 common.h:97
+            s.reflected_direction = vsfma(s.normal, -2.0f * NdotRd, s.viewing_direction);  // reflectWithDot :101
+        }
+        v3 current = is_ref ? splat(0) : from(S.ambient);
+        if (S.lights) current = shade_from_lights(t, S, s, ray, current);
+        if (S.n_emissive)
+            if (shade_from_emissive_quads(t, S, s, ray, current)) max_distance = hit.distance;
+        color = vvfma(current, throughput, color);
+        if (S.lights && shade_lights(t, S, s.viewing_origin, s.viewing_direction, max_distance, color))
+            lights_shaded = true;
+        if (is_ref && --depth) {
+            if (M->is & REFLECTIVE) ray.direction = s.reflected_direction;
+            else {                                                     // refract common.h:105
+                v3 Vv = s.viewing_direction, N = s.normal;
+                float c = ior * ior * (1 - (NdotRd * NdotRd));
+                if (c > 1) ray.direction = splat(0);
+                else {
+                    Vv = vscale(Vv, ior);
+                    Vv = vsfma(N, ior * -NdotRd - sqrtf(1 - c), Vv);
+                    ray.direction = norm(Vv);
+                }
+                if (ray.direction.x == 0 && ray.direction.y == 0 && ray.direction.z == 0)
+                    ray.direction = s.reflected_direction;
+            }
+            t.count(C_BOUNCE);
+            t.closest.distance = t.closest.distance_squared = INFINITY;       // traceRay trace.h:89
+            if (trace_scene(t, S, ray, false, nullptr, 0, 0, 0.0f, false)) {
+                t.count(C_SHADE);
+                s.prim_index = hit.object_id;
+                s.material = M = S.materials + hit.material_id;
+                s.albedo = from(M->albedo);
+                if (M->use && M->texture_count) apply_textures(t, S, s, hit, *M, du, dv, false);
+                if (hit.object_type == PrimitiveType_Quad && (M->is & EMISSIVE)) {
+                    color = hit.from_behind ? splat(0) : from(M->emission);
+                    break;
+                }
+                if (M->brdf != BRDF_CookTorrance) throughput = vmul(throughput, from(M->reflectivity));
+                s.viewing_origin = ray.origin;
+                s.viewing_direction = ray.direction;
+                continue;
+            }
+        }
+        break;
+    }
+    return color;
+}
+
+// ---- the frame kernels -----------------------------------------------------------------------
+// computeSSB render/SSB.h:5 for one primitive; the result is folded with IS_VISIBLE into one rect
+// (an invisible primitive gets an empty rect) so that the primary-ray cull is a single test.
+__device__ bool compute_ssb(int4 &b, v3 pos, float r, float fl, const ViewDev &v) {
+    b.x = v.grid_w + 1; b.z = v.grid_w + 1; b.y = v.grid_h + 1; b.w = v.grid_h + 1;
+    if (pos.z <= -r) return false;
+    float x = pos.x, y = pos.y, z = pos.z, left, right, top, bottom, factor;
+    if (z <= r) {
+        float h = fabsf(z) / fl;
+        top = y + r;
+        bottom = y - r;
+        if (h < bottom || top < -h) return false;
+        float w = h * v.width_over_height;
+        right = x + r;
+        left = x - r;
+        if (w < left || right < -w) return false;
+        b.x = -w < left ? (int)(uint16_t)(v.f_width * (left + w) / (2 * w)) : 0;
+        b.z = right < w ? (int)(uint16_t)(v.f_width * (right + w) / (2 * w)) : (int)v.grid_w;
+        b.y = top < h ? (int)(uint16_t)(v.f_height * (h - top) / (2 * h)) : 0;
+        b.w = -h < bottom ? (int)(uint16_t)(v.f_height * (h - bottom) / (2 * h)) : (int)v.grid_h;
+        return true;
+    }
+    float den = z * z - r * r;
+    factor = fl / den;
+    float yz = y * z;
+    float sqr = y * y + den;
+    sqr = r * sqrtf(sqr);
+    bottom = factor * (yz - sqr);
+    top = factor * (yz + sqr);
+    if (bottom < 1 && top > -1) {
+        factor *= v.height_over_width;
+        float xz = x * z;
+        sqr = r * sqrtf(x * x + den);
+        left = factor * (xz - sqr);
+        right = factor * (xz + sqr);
+        if (left < 1 && right > -1) {
+            bottom = bottom > -1 ? bottom : -1; bottom += 1;
+            top = top < 1 ? top : 1; top += 1;
+            left = left > -1 ? left : -1; left += 1;
+            right = right < 1 ? right : 1; right += 1;
+            top = 2 - top;
+            bottom = 2 - bottom;
+            b.x = (int)(uint16_t)(v.h_width * left);
+            b.z = (int)(uint16_t)(v.h_width * right);
+            b.w = (int)(uint16_t)(v.h_height * bottom);
+            b.y = (int)(uint16_t)(v.h_height * top);
+            return true;
+        }
+    }
+    return false;
+}
+
+// updatePrimitiveSSB render/SSB.h:137 for every primitive of one view
+__global__ void ssb_kernel(SceneDev S, ViewDev v, int4 *ssb) {
+    u32t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.n_prims) return;
+    const Primitive p = S.prims_raw[i];
+    v3 view = vmat3(from(p.position) - v.cam_pos, v.cam_rot_matrix_inv);
+    float radius;
+    v3 sc = from(p.scale);
+    switch (p.type) {
+        case PrimitiveType_Quad: case PrimitiveType_Box: radius = len(sc); break;
+        case PrimitiveType_Tetrahedron: { float m = sc.x; if (sc.y > m) m = sc.y; if (sc.z > m) m = sc.z; radius = m * kSqrt2; } break;
+        case PrimitiveType_Sphere: { float m = sc.x; if (sc.y > m) m = sc.y; if (sc.z > m) m = sc.z; radius = m; } break;
+        case PrimitiveType_Mesh: {
+            const MeshDev &M = S.meshes[p.id];
+            float mn = len(vmul(sc, V(M.mesh_aabb[0], M.mesh_aabb[1], M.mesh_aabb[2])));
+            float mx = len(vmul(sc, V(M.mesh_aabb[3], M.mesh_aabb[4], M.mesh_aabb[5])));
+            radius = mx > mn ? mx : mn;
+        } break;
+        default: {
+            // updatePrimitiveSSB returns without touching other types: keep the uploaded values
+            const bool vis = p.flags & IS_VISIBLE;
+            ssb[i] = vis ? make_int4(p.screen_bounds.min.x, p.screen_bounds.min.y, p.screen_bounds.max.x, p.screen_bounds.max.y)
+                         : make_int4(1, 1, 0, 0);
+            return;
+        }
+    }
+    int4 b;
+    bool vis = compute_ssb(b, view, radius, v.focal_length, v);
+    ssb[i] = vis ? b : make_int4(1, 1, 0, 0);
+}
+
+// The reference walks each row of the QCAA grid by repeated addition (raytracer.h:156-170):
+// row y starts at start + down added y times, pixel x at that plus right added x times.  One lane
+// per row keeps that exact sequence; 32 consecutive values per lane go through shared memory so
+// the stores to the (W+1)x(H+1) grid stay coalesced.
+__global__ void ray_rows_kernel(ViewDev v, float *dirs) {
+    __shared__ float tile[32][32 * 3 + 1];
+    const int lane = threadIdx.x;
+    const u32t row = blockIdx.x * 32 + lane;
+    v3 start = v.pp_start;
+    for (u32t y = 0; y < row && y < v.grid_h; y++) start = start + v.pp_down;
+    v3 cur = start;
+    const u32t rows_here = min(32u, v.grid_h - blockIdx.x * 32);
+    for (u32t x0 = 0; x0 < v.grid_w; x0 += 32) {
+        for (int k = 0; k < 32; k++) {
+            tile[lane][3 * k + 0] = cur.x;
+            tile[lane][3 * k + 1] = cur.y;
+            tile[lane][3 * k + 2] = cur.z;
+            cur = cur + v.pp_right;
+        }
+        __syncwarp();
+        const u32t n = min(32u, v.grid_w - x0);
+        for (u32t r = 0; r < rows_here; r++) {
+            float *dst = dirs + ((size_t)(blockIdx.x * 32 + r) * v.grid_w + x0) * 3;
+            for (u32t k = lane; k < 3 * n; k += 32) dst[k] = tile[r][k];
+        }
+        __syncwarp();
+    }
+}
+
+// rayTrace render/raytracer.h:81 for one QCAA grid point, writing the FloatPixel the reference's
+// setPixel leaves after beginDrawing's clear (viewport.h:88): hit -> (color, 1, z), miss ->
+// (black, 0, +inf).
+template <bool CNT>
+__global__ void __launch_bounds__(128) trace_kernel(SceneDev S, ViewDev v, const int4 *ssb, const float *dirs,
+                                                    FloatPixel *out, u32t *prim_ids, unsigned *status,
+                                                    unsigned long long *counters) {
+    const u32t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // a block covers 16x8 grid points; each warp an 8x4 tile
+    const u32t x = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
+    const u32t y = blockIdx.y * 8 + (warp >> 1) * 4 + (lane >> 3);
+    const bool active = x < v.grid_w && y < v.grid_h;
+    TState<CNT> t;
+    t.status = 0;
+    if (CNT) for (int k = 0; k < C_COUNT; k++) t.cnt[k] = 0;
+    if (active) {
+        const size_t idx = (size_t)y * v.grid_w + x;
+        v3 current = V(dirs[3 * idx], dirs[3 * idx + 1], dirs[3 * idx + 2]);
+        RayD ray;
+        ray.origin = v.cam_pos;
+        ray.direction = norm(current);
+        ray.rcp = rcp(ray.direction);
+        t.depth = v.depth;
+        t.closest.distance = t.closest.distance_squared = INFINITY;
+        t.closest.cone_width = 0;
+        t.mesh_closest.object_type = PrimitiveType_Mesh;
+        t.current.cone_width = 0;
+        t.count(C_PRIMARY);
+        v3 Ro = ray.origin, Rd = ray.direction, color = splat(0);
+        bool lights_shaded = false;
+        bool hit_found;
+        if (v.primary_tlas) {
+            RayD pr = ray;
+            pre_prep(pr);
+            hit_found = trace_scene(t, S, pr, false, ssb, (int)x, (int)y, v.cone_angle, true);
+        } else {
+            hit_found = hit_primitives(t, S, ray, S.tlas_leaf_ids, 0, S.n_prims, false, ssb, (int)x, (int)y, v.cone_angle);
+        }
+        Hit &hit = t.closest;
+        if (prim_ids) prim_ids[idx] = hit_found ? hit.object_id : 0xFFFFFFFFu;
+        float closest_distance = hit_found ? hit.distance : INFINITY;
+        float z = INFINITY;
+        if (hit_found) {
+            z = qrot(hit.position - v.cam_pos, v.cam_rot_inv).z;
+            switch (v.mode) {
+                case RenderMode_Beauty: color = shade_surface(t, S, ray, lights_shaded); break;
+                case RenderMode_Depth: color = splat(4 / hit.distance); break;
+                case RenderMode_Normals: {
+                    const Material &M = S.materials[hit.material_id];
+                    if (M.texture_count > 1 && (M.use & NORMAL_MAP)) {
+                        float u = hit.u * M.uv_repeat.x, vv = hit.v * M.uv_repeat.y;
+                        hit.uv_area /= M.uv_repeat.x / M.uv_repeat.y;
+                        float du = duv_ray_cone(hit.NdotV, hit.cone_width, hit.area, hit.uv_area);
+                        q4 rot = normal_rotation(sample_normal(t, S, M.texture_ids[1], u, vv, du, 0.0f));
+                        hit.normal = qrot(hit.normal, rot);
+                    }
+                    color = V(0.5f * (hit.normal.x + 1), 0.5f * (hit.normal.y + 1), 0.5f * (hit.normal.z + 1));
+                } break;
+                case RenderMode_UVs: color = V(0.5f * hit.u, 0.5f * hit.v, 0.5f); break;
+            }
+        }
+        if (v.mode == RenderMode_Beauty && S.lights && !lights_shaded) {
+            if (shade_lights(t, S, Ro, Rd, closest_distance, color)) {
+                hit_found = true;
+                z = t.sphere.closest_distance;
+            }
+        }
+        float4 c01;
+        double depth;
+        if (hit_found) {
+            if (v.mode == RenderMode_Beauty) {
+                color.x = tone_mapped(color.x);
+                color.y = tone_mapped(color.y);
+                color.z = tone_mapped(color.z);
+            }
+            color = vscale(color, 255.0f);
+            color = vmul(color, color);
+            c01 = make_float4(color.x, color.y, color.z, 1.0f);
+            depth = (double)z;
+        } else {
+            c01 = make_float4(0, 0, 0, 0);
+            depth = (double)INFINITY;
+        }
+        float2 *o = reinterpret_cast<float2 *>(out + idx);
+        o[0] = make_float2(c01.x, c01.y);
+        o[1] = make_float2(c01.z, c01.w);
+        reinterpret_cast<double *>(o)[2] = depth;
+    }
+    if (t.status) atomicOr(status, t.status);
+    if (CNT) {
+        for (int k = 0; k < C_COUNT; k++) {
+            unsigned long long s = t.cnt[k];
+            for (int off = 16; off; off >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, off);
+            if (lane == 0 && s) atomicAdd(counters + k, s);
+        }
+    }
+}
+
+// drawViewportToWindowContent viewport/viewport.h:12 (QCAA branch): the 2x2 corners' colour times
+// opacity, averaged, square-rooted in double, truncated to u8; all-infinite corners -> background.
+__global__ void resolve_kernel(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out) {
+    u32t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= width || y >= height) return;
+    const FloatPixel TL = in[(size_t)y * grid_w + x], TR = in[(size_t)y * grid_w + x + 1];
+    const FloatPixel BL = in[(size_t)(y + 1) * grid_w + x], BR = in[(size_t)(y + 1) * grid_w + x + 1];
+    uint32_t px;
+    if (BL.depth == INFINITY && BR.depth == INFINITY && TL.depth == INFINITY && TR.depth == INFINITY) {
+        px = 0xFF000000u;
+    } else {
+        v3 c = vscale(vsfma(from(TL.color), TL.opacity, vsfma(from(TR.color), TR.opacity,
+                      vsfma(from(BL.color), BL.opacity, vscale(from(BR.color), BR.opacity)))), 0.25f);
+        unsigned R = (unsigned char)(c.x > (255 * 255) ? 255.0 : sqrt((double)c.x));
+        unsigned G = (unsigned char)(c.y > (255 * 255) ? 255.0 : sqrt((double)c.y));
+        unsigned B = (unsigned char)(c.z > (255 * 255) ? 255.0 : sqrt((double)c.z));
+        px = B | (G << 8) | (R << 16) | 0xFF000000u;
+    }
+    out[(size_t)y * width + x] = px;
+}
+
+// ---- launchers -------------------------------------------------------------------------------
+void launch_ssb(const SceneDev &S, const ViewDev &v, int4 *ssb, cudaStream_t st) {
+    if (!S.n_prims) return;
+    ssb_kernel<<<(S.n_prims + 127) / 128, 128, 0, st>>>(S, v, ssb);
+}
+void launch_ray_rows(const ViewDev &v, float *dirs, cudaStream_t st) {
+    ray_rows_kernel<<<(v.grid_h + 31) / 32, 32, 0, st>>>(v, dirs);
+}
+void launch_trace(const SceneDev &S, const ViewDev &v, const int4 *ssb, const float *dirs, FloatPixel *out,
+                  u32t *prim_ids, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st) {
+    dim3 grid((v.grid_w + 15) / 16, (v.grid_h + 7) / 8);
+    if (count) trace_kernel<true><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters);
+    else trace_kernel<false><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters);
+}
+void launch_resolve(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out, cudaStream_t st) {
+    dim3 grid((width + 127) / 128, height);
+    resolve_kernel<<<grid, 128, 0, st>>>(in, grid_w, width, height, out);
+}
+
+}  // namespace st

@@ -1,0 +1,116 @@
+"""Shared test helpers: run the oracle / the reference harness on SceneData and compare frames."""
+import ctypes as C
+
+import numpy as np
+
+import oracle
+from slimtracin_b200 import scenes, structs as S
+
+
+def tlas_sah(sd, which="orc"):
+    """The reference's top-down SAH TLAS (updateSceneBVH) via the oracle or the reference itself."""
+    sc, keep = sd.to_ctypes()
+    if which == "orc":
+        oracle.restatement().orc_update_scene_bvh(C.byref(sc))
+    else:
+        oracle.reference().ref_update_scene_bvh(C.byref(sc))
+    sd.read_back_tlas(sc)
+    return sd
+
+
+def blas_sah(md, which="orc"):
+    """The reference's BLAS build (updateMeshBVH) into md via the oracle or the reference."""
+    keep = []
+    md.allocate_bvh()
+    m = md.to_ctypes(keep)
+    if which == "orc":
+        oracle.restatement().orc_update_mesh_bvh(C.byref(m))
+    else:
+        oracle.reference().ref_update_mesh_bvh(C.byref(m))
+    md.read_back(m)
+    return md
+
+
+def oracle_frame(sd, cam, w, h, depth=2, mode=S.RM_BEAUTY, cone_angle=0.0, threads=8, counters=False):
+    """The oracle's render: SSB update on a copy of the primitives, then the frame."""
+    orc = oracle.restatement()
+    d = sd.copy()
+    sc, keep = d.to_ctypes()
+    fr = scenes.Frame(w, h, cam, depth=depth, mode=mode, cone_angle=cone_angle)
+    orc.orc_update_scene_ssb(C.byref(sc), C.byref(fr.viewport))
+    ids = np.zeros(fr.rays, dtype=np.uint32)
+    cnt = np.zeros(16, dtype=np.uint64)
+    orc.orc_render_frame(C.byref(sc), C.byref(fr.viewport), threads, ids.ctypes.data, cnt.ctypes.data)
+    fr.prim_ids = ids
+    fr.counters = cnt
+    return fr
+
+
+def reference_frame(sd, cam, w, h, depth=2, mode=S.RM_BEAUTY, cone_angle=0.0, threads=8):
+    """The reference's own render of the same scene (updateSceneSSB, beginDrawing, rayTrace per
+    pixel, drawViewportToWindowContent)."""
+    ref = oracle.reference()
+    d = sd.copy()
+    sc, keep = d.to_ctypes()
+    fr = scenes.Frame(w, h, cam, depth=depth, mode=mode, cone_angle=cone_angle)
+    ref.ref_update_scene_ssb(C.byref(sc), C.byref(fr.viewport))
+    ref.ref_begin_drawing(C.byref(fr.viewport))
+    fr.viewport.projection_plane.cone_angle = np.float32(cone_angle)
+    ref.ref_render_rows(C.byref(sc), C.byref(fr.viewport), threads, 0, 1, fr.grid_h)
+    ref.ref_resolve(C.byref(fr.viewport))
+    return fr
+
+
+def gpu_frame(renderer, slot, sd, cam, w, h, depth=2, mode=S.RM_BEAUTY, cone_angle=0.0, counters=False):
+    fr = scenes.Frame(w, h, cam, depth=depth, mode=mode, cone_angle=cone_angle)
+    ids = np.zeros(fr.rays, dtype=np.uint32)
+    opt = renderer.render(slot, sd, fr, prim_ids=ids, count_work=counters)
+    fr.prim_ids = ids
+    fr.options = opt
+    fr.counters = np.array([opt.counters[k] for k in range(16)], dtype=np.uint64)
+    return fr
+
+
+def compare(a, b, mode):
+    """Parity figures of two frames of the same view.
+    exact        fraction of grid points whose FloatPixel bytes are identical
+    id_match     fraction of grid points with the same primary-hit primitive id (when both have ids)
+    u8_within1   fraction of resolved pixels whose RGB differ by at most 1 in every channel
+    max_rel      largest relative difference of sqrt(color) over points both sides hit"""
+    fa, fb = a.float_pixels, b.float_pixels
+    out = {"exact": float((fa.view(np.uint8).reshape(-1, 24) == fb.view(np.uint8).reshape(-1, 24)).all(1).mean())}
+    if getattr(a, "prim_ids", None) is not None and getattr(b, "prim_ids", None) is not None:
+        out["id_match"] = float((a.prim_ids == b.prim_ids).mean())
+    pa = a.pixels.view(np.uint8).reshape(-1, 4)[:, :3].astype(int)
+    pb = b.pixels.view(np.uint8).reshape(-1, 4)[:, :3].astype(int)
+    out["u8_within1"] = float((np.abs(pa - pb).max(1) <= 1).mean())
+    out["u8_max"] = int(np.abs(pa - pb).max()) if len(pa) else 0
+    both = np.isfinite(fa["depth"]) & np.isfinite(fb["depth"])
+    ca = np.sqrt(fa["color"][both].astype(np.float64)) / 255.0
+    cb = np.sqrt(fb["color"][both].astype(np.float64)) / 255.0
+    rel = np.abs(ca - cb) / np.maximum(np.abs(ca), 1e-3)
+    out["max_rel"] = float(rel.max()) if rel.size else 0.0
+    out["rel_ok"] = float((rel.max(1) <= 1e-4).mean()) if rel.size else 1.0
+    out["hit_agree"] = float((np.isfinite(fa["depth"]) == np.isfinite(fb["depth"])).mean())
+    return out
+
+
+def assert_parity(m, mode, id_min=0.9999, u8_min=0.999, rel_min=0.999):
+    """The stated tolerances: primary-hit ids on >= 99.99% of grid points, beauty RGB within 1/255
+    on >= 99.9% of pixels, depth/normal/UV within 1e-4 relative on >= 99.9% of hit points."""
+    if "id_match" in m:
+        assert m["id_match"] >= id_min, m
+    if mode == S.RM_BEAUTY:
+        assert m["u8_within1"] >= u8_min, m
+    else:
+        assert m["rel_ok"] >= rel_min, m
+        assert m["u8_within1"] >= u8_min, m
+
+
+def small_config1(subdivisions=3, texture_size=64, blas="orc"):
+    """config1 at test scale: a small displaced icosphere, 64^2 textures, the same 8 instances,
+    materials and emissive quads."""
+    sd, cam = scenes.config1(subdivisions=subdivisions, texture_size=texture_size)
+    if blas in ("orc", "ref"):
+        blas_sah(sd.meshes[0], blas)
+    return sd, cam

@@ -1,0 +1,181 @@
+"""Device path vs the oracle, called through the C ABI (libslimtracin_b200.so)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+from slimtracin_b200 import api, scenes, structs as S
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+MODES = [S.RM_BEAUTY, S.RM_DEPTH, S.RM_NORMALS, S.RM_UVS]
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_config0_all_modes(renderer, mode):
+    sd, cam = scenes.config0()
+    H.tlas_sah(sd)
+    renderer.upload(0, sd, tlas="host")
+    g = H.gpu_frame(renderer, 0, sd, cam, 640, 480, depth=2, mode=mode)
+    o = H.oracle_frame(sd, cam, 640, 480, depth=2, mode=mode)
+    m = H.compare(g, o, mode)
+    print("config0", mode, m)
+    H.assert_parity(m, mode)
+    assert m["exact"] > 0.999, m
+
+
+@pytest.mark.parametrize("depth", [1, 3])
+def test_point_and_area_lights(renderer, depth):
+    """06_AreaLights: point lights and emissive quads together, so the shadow rays' overwrite of the
+    closest hit reaches the emissive-quad test (surface.h:14-17,55)."""
+    sd, cam = scenes.example_area_lights()
+    H.tlas_sah(sd)
+    renderer.upload(1, sd, tlas="host")
+    g = H.gpu_frame(renderer, 1, sd, cam, 320, 240, depth=depth)
+    o = H.oracle_frame(sd, cam, 320, 240, depth=depth)
+    m = H.compare(g, o, S.RM_BEAUTY)
+    print("area", depth, m)
+    H.assert_parity(m, S.RM_BEAUTY)
+
+
+@pytest.mark.parametrize("mode", [S.RM_BEAUTY, S.RM_NORMALS, S.RM_UVS])
+def test_config1_small_reference_blas(renderer, mode):
+    """Meshes, Cook-Torrance, glass and mirror bounces, textures, emissive quads, BLAS from the
+    reference's SAH builder."""
+    sd, cam = H.small_config1(subdivisions=3, texture_size=64, blas="orc")
+    H.tlas_sah(sd)
+    renderer.upload(2, sd, tlas="host")
+    g = H.gpu_frame(renderer, 2, sd, cam, 320, 180, depth=4, mode=mode)
+    o = H.oracle_frame(sd, cam, 320, 180, depth=4, mode=mode)
+    m = H.compare(g, o, mode)
+    print("config1-small", mode, m)
+    H.assert_parity(m, mode)
+
+
+def test_counters_match_oracle(renderer):
+    """Same traversal, same work: every event counter equals the oracle's."""
+    sd, cam = H.small_config1(subdivisions=2, texture_size=32, blas="orc")
+    H.tlas_sah(sd)
+    renderer.upload(3, sd, tlas="host")
+    g = H.gpu_frame(renderer, 3, sd, cam, 160, 90, depth=4, counters=True)
+    o = H.oracle_frame(sd, cam, 160, 90, depth=4)
+    print("gpu", g.counters[:10], "oracle", o.counters[:10])
+    assert np.array_equal(g.counters[:10], o.counters[:10])
+    sd0, cam0 = scenes.example_area_lights()
+    H.tlas_sah(sd0)
+    renderer.upload(3, sd0, tlas="host")
+    g = H.gpu_frame(renderer, 3, sd0, cam0, 160, 120, depth=2, counters=True)
+    o = H.oracle_frame(sd0, cam0, 160, 120, depth=2)
+    assert np.array_equal(g.counters[:10], o.counters[:10]), (g.counters[:10], o.counters[:10])
+
+
+def test_config2_primary_tlas(renderer):
+    """Hundreds of primitives: primary rays walk the TLAS with the SSB cull instead of the
+    reference's brute-force loop; results must not change."""
+    sd, cam = scenes.config2(count=384, spread=6.0)
+    H.tlas_sah(sd)
+    renderer.upload(4, sd, tlas="host")
+    g = H.gpu_frame(renderer, 4, sd, cam, 320, 180, depth=2)
+    o = H.oracle_frame(sd, cam, 320, 180, depth=2)
+    m = H.compare(g, o, S.RM_BEAUTY)
+    print("config2-384", m)
+    H.assert_parity(m, S.RM_BEAUTY)
+
+
+def test_lbvh_tlas_bit_exact(renderer):
+    """The device LBVH30 TLAS: node array, leaf order and height equal the oracle's specification."""
+    orc = oracle.restatement()
+    for count in (2, 3, 16, 384, 4096):
+        sd, cam = scenes.config2(count=count)
+        renderer.upload(5, sd, tlas=None)
+        renderer.build_tlas(5, sd, api.ST_BVH_LBVH30)
+        sc, keep = sd.to_ctypes()
+        n = count
+        boxes = np.zeros(6 * n, dtype=np.float32)
+        orc.orc_primitive_aabbs(C.byref(sc), boxes.ctypes.data)
+        codes = np.zeros(n, np.uint32)
+        order = np.zeros(n, np.uint32)
+        nodes = np.zeros(2 * n, dtype=S.BVHNODE_DT)
+        leaf = np.zeros(n, np.uint32)
+        info = np.zeros(2, np.uint32)
+        orc.orc_lbvh30(boxes.ctypes.data, n, 2, codes.ctypes.data, order.ctypes.data, nodes.ctypes.data,
+                       leaf.ctypes.data, info.ctypes.data)
+        assert sd.tlas_node_count == info[0] and sd.tlas_height == info[1], (count, sd.tlas_node_count, info)
+        k = int(info[0])
+        assert np.array_equal(sd.tlas_leaf_ids[:n], leaf)
+        assert np.array_equal(sd.tlas_nodes[:k].view(np.uint8), nodes[:k].view(np.uint8)), count
+
+
+def test_render_with_lbvh_tlas(renderer):
+    """Any-hit shadow rays take the first occluder found, so with a different TLAS the oracle is
+    given the same (device-built) TLAS."""
+    sd, cam = scenes.config0()
+    renderer.upload(6, sd, tlas=None)
+    renderer.build_tlas(6, sd, api.ST_BVH_LBVH30)
+    g = H.gpu_frame(renderer, 6, sd, cam, 320, 240, depth=2)
+    o = H.oracle_frame(sd, cam, 320, 240, depth=2)
+    m = H.compare(g, o, S.RM_BEAUTY)
+    H.assert_parity(m, S.RM_BEAUTY)
+
+
+def test_blas_lbvh_triangle_records(renderer):
+    """Device BLAS: every Triangle record equals the reference's precompute of the same source
+    triangle (builder_top_down.h:330-363), and leaf_ids is the inverse of the leaf order."""
+    md = scenes.displaced_icosphere(4, seed=7)
+    renderer.build_blas(md)
+    ref = scenes.displaced_icosphere(4, seed=7)
+    H.blas_sah(ref, "orc")
+    # map each leaf-ordered slot back to its source triangle through leaf_ids (source -> slot)
+    n = md.triangle_count
+    slot_of_src_dev = md.leaf_ids[:n]
+    slot_of_src_ref = ref.leaf_ids[:n]
+    assert np.array_equal(np.sort(slot_of_src_dev), np.arange(n))
+    dev_by_src = md.triangles[slot_of_src_dev]
+    ref_by_src = ref.triangles[slot_of_src_ref]
+    assert np.array_equal(dev_by_src.view(np.uint8), ref_by_src.view(np.uint8))
+    assert md.height + 2 <= 64
+
+
+def test_render_with_lbvh_blas(renderer):
+    sd, cam = H.small_config1(subdivisions=3, texture_size=64, blas=None)
+    renderer.build_blas(sd.meshes[0])
+    H.tlas_sah(sd)
+    renderer.upload(7, sd, tlas="host")
+    g = H.gpu_frame(renderer, 7, sd, cam, 320, 180, depth=4)
+    o = H.oracle_frame(sd, cam, 320, 180, depth=4)
+    m = H.compare(g, o, S.RM_BEAUTY)
+    H.assert_parity(m, S.RM_BEAUTY)
+
+
+def test_refit_after_motion(renderer):
+    sd, cam = scenes.config2(count=256)
+    renderer.upload(8, sd, tlas=None)
+    renderer.build_tlas(8, sd, api.ST_BVH_LBVH30)
+    scenes.advance_config2(sd, 3)
+    renderer.update_primitives(8, sd.primitives, np.arange(256))
+    renderer.build_tlas(8, sd, api.ST_BVH_REFIT)
+    # every leaf box contains its primitives' boxes and every parent contains its children
+    nodes = sd.tlas_nodes[:sd.tlas_node_count]
+    for i, nd in enumerate(nodes):
+        if nd["child_count"] == 0:
+            f = nd["first_child_id"]
+            for c in (f, f + 1):
+                assert np.all(nodes[c]["aabb"][:3] >= nd["aabb"][:3]) and np.all(nodes[c]["aabb"][3:] <= nd["aabb"][3:])
+    g = H.gpu_frame(renderer, 8, sd, cam, 256, 144, depth=2)
+    o = H.oracle_frame(sd, cam, 256, 144, depth=2)
+    H.assert_parity(H.compare(g, o, S.RM_BEAUTY), S.RM_BEAUTY)
+
+
+def test_layout_matches_reference_headers():
+    if not oracle.reference_available():
+        pytest.skip("reference harness not built")
+    L = api.lib()
+    ref = oracle.reference()
+    import re
+    names = re.findall(r"ST_LAYOUT_(?:STRUCT|FIELD)\(([A-Za-z]+)(?:, ([A-Za-z_]+))?\)",
+                       open(H.__file__.replace("tests/helpers.py", "include/slimtracin_layout.h")).read())
+    for s, f in names:
+        q = (s + ("." + f if f else "")).encode()
+        assert L.st_layout_query(q) == ref.ref_layout_query(q), q

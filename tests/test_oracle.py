@@ -1,0 +1,211 @@
+"""The oracle (oracle/oracle.c) pinned against the reference's own code and the golden fixtures."""
+import ctypes as C
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from slimtracin_b200 import scenes, structs as S
+from tests import helpers as H
+from tests.golden import make_golden as G
+
+GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "golden.json")))
+FRAMES = np.load(os.path.join(os.path.dirname(__file__), "golden", "frames.npz"))
+needs_ref = pytest.mark.skipif(not oracle.reference_available(), reason="reference harness not built")
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).view(np.uint8).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN["renders"]))
+def test_oracle_reproduces_golden_renders(name):
+    """Bit-exact: the oracle's float grid hashes to the reference's, and its u8 frame is equal."""
+    g = GOLDEN["renders"][name]
+    sd, cam = G.make_scene(g["kind"], "orc")
+    assert sha(sd.tlas_nodes[:sd.tlas_node_count]) == g["tlas_sha256"]
+    fr = H.oracle_frame(sd, cam, g["w"], g["h"], depth=g["depth"], mode=g["mode"])
+    assert sha(fr.float_pixels) == g["float_sha256"], name
+    rgb = np.stack([fr.pixels["R"], fr.pixels["G"], fr.pixels["B"]], -1).reshape(g["h"], g["w"], 3)
+    assert np.array_equal(rgb, FRAMES[name])
+
+
+@needs_ref
+@pytest.mark.parametrize("case", ["config0", "area", "config1_small", "config2_320"])
+@pytest.mark.parametrize("mode", [S.RM_BEAUTY, S.RM_NORMALS])
+def test_oracle_matches_reference_live(case, mode):
+    """Larger renders than the fixtures, oracle vs the reference run here, every byte equal."""
+    if case == "config0":
+        sd, cam = scenes.config0()
+        w, h, depth = 320, 240, 2
+    elif case == "area":
+        sd, cam = scenes.example_area_lights()
+        w, h, depth = 240, 180, 4
+    elif case == "config1_small":
+        sd, cam = scenes.config1(subdivisions=3, texture_size=64)
+        H.blas_sah(sd.meshes[0], "ref")
+        w, h, depth = 192, 108, 4
+    else:
+        sd, cam = scenes.config2(count=320)
+        w, h, depth = 128, 72, 2
+    H.tlas_sah(sd, "ref")
+    r = H.reference_frame(sd, cam, w, h, depth=depth, mode=mode)
+    o = H.oracle_frame(sd, cam, w, h, depth=depth, mode=mode)
+    assert np.array_equal(r.float_pixels.view(np.uint8), o.float_pixels.view(np.uint8))
+    assert np.array_equal(r.pixels.view(np.uint8).reshape(-1, 4)[:, :3], o.pixels.view(np.uint8).reshape(-1, 4)[:, :3])
+
+
+@pytest.mark.parametrize("kind", sorted(GOLDEN["tlas"]))
+def test_sah_tlas_matches_golden(kind):
+    g = GOLDEN["tlas"][kind]
+    sd, _ = G.make_scene(kind, "orc")
+    assert sd.tlas_node_count == g["node_count"] and sd.tlas_height == g["height"]
+    assert sha(sd.tlas_nodes[:sd.tlas_node_count]) == g["nodes_sha256"]
+    assert sha(sd.tlas_leaf_ids) == g["leaf_ids_sha256"]
+
+
+@needs_ref
+@pytest.mark.parametrize("sub", [2, 3, 4])
+def test_sah_blas_matches_reference(sub):
+    a = H.blas_sah(scenes.displaced_icosphere(sub, seed=11), "orc")
+    b = H.blas_sah(scenes.displaced_icosphere(sub, seed=11), "ref")
+    assert (a.node_count, a.height) == (b.node_count, b.height)
+    assert np.array_equal(a.nodes[:a.node_count].view(np.uint8), b.nodes[:b.node_count].view(np.uint8))
+    assert np.array_equal(a.leaf_ids, b.leaf_ids)
+    assert np.array_equal(a.triangles.view(np.uint8), b.triangles.view(np.uint8))
+
+
+@needs_ref
+def test_monkey_mesh_golden():
+    """The one fixture the reference ships: rebuilding monkey.mesh's BLAS from its own vertex data
+    reproduces the stored nodes, leaf ids and Triangle records byte for byte."""
+    if not os.path.exists(G.MONKEY) or GOLDEN["monkey"] is None:
+        pytest.skip("monkey.mesh not present")
+    ref = oracle.reference()
+    m = S.Mesh()
+    arena = ref.ref_load_mesh(G.MONKEY.encode(), C.byref(m))
+    g = GOLDEN["monkey"]
+    t, v = m.triangle_count, m.vertex_count
+    assert (t, v, m.bvh.node_count, m.bvh.height) == (g["triangles"], g["vertices"], g["node_count"], g["height"])
+
+    def arr(ptr, n, dt, shape):
+        return np.ctypeslib.as_array((C.c_uint8 * (n * np.dtype(dt).itemsize)).from_address(ptr)).view(dt).reshape(shape).copy()
+
+    md = scenes.MeshData(arr(m.vertex_positions, 3 * v, np.float32, (v, 3)),
+                         arr(m.vertex_normals, 3 * m.normals_count, np.float32, (m.normals_count, 3)),
+                         arr(m.vertex_uvs, 2 * m.uvs_count, np.float32, (m.uvs_count, 2)),
+                         arr(m.vertex_position_indices, 3 * t, np.uint32, (t, 3)),
+                         np.array([m.aabb.min.x, m.aabb.min.y, m.aabb.min.z, m.aabb.max.x, m.aabb.max.y, m.aabb.max.z], np.float32),
+                         normal_indices=arr(m.vertex_normal_indices, 3 * t, np.uint32, (t, 3)),
+                         uv_indices=arr(m.vertex_uvs_indices, 3 * t, np.uint32, (t, 3)))
+    ref.ref_free(arena)
+    H.blas_sah(md, "orc")
+    assert (md.node_count, md.height) == (g["node_count"], g["height"])
+    assert sha(md.nodes[:md.node_count]) == g["nodes_sha256"]
+    assert sha(md.leaf_ids) == g["leaf_ids_sha256"]
+    assert sha(md.triangles) == g["triangles_sha256"]
+
+
+@pytest.mark.parametrize("key", sorted(GOLDEN["textures"]))
+def test_texture_bake_matches_reference(key):
+    """scenes.bake_texture (the residency format the device samples) equals bmp2texture's
+    loadTexture on the same image, mip by mip."""
+    g = GOLDEN["textures"][key]
+    wh, w_, m_ = key.split("_")
+    w, h = map(int, wh.split("x"))
+    wrap, mip = int(w_[1:]), int(m_[1:])
+    rng = np.random.default_rng(g["seed"])
+    # regenerate the same sequence of images as make_golden (one per key, in its order)
+    order = ["8x8_w1_m1", "16x8_w0_m1", "12x10_w1_m1", "33x17_w0_m0", "64x64_w1_m1"]
+    for k in order:
+        kw, kh = map(int, k.split("_")[0].split("x"))
+        img = rng.integers(0, 256, size=(kh, kw, 3), dtype=np.uint8)
+        if k == key:
+            break
+    td = scenes.bake_texture(img, bool(wrap), bool(mip))
+    assert len(td.mips) == len(g["mips"])
+    for (mw, mh, quads), (gw, gh, gd) in zip(td.mips, g["mips"]):
+        assert (mw, mh) == (gw, gh)
+        assert hashlib.sha256(quads.tobytes()).hexdigest() == gd
+
+
+@needs_ref
+def test_projection_plane_matches_reference():
+    ref = oracle.reference()
+    for cam in (scenes.CameraSpec(), scenes.look_at((3, 8, -20), (0, 1, 0)), scenes.look_at((-7, 2, 9), (1, 0, -2))):
+        for w, h in ((640, 480), (1920, 1080), (257, 99)):
+            fr = scenes.Frame(w, h, cam)
+            mine = (C.c_uint8 * C.sizeof(S.ProjectionPlane)).from_buffer_copy(fr.viewport.projection_plane)
+            ref.ref_begin_drawing(C.byref(fr.viewport))
+            theirs = (C.c_uint8 * C.sizeof(S.ProjectionPlane)).from_buffer_copy(fr.viewport.projection_plane)
+            assert bytes(mine) == bytes(theirs)
+
+
+@needs_ref
+def test_ssb_matches_reference():
+    ref, orc = oracle.reference(), oracle.restatement()
+    for sd, cam in (scenes.config0(), scenes.config2(count=512), scenes.config1(subdivisions=1, texture_size=8)):
+        for w, h in ((640, 480), (320, 180)):
+            a, b = sd.copy(), sd.copy()
+            sa, ka = a.to_ctypes()
+            sb, kb = b.to_ctypes()
+            fa, fb = scenes.Frame(w, h, cam), scenes.Frame(w, h, cam)
+            ref.ref_update_scene_ssb(C.byref(sa), C.byref(fa.viewport))
+            orc.orc_update_scene_ssb(C.byref(sb), C.byref(fb.viewport))
+            for f in S.PRIMITIVE_DT.names:   # fields only: the reference may write the 2 padding bytes
+                assert np.array_equal(a.primitives[f], b.primitives[f]), f
+
+
+def _lbvh(boxes, max_leaf):
+    orc = oracle.restatement()
+    n = len(boxes)
+    codes, order = np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+    nodes, leaf, info = np.zeros(2 * n, dtype=S.BVHNODE_DT), np.zeros(n, np.uint32), np.zeros(2, np.uint32)
+    boxes = np.ascontiguousarray(boxes, np.float32)
+    orc.orc_lbvh30(boxes.ctypes.data, n, max_leaf, codes.ctypes.data, order.ctypes.data, nodes.ctypes.data,
+                   leaf.ctypes.data, info.ctypes.data)
+    return codes, order, nodes[:info[0]], leaf, int(info[0]), int(info[1])
+
+
+@pytest.mark.parametrize("n,max_leaf", [(1, 2), (2, 2), (3, 2), (17, 2), (1000, 2), (5000, 4), (4096, 2)])
+def test_lbvh_oracle_structure(n, max_leaf):
+    """The LBVH30 specification: order sorts (code, index); every item sits in exactly one leaf of at
+    most max_leaf items; every node box is the union of what it covers; children pairs are
+    adjacent; height is the deepest leaf's depth."""
+    rng = np.random.default_rng(n)
+    c = rng.uniform(-10, 10, (n, 3))
+    e = rng.uniform(0.01, 1, (n, 3))
+    boxes = np.concatenate([c - e, c + e], 1)
+    codes, order, nodes, leaf, count, height = _lbvh(boxes, max_leaf)
+    keys = codes[order].astype(np.uint64) << np.uint64(32) | order.astype(np.uint64)
+    assert np.all(np.diff(keys.astype(np.float64)) > 0) or n == 1
+    assert np.array_equal(leaf, order)
+    covered = np.zeros(n, int)
+    depth_max = 0
+
+    def walk(i, depth):
+        nonlocal depth_max
+        nd = nodes[i]
+        if nd["child_count"]:
+            f, k = nd["first_child_id"], nd["child_count"]
+            assert k <= max(max_leaf, 1) or (i == 0 and n <= max_leaf)
+            covered[f:f + k] += 1
+            items = boxes[order[f:f + k]]
+            assert np.array_equal(nd["aabb"][:3], items[:, :3].min(0).astype(np.float32))
+            assert np.array_equal(nd["aabb"][3:], items[:, 3:].max(0).astype(np.float32))
+            depth_max = max(depth_max, depth)
+            return items[:, :3].min(0), items[:, 3:].max(0)
+        f = nd["first_child_id"]
+        assert f % 2 == 1 and f + 1 < count
+        assert nodes[f]["depth"] == depth + 1 and nodes[f + 1]["depth"] == depth + 1
+        a, b = walk(f, depth + 1), walk(f + 1, depth + 1)
+        lo, hi = np.minimum(a[0], b[0]), np.maximum(a[1], b[1])
+        assert np.array_equal(nd["aabb"][:3], lo.astype(np.float32)) and np.array_equal(nd["aabb"][3:], hi.astype(np.float32))
+        return lo, hi
+
+    walk(0, 0)
+    assert np.all(covered == 1)
+    assert height == max(depth_max, 1)
