@@ -50,7 +50,7 @@ enum st_status {
 /* TLAS/BLAS build modes for st_update_scene_bvh / st_update_mesh_bvh. */
 enum st_bvh_mode {
     ST_BVH_LBVH30 = 1,      /* 30-bit Morton LBVH: device radix sort, Karras topology, leaf collapse */
-    ST_BVH_BINNED_SAH = 2,  /* top-down binned SAH on the device */
+    ST_BVH_BINNED_SAH = 2,  /* breadth-first binned SAH (32 bins) on the device */
     ST_BVH_REFIT = 3        /* keep the resident topology, recompute every AABB bottom-up */
 };
 
@@ -132,6 +132,15 @@ ST_API int st_update_scene_bvh(st_ctx *ctx, int slot, Scene *scene, int mode);
  * reference's outputs into the caller's arrays: mesh->bvh.nodes (capacity 2*triangle_count),
  * mesh->bvh.leaf_ids, mesh->bvh.node_count/height and the BVH-ordered mesh->triangles. */
 ST_API int st_update_mesh_bvh(st_ctx *ctx, Mesh *mesh, int mode);
+
+/* The device builders of st_update_scene_bvh (mode ST_BVH_LBVH30 or ST_BVH_BINNED_SAH) over any `n`
+ * caller boxes (host array, 6 floats each: min.xyz, max.xyz) with leaves of at most `max_leaf`
+ * items.  Outputs (host): codes[n] the Morton code of each item (LBVH30 only, optional),
+ * order[n] the items in leaf order, nodes[2n] in the reference's BVHNode layout, info =
+ * {node_count, height}.  No reference counterpart: it exposes the builders behind updateSceneBVH's
+ * replacement to callers with their own boxes. */
+ST_API int st_build_bvh(st_ctx *ctx, int mode, const float *aabbs, uint32_t n, uint32_t max_leaf, uint32_t *codes,
+                        uint32_t *order, BVHNode *nodes, uint32_t info[2]);
 
 /* ---- render: render/raytracer.h:302 ------------------------------------------------------------ */
 /* renderScene (raytracer.h:302) + the QCAA resolve of drawViewportToWindowContent (viewport.h:12).

@@ -67,4 +67,6 @@ def restatement():
                                C.c_void_p, C.c_void_p]  # aabbs, n, max_leaf, codes, order, nodes, leaf_ids, info
     lib.orc_lbvh30.restype = C.c_int
     lib.orc_primitive_aabbs.argtypes = [C.c_void_p, C.c_void_p]
+    lib.orc_binned_sah.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.orc_binned_sah.restype = C.c_int
     return lib

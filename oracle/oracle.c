@@ -1632,3 +1632,151 @@ int orc_lbvh30(const float *aabbs, uint32_t n, uint32_t max_leaf, uint32_t *code
     free(slot); free(rank); free(first); free(last); free(lchild); free(rchild); free(parent); free(keys);
     return 0;
 }
+
+/* ---- binned SAH (project specification; the reference's builder is the full-sweep SAH above) -- */
+#define ORC_BINS 32
+typedef struct { u32 begin, end, slot; AABB box, cbox; } OTask;
+
+static inline f32 half_area_t(const AABB *a) {
+    f32 ex = a->max.x - a->min.x, ey = a->max.y - a->min.y, ez = a->max.z - a->min.z;
+    return ex * ey + ey * ez + ez * ex;
+}
+static inline void grow(AABB *a, const float *b) {
+    a->min.x = tmin(a->min.x, b[0]); a->min.y = tmin(a->min.y, b[1]); a->min.z = tmin(a->min.z, b[2]);
+    a->max.x = tmax(a->max.x, b[3]); a->max.y = tmax(a->max.y, b[4]); a->max.z = tmax(a->max.z, b[5]);
+}
+static inline void grow_box(AABB *a, const AABB *b) { grow(a, &b->min.x); }
+static inline void empty_box(AABB *a) { a->min = splat(INFINITY); a->max = splat(-INFINITY); }
+static inline u32 bin_of(f32 c, f32 lo, f32 scale) {
+    f32 t = (c - lo) * scale;
+    if (!(t > 0.0f)) return 0;
+    if (t >= (f32)(ORC_BINS - 1)) return ORC_BINS - 1;
+    return (u32)t;
+}
+
+/* Breadth-first binned SAH over n item boxes, leaves of at most max_leaf items:
+ *   centroid (min+max)*0.5; a node's centroid box and box are unions under the IEEE total order;
+ *   per axis with a non-zero centroid extent e, bin = clamp((c - lo) * (32/e)) into 32 bins;
+ *   split candidates after bin k (k = 0..30) cost halfArea(L)*nL + halfArea(R)*nR (the
+ *   reference's surface-area formula, AABB.h:39), skipping empty sides; the lowest cost wins,
+ *   ties to the lower axis then the lower k; with no candidate the range is split at its middle;
+ *   the partition is stable; the split nodes of one level get child pairs in level order
+ *   (pair p -> slots 1+2p, 2+2p); depth = level, height = deepest leaf (1 for a root leaf). */
+int orc_binned_sah(const float *aabbs, uint32_t n, uint32_t max_leaf, uint32_t *order, BVHNode *nodes,
+                   uint32_t *info) {
+    f32 *cent = (f32*)malloc(sizeof(f32) * 3 * (n ? n : 1));
+    u32 *ids = (u32*)malloc(sizeof(u32) * (n ? n : 1)), *tmp = (u32*)malloc(sizeof(u32) * (n ? n : 1));
+    OTask *cur = (OTask*)malloc(sizeof(OTask) * (n ? n : 1)), *next = (OTask*)malloc(sizeof(OTask) * (n ? n : 1));
+    AABB root, rootc;
+    empty_box(&root);
+    empty_box(&rootc);
+    for (u32 i = 0; i < n; i++) {
+        ids[i] = i;
+        for (int a = 0; a < 3; a++) cent[3 * i + a] = (aabbs[6 * i + a] + aabbs[6 * i + 3 + a]) * 0.5f;
+        grow(&root, aabbs + 6 * i);
+        f32 c6[6] = {cent[3 * i], cent[3 * i + 1], cent[3 * i + 2], cent[3 * i], cent[3 * i + 1], cent[3 * i + 2]};
+        grow(&rootc, c6);
+    }
+    u32 ncur = 1, pairs = 0, height = 1, level = 0;
+    cur[0].begin = 0; cur[0].end = n; cur[0].slot = 0; cur[0].box = root; cur[0].cbox = rootc;
+    while (ncur) {
+        u32 nnext = 0;
+        for (u32 t = 0; t < ncur; t++) {
+            OTask *T = cur + t;
+            BVHNode *node = nodes + T->slot;
+            u32 cnt = T->end - T->begin;
+            memset(node, 0, sizeof(*node));
+            node->aabb = T->box;
+            node->depth = (u16)level;
+            if (cnt <= max_leaf) {
+                node->first_child_id = T->begin;
+                node->child_count = (u16)cnt;
+                if (level > height) height = level;
+                continue;
+            }
+            /* bins of the three axes */
+            u32 bc[3][ORC_BINS];
+            AABB bb[3][ORC_BINS], bcb[3][ORC_BINS];
+            f32 lo[3], scale[3];
+            int valid[3];
+            const f32 *cl = &T->cbox.min.x;
+            for (int a = 0; a < 3; a++) {
+                f32 e = cl[3 + a] - cl[a];
+                valid[a] = e > 0.0f;
+                lo[a] = cl[a];
+                scale[a] = valid[a] ? (f32)ORC_BINS / e : 0.0f;
+                for (int b = 0; b < ORC_BINS; b++) { bc[a][b] = 0; empty_box(&bb[a][b]); empty_box(&bcb[a][b]); }
+            }
+            for (u32 k = T->begin; k < T->end; k++) {
+                u32 i = ids[k];
+                f32 c6[6] = {cent[3 * i], cent[3 * i + 1], cent[3 * i + 2], cent[3 * i], cent[3 * i + 1], cent[3 * i + 2]};
+                for (int a = 0; a < 3; a++) {
+                    if (!valid[a]) continue;
+                    u32 b = bin_of(cent[3 * i + a], lo[a], scale[a]);
+                    bc[a][b]++;
+                    grow(&bb[a][b], aabbs + 6 * i);
+                    grow(&bcb[a][b], c6);
+                }
+            }
+            int best_axis = -1, best_k = -1;
+            f32 best = INFINITY;
+            for (int a = 0; a < 3; a++) {
+                if (!valid[a]) continue;
+                AABB R[ORC_BINS];
+                u32 nR[ORC_BINS];
+                AABB acc;
+                empty_box(&acc);
+                u32 an = 0;
+                for (int b = ORC_BINS - 1; b >= 1; b--) { grow_box(&acc, &bb[a][b]); an += bc[a][b]; R[b] = acc; nR[b] = an; }
+                empty_box(&acc);
+                an = 0;
+                for (int k = 0; k < ORC_BINS - 1; k++) {
+                    grow_box(&acc, &bb[a][k]);
+                    an += bc[a][k];
+                    if (!an || !nR[k + 1]) continue;
+                    f32 cost = half_area_t(&acc) * (f32)an + half_area_t(&R[k + 1]) * (f32)nR[k + 1];
+                    if (cost < best) { best = cost; best_axis = a; best_k = k; }
+                }
+            }
+            OTask L, Rt;
+            u32 mid;
+            if (best_axis >= 0) {
+                u32 nl = 0, p = T->begin;
+                for (u32 k = T->begin; k < T->end; k++)
+                    if (bin_of(cent[3 * ids[k] + best_axis], lo[best_axis], scale[best_axis]) <= (u32)best_k) tmp[p++] = ids[k], nl++;
+                for (u32 k = T->begin; k < T->end; k++)
+                    if (bin_of(cent[3 * ids[k] + best_axis], lo[best_axis], scale[best_axis]) > (u32)best_k) tmp[p++] = ids[k];
+                memcpy(ids + T->begin, tmp + T->begin, sizeof(u32) * cnt);
+                mid = T->begin + nl;
+                empty_box(&L.box); empty_box(&L.cbox); empty_box(&Rt.box); empty_box(&Rt.cbox);
+                for (int b = 0; b < ORC_BINS; b++) {
+                    if (b <= best_k) { grow_box(&L.box, &bb[best_axis][b]); grow_box(&L.cbox, &bcb[best_axis][b]); }
+                    else { grow_box(&Rt.box, &bb[best_axis][b]); grow_box(&Rt.cbox, &bcb[best_axis][b]); }
+                }
+            } else {
+                mid = T->begin + cnt / 2;
+                empty_box(&L.box); empty_box(&L.cbox); empty_box(&Rt.box); empty_box(&Rt.cbox);
+                for (u32 k = T->begin; k < T->end; k++) {
+                    u32 i = ids[k];
+                    f32 c6[6] = {cent[3 * i], cent[3 * i + 1], cent[3 * i + 2], cent[3 * i], cent[3 * i + 1], cent[3 * i + 2]};
+                    if (k < mid) { grow(&L.box, aabbs + 6 * i); grow(&L.cbox, c6); }
+                    else { grow(&Rt.box, aabbs + 6 * i); grow(&Rt.cbox, c6); }
+                }
+            }
+            node->first_child_id = 1 + 2 * pairs;
+            L.begin = T->begin; L.end = mid; L.slot = 1 + 2 * pairs;
+            Rt.begin = mid; Rt.end = T->end; Rt.slot = 2 + 2 * pairs;
+            pairs++;
+            next[nnext++] = L;
+            next[nnext++] = Rt;
+        }
+        OTask *sw = cur; cur = next; next = sw;
+        ncur = nnext;
+        level++;
+    }
+    memcpy(order, ids, sizeof(u32) * n);
+    info[0] = 1 + 2 * pairs;
+    info[1] = height;
+    free(cent); free(ids); free(tmp); free(cur); free(next);
+    return 0;
+}

@@ -43,6 +43,12 @@ void orc_primitive_aabbs(const Scene *scene, float *out);
 int orc_lbvh30(const float *aabbs, uint32_t n, uint32_t max_leaf, uint32_t *codes, uint32_t *order,
                BVHNode *nodes, uint32_t *leaf_ids, uint32_t *info);
 
+/* Binned SAH over `n` AABBs (32 bins, breadth-first, the project's specification; see oracle.c).
+ * Outputs order[n] (leaf order), nodes[2n] in the reference's BVHNode layout, info = {node_count,
+ * height}.  Returns 0. */
+int orc_binned_sah(const float *aabbs, uint32_t n, uint32_t max_leaf, uint32_t *order, BVHNode *nodes,
+                   uint32_t *info);
+
 #ifdef __cplusplus
 }
 #endif

@@ -70,6 +70,7 @@ def lib():
             "st_update_scene_bvh": (i, [vp, i, vp, i]),
             "st_update_mesh_bvh": (i, [vp, vp, i]),
             "st_render_scene": (i, [vp, i, vp, vp]),
+            "st_build_bvh": (i, [vp, i, vp, u32, u32, vp, vp, vp, vp]),
             "st_render_ex": (i, [vp, i, vp, vp, C.POINTER(st_render_options)]),
         }
         for name, (res, args) in sig.items():
@@ -154,6 +155,17 @@ class Renderer:
         ids = np.ascontiguousarray(ids, dtype=np.uint32)
         self._check(self.L.st_update_primitives(self.ctx, slot, prims.ctypes.data, ids.ctypes.data, len(ids)),
                     "st_update_primitives")
+
+    def build_lbvh(self, boxes, max_leaf, mode=ST_BVH_LBVH30):
+        """A device BVH over caller boxes (n x 6 float32): returns codes, order, nodes, node_count,
+        height (codes only for LBVH30)."""
+        boxes = np.ascontiguousarray(boxes, dtype=np.float32)
+        n = len(boxes)
+        codes, order = np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+        nodes, info = np.zeros(2 * n, dtype=S.BVHNODE_DT), np.zeros(2, np.uint32)
+        self._check(self.L.st_build_bvh(self.ctx, mode, boxes.ctypes.data, n, max_leaf, codes.ctypes.data,
+                                        order.ctypes.data, nodes.ctypes.data, info.ctypes.data), "st_build_bvh")
+        return codes, order, nodes[:info[0]], int(info[0]), int(info[1])
 
     def free(self, slot):
         self._check(self.L.st_free_scene(self.ctx, slot), "st_free_scene")

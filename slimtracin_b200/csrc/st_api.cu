@@ -504,6 +504,16 @@ int st_update_scene_bvh(st_ctx *ctx, int slot, Scene *scene, int mode) {
         S->tlas_node_count = info[0];
         S->tlas_height = info[1];
         if (S->tlas_height + 2 > (u32t)kStack) return ST_ERR_BAD_SCENE;
+    } else if (mode == ST_BVH_BINNED_SAH) {
+        if (lbvh_reserve(ctx->lbvh, n) != cudaSuccess) return ST_ERR_OUT_OF_MEMORY;
+        launch_prim_aabbs(P<Primitive>(S->prims_raw), P<MeshDev>(S->meshes), n, ctx->lbvh.aabbs, ctx->stream);
+        u32t info[2];
+        cudaError_t e = sah_build(ctx->lbvh.aabbs, n, MAX_OBJS_PER_SCENE_BVH_NODE, P<BVHNode>(S->tlas_nodes),
+                                  P<u32t>(S->tlas_leaf_ids), info, ctx->stream);
+        if (e != cudaSuccess) return fail_cuda(ctx, e);
+        S->tlas_node_count = info[0];
+        S->tlas_height = info[1];
+        if (S->tlas_height + 2 > (u32t)kStack) return ST_ERR_BAD_SCENE;
     } else if (mode == ST_BVH_REFIT) {
         if (!S->tlas_valid) return ST_ERR_NOT_RESIDENT;
         launch_prim_aabbs(P<Primitive>(S->prims_raw), P<MeshDev>(S->meshes), n, P<float>(S->tlas_aabbs), ctx->stream);
@@ -539,7 +549,7 @@ int st_update_mesh_bvh(st_ctx *ctx, Mesh *mesh, int mode) {
     if (!ctx || !mesh || !mesh->vertex_positions || !mesh->vertex_position_indices || !mesh->vertex_normals ||
         !mesh->vertex_normal_indices || !mesh->triangles || !mesh->bvh.nodes || !mesh->bvh.leaf_ids)
         return ST_ERR_INVALID_ARG;
-    if (mode != ST_BVH_LBVH30) return ST_ERR_INVALID_ARG;
+    if (mode != ST_BVH_LBVH30 && mode != ST_BVH_BINNED_SAH) return ST_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
     const u32t n = mesh->triangle_count;
     if (!n) return ST_ERR_BAD_SCENE;
@@ -578,7 +588,9 @@ int st_update_mesh_bvh(st_ctx *ctx, Mesh *mesh, int mode) {
     }
     launch_tri_aabbs(pos, pidx, n, ctx->lbvh.aabbs, st);
     u32t info[2];
-    cudaError_t e = lbvh_build(ctx->lbvh, n, MAX_TRIANGLES_PER_MESH_BVH_NODE, nodes, order, info, st);
+    cudaError_t e = mode == ST_BVH_LBVH30
+        ? lbvh_build(ctx->lbvh, n, MAX_TRIANGLES_PER_MESH_BVH_NODE, nodes, order, info, st)
+        : sah_build(ctx->lbvh.aabbs, n, MAX_TRIANGLES_PER_MESH_BVH_NODE, nodes, order, info, st);
     if (e == cudaSuccess) {
         launch_tri_records(pos, nrm, uv, pidx, nidx, uidx, mesh->uvs_count ? 1 : 0, order, n, tris, inverse, st);
         cudaMemcpyAsync(mesh->bvh.nodes, nodes, sizeof(BVHNode) * info[0], cudaMemcpyDeviceToHost, st);
@@ -593,6 +605,41 @@ int st_update_mesh_bvh(st_ctx *ctx, Mesh *mesh, int mode) {
     if (e != cudaSuccess) return fail_cuda(ctx, e);
     mesh->bvh.node_count = info[0];
     mesh->bvh.height = info[1];
+    return ST_OK;
+}
+
+int st_build_bvh(st_ctx *ctx, int mode, const float *aabbs, uint32_t n, uint32_t max_leaf, uint32_t *codes,
+                 uint32_t *order, BVHNode *nodes, uint32_t info[2]) {
+    if (!ctx || !aabbs || !nodes || !order || !info || n == 0 || max_leaf == 0 || max_leaf > 0xFFFF ||
+        (mode != ST_BVH_LBVH30 && mode != ST_BVH_BINNED_SAH))
+        return ST_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    if (lbvh_reserve(ctx->lbvh, n) != cudaSuccess) return ST_ERR_OUT_OF_MEMORY;
+    cudaStream_t st = ctx->stream;
+    char *base = nullptr;
+    const size_t bytes = sizeof(BVHNode) * 2 * (size_t)n + sizeof(u32t) * 2 * (size_t)n + 512;
+    if (ctx->in_use + bytes > ctx->budget) return ST_ERR_BUDGET;
+    ST_CUDA(cudaMallocAsync((void **)&base, bytes, st));
+    BVHNode *d_nodes = (BVHNode *)base;
+    u32t *d_order = (u32t *)(base + ((sizeof(BVHNode) * 2 * (size_t)n + 255) & ~(size_t)255));
+    u32t *d_codes = d_order + n;
+    cudaMemcpyAsync(ctx->lbvh.aabbs, aabbs, sizeof(float) * 6 * (size_t)n, cudaMemcpyHostToDevice, st);
+    u32t inf[2];
+    cudaError_t e = mode == ST_BVH_LBVH30 ? lbvh_build(ctx->lbvh, n, max_leaf, d_nodes, d_order, inf, st)
+                                          : sah_build(ctx->lbvh.aabbs, n, max_leaf, d_nodes, d_order, inf, st);
+    if (e == cudaSuccess) {
+        if (mode == ST_BVH_LBVH30) launch_codes_by_item(ctx->lbvh, n, d_codes, st);
+        else codes = nullptr;
+        cudaMemcpyAsync(nodes, d_nodes, sizeof(BVHNode) * inf[0], cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(order, d_order, sizeof(u32t) * n, cudaMemcpyDeviceToHost, st);
+        if (codes) cudaMemcpyAsync(codes, d_codes, sizeof(u32t) * n, cudaMemcpyDeviceToHost, st);
+        e = cudaStreamSynchronize(st);
+    }
+    cudaFreeAsync(base, st);
+    cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail_cuda(ctx, e);
+    info[0] = inf[0];
+    info[1] = inf[1];
     return ST_OK;
 }
 

@@ -198,7 +198,7 @@ __global__ void scan_down_kernel(const u32t *in, u32t *out, u32t n, const u32t *
     u32t ex = block_exclusive_scan_256(s, sm, total) + sums[blockIdx.x];
     for (int k = 0; k < 4; k++) { if (base + k < n) out[base + k] = ex; ex += v[k]; }
 }
-static void scan_exclusive(const u32t *in, u32t *out, u32t n, u32t *sums, u32t *total, cudaStream_t st) {
+void scan_exclusive_u32(const u32t *in, u32t *out, u32t n, u32t *sums, u32t *total, cudaStream_t st) {
     u32t nb = (n + SCAN_BLOCK - 1) / SCAN_BLOCK;
     scan_reduce_kernel<<<nb, 256, 0, st>>>(in, n, sums);
     scan_top_kernel<<<1, 256, 0, st>>>(sums, nb, total);
@@ -365,6 +365,14 @@ __global__ void single_leaf_kernel(const float *aabbs, const u32t *order, u32t n
     write_node(out[0], b, 0, n, 0);
 }
 
+__global__ void codes_by_item_kernel(const u32t *sorted_codes, const u32t *order, u32t n, u32t *out) {
+    u32t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) out[order[k]] = sorted_codes[k];
+}
+void launch_codes_by_item(const LbvhScratch &s, u32t n, u32t *out, cudaStream_t st) {
+    if (n) codes_by_item_kernel<<<(n + 255) / 256, 256, 0, st>>>(s.codes, s.order, n, out);
+}
+
 cudaError_t lbvh_reserve(LbvhScratch &s, u32t n) {
     if (n <= s.capacity) return cudaSuccess;
     lbvh_release(s);
@@ -415,7 +423,7 @@ cudaError_t lbvh_build(LbvhScratch &s, u32t n, u32t max_leaf, BVHNode *out_nodes
     u32t *kin = s.codes, *vin = s.order, *kout = s.codes_alt, *vout = s.order_alt;
     for (int pass = 0; pass < 4; pass++) {
         rs_hist_kernel<<<nblocks, RS_THREADS, 0, st>>>(kin, n, 8 * pass, hist, nblocks);
-        scan_exclusive(hist, hist, 256 * nblocks, sums, nullptr, st);
+        scan_exclusive_u32(hist, hist, 256 * nblocks, sums, nullptr, st);
         rs_scatter_kernel<<<nblocks, RS_THREADS, 0, st>>>(kin, vin, kout, vout, n, 8 * pass, hist, nblocks);
         u32t *tk = kin; kin = kout; kout = tk;
         u32t *tv = vin; vin = vout; vout = tv;
@@ -432,7 +440,7 @@ cudaError_t lbvh_build(LbvhScratch &s, u32t n, u32t max_leaf, BVHNode *out_nodes
     karras_kernel<<<(ni + T - 1) / T, T, 0, st>>>(s.codes, s.order, n, s.first, s.last, s.lchild, s.rchild, s.parent,
                                                   s.leaf_parent);
     keep_flags_kernel<<<(ni + T - 1) / T, T, 0, st>>>(s.first, s.last, ni, max_leaf, s.flags);
-    scan_exclusive(s.flags, s.rank, ni, s.hist, s.info + 2, st);
+    scan_exclusive_u32(s.flags, s.rank, ni, s.hist, s.info + 2, st);
     // arrivals reuse codes_alt (free after the sort)
     cudaMemsetAsync(s.codes_alt, 0, sizeof(u32t) * ni, st);
     karras_boxes_kernel<<<(n + T - 1) / T, T, 0, st>>>(s.aabbs, s.order, n, s.lchild, s.rchild, s.parent, s.leaf_parent,

@@ -50,6 +50,11 @@ void lbvh_release(LbvhScratch &s);
 // out_nodes must hold 2n nodes; out_order n ids.  info (host) receives node_count, height.
 cudaError_t lbvh_build(LbvhScratch &s, u32t n, u32t max_leaf, BVHNode *out_nodes, u32t *out_order,
                        u32t info[2], cudaStream_t st);
+// Binned SAH over n device boxes (st_sah.cu): reference-layout nodes (2n capacity) + leaf order.
+cudaError_t sah_build(const float *aabbs, u32t n, u32t max_leaf, BVHNode *out_nodes, u32t *out_order, u32t info[2],
+                      cudaStream_t st);
+// After lbvh_build: the Morton code of every item, by item index.
+void launch_codes_by_item(const LbvhScratch &s, u32t n, u32t *out, cudaStream_t st);
 // World boxes of primitives as updateSceneBVH computes them (builder_top_down.h:370-377).
 void launch_prim_aabbs(const Primitive *prims, const MeshDev *meshes, u32t n, float *aabbs, cudaStream_t st);
 // Triangle boxes with the reference's EPS padding (builder_top_down.h:283-318).

@@ -90,14 +90,14 @@ __device__ bool trace_mesh(TState<CNT> &t, const SceneDev &S, const MeshDev &M, 
             if (rgo) {
                 if (!any_hit && ld > rd) { near_pair = P.d.z; far_pair = P.d.x; }
                 if (sp >= kStack) { t.status |= S_STACK_OVERFLOW; return false; }
-                t.stack[sp++] = far_pair;
+                t.mesh_stack[sp++] = far_pair;
             }
             pair = near_pair;
         } else if (rgo) {
             pair = P.d.z;
         } else {
             if (sp == 0) break;
-            pair = t.stack[--sp];
+            pair = t.mesh_stack[--sp];
         }
     }
     return found;
@@ -228,14 +228,14 @@ __device__ bool trace_scene(TState<CNT> &t, const SceneDev &S, RayD &ray, bool a
             if (rgo) {
                 if (!any_hit && ld > rd) { near_pair = P.d.z; far_pair = P.d.x; }
                 if (sp >= kStack) { t.status |= S_STACK_OVERFLOW; return found; }
-                t.stack[sp++] = far_pair;
+                t.scene_stack[sp++] = far_pair;
             }
             pair = near_pair;
         } else if (rgo) {
             pair = P.d.z;
         } else {
             if (sp == 0) break;
-            pair = t.stack[--sp];
+            pair = t.scene_stack[--sp];
         }
     }
     return found;
@@ -682,6 +682,7 @@ __global__ void resolve_kernel(const FloatPixel *in, u32t grid_w, u32t width, u3
     out[(size_t)y * width + x] = px;
 }
 
+#ifndef ST_HOST_EMU
 // ---- launchers -------------------------------------------------------------------------------
 void launch_ssb(const SceneDev &S, const ViewDev &v, int4 *ssb, cudaStream_t st) {
     if (!S.n_prims) return;
@@ -701,4 +702,5 @@ void launch_resolve(const FloatPixel *in, u32t grid_w, u32t width, u32t height, 
     resolve_kernel<<<grid, 128, 0, st>>>(in, grid_w, width, height, out);
 }
 
+#endif  // ST_HOST_EMU
 }  // namespace st

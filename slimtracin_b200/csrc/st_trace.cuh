@@ -44,7 +44,8 @@ struct TState {
     u32t depth;
     unsigned status;
     unsigned cnt[CNT ? C_COUNT : 1];
-    u32t stack[kStack];
+    u32t scene_stack[kStack];   // the TLAS walk (the reference's trace->scene_stack, trace.h:22)
+    u32t mesh_stack[kStack];    // the BLAS walk nested inside it (trace->mesh_stack, mesh.h:42)
     __device__ __forceinline__ void count(int k, unsigned n = 1) { if (CNT) cnt[k] += n; }
 };
 

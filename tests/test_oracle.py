@@ -159,19 +159,24 @@ def test_ssb_matches_reference():
                 assert np.array_equal(a.primitives[f], b.primitives[f]), f
 
 
-def _lbvh(boxes, max_leaf):
+def _lbvh(boxes, max_leaf, builder="lbvh"):
     orc = oracle.restatement()
     n = len(boxes)
     codes, order = np.zeros(n, np.uint32), np.zeros(n, np.uint32)
     nodes, leaf, info = np.zeros(2 * n, dtype=S.BVHNODE_DT), np.zeros(n, np.uint32), np.zeros(2, np.uint32)
     boxes = np.ascontiguousarray(boxes, np.float32)
-    orc.orc_lbvh30(boxes.ctypes.data, n, max_leaf, codes.ctypes.data, order.ctypes.data, nodes.ctypes.data,
-                   leaf.ctypes.data, info.ctypes.data)
+    if builder == "lbvh":
+        orc.orc_lbvh30(boxes.ctypes.data, n, max_leaf, codes.ctypes.data, order.ctypes.data, nodes.ctypes.data,
+                       leaf.ctypes.data, info.ctypes.data)
+    else:
+        orc.orc_binned_sah(boxes.ctypes.data, n, max_leaf, order.ctypes.data, nodes.ctypes.data, info.ctypes.data)
+        leaf = order.copy()
     return codes, order, nodes[:info[0]], leaf, int(info[0]), int(info[1])
 
 
+@pytest.mark.parametrize("builder", ["lbvh", "binned_sah"])
 @pytest.mark.parametrize("n,max_leaf", [(1, 2), (2, 2), (3, 2), (17, 2), (1000, 2), (5000, 4), (4096, 2)])
-def test_lbvh_oracle_structure(n, max_leaf):
+def test_bvh_oracle_structure(n, max_leaf, builder):
     """The LBVH30 specification: order sorts (code, index); every item sits in exactly one leaf of at
     most max_leaf items; every node box is the union of what it covers; children pairs are
     adjacent; height is the deepest leaf's depth."""
@@ -179,9 +184,11 @@ def test_lbvh_oracle_structure(n, max_leaf):
     c = rng.uniform(-10, 10, (n, 3))
     e = rng.uniform(0.01, 1, (n, 3))
     boxes = np.concatenate([c - e, c + e], 1)
-    codes, order, nodes, leaf, count, height = _lbvh(boxes, max_leaf)
-    keys = codes[order].astype(np.uint64) << np.uint64(32) | order.astype(np.uint64)
-    assert np.all(np.diff(keys.astype(np.float64)) > 0) or n == 1
+    codes, order, nodes, leaf, count, height = _lbvh(boxes, max_leaf, builder)
+    if builder == "lbvh":
+        keys = codes[order].astype(np.uint64) << np.uint64(32) | order.astype(np.uint64)
+        assert np.all(np.diff(keys.astype(np.float64)) > 0) or n == 1
+    assert np.array_equal(np.sort(order), np.arange(n))
     assert np.array_equal(leaf, order)
     covered = np.zeros(n, int)
     depth_max = 0
