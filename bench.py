@@ -73,7 +73,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -107,8 +107,8 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
-def cpu_reference_rows(sd, cam, rows, threads):
-    """Time the reference's renderer (oracle/_ref) on `rows` rows spread evenly over the frame."""
+def reference_frame_setup(sd, cam):
+    """The reference's per-frame set-up on a private copy of the scene: updateSceneSSB, beginDrawing."""
     import oracle
     ref = oracle.reference()
     d = sd.copy()
@@ -116,20 +116,21 @@ def cpu_reference_rows(sd, cam, rows, threads):
     fr = scenes.Frame(WIDTH, HEIGHT, cam, depth=DEPTH)
     ref.ref_update_scene_ssb(C.byref(sc), C.byref(fr.viewport))
     ref.ref_begin_drawing(C.byref(fr.viewport))
-    step = max(1, fr.grid_h // rows)
-    first = step // 2
-    t = time.perf_counter()
-    ref.ref_render_rows(C.byref(sc), C.byref(fr.viewport), threads, first, step, rows)
-    dt = time.perf_counter() - t
-    return rows * fr.grid_w, dt
+    return ref, sc, fr, (d, keep)
 
 
-def calibrated_reference(sd, cam, threads, budget_s):
-    """Pick a row count whose reference render takes about budget_s seconds."""
-    rays, dt = cpu_reference_rows(sd, cam, max(threads, 8), threads)
-    per_row = dt / max(threads, 8)
-    rows = int(max(threads, min(1081, budget_s / max(per_row, 1e-6))))
-    return rows
+def cpu_reference_sample(sd, cam, threads, budget_s):
+    """The reference's renderer (oracle/_ref) on whole frames of the same scene bytes, repeated until
+    about budget_s seconds have passed.  Returns (rays, seconds, frames)."""
+    ref, sc, fr, keep = reference_frame_setup(sd, cam)
+    rays, total, frames = 0, 0.0, 0
+    while total < budget_s or frames == 0:
+        t = time.perf_counter()
+        ref.ref_render_rows(C.byref(sc), C.byref(fr.viewport), threads, 0, 1, fr.grid_h)
+        total += time.perf_counter() - t
+        rays += fr.rays
+        frames += 1
+    return rays, total, frames
 
 
 def run_reference_arm(args):
@@ -145,26 +146,32 @@ def run_reference_arm(args):
     blas_on_device(sd)
     import tests.helpers as H
     H.tlas_sah(sd, "ref")
-    rows = calibrated_reference(sd, cam, threads, 6.0)
-    for _ in range(args.warmup):
-        cpu_reference_rows(sd, cam, max(threads, 8), threads)
-    times, rays = [], 0
-    for _ in range(args.steps):
-        r, dt = cpu_reference_rows(sd, cam, rows, threads)
-        times.append(dt)
-        rays += r
-    total = sum(times)
+    ref, sc, fr, keep = reference_frame_setup(sd, cam)
+    # each step renders whole frames; steps are capped so the run stays within a few minutes
+    t0 = time.perf_counter()
+    ref.ref_render_rows(C.byref(sc), C.byref(fr.viewport), threads, 0, 1, fr.grid_h)
+    frame_s = time.perf_counter() - t0
+    steps = max(1, min(args.steps, int(120.0 / max(frame_s, 1e-3))))
+    for _ in range(min(args.warmup, 3)):
+        ref.ref_render_rows(C.byref(sc), C.byref(fr.viewport), threads, 0, 1, fr.grid_h)
+    total, rays = 0.0, 0
+    for _ in range(steps):
+        t = time.perf_counter()
+        ref.ref_render_rows(C.byref(sc), C.byref(fr.viewport), threads, 0, 1, fr.grid_h)
+        total += time.perf_counter() - t
+        rays += fr.rays
     value = rays / total / 1e6
+    rows = fr.grid_h
     grid = (WIDTH + 1) * (HEIGHT + 1)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * grid / (value * 1e6),
+            "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * grid / (value * 1e6),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded config1 scene bytes, identical to the device arm)",
             "config": {"workload": "config1 1080p PBR mesh scene, depth 4, 1.31M-triangle BLAS x 8 instances",
                        "width": WIDTH, "height": HEIGHT, "depth": DEPTH, "rays_per_frame": grid},
             "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": "reference",
-                             "sample": f"{rows} of {HEIGHT + 1} QCAA rows per step, rows spread evenly; "
-                                       f"reference rayTrace (raytracer.h:81) per pixel, {threads} threads"},
+                             "sample": f"{steps} whole frames ({rows} QCAA rows each), reference rayTrace "
+                                       f"(raytracer.h:81) per pixel, {threads} threads, {total:.1f} s"},
             "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -183,7 +190,7 @@ def blas_on_device(sd):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -228,14 +235,15 @@ def main():
             flush.zero_()
         return r.render_device(0, sd, frame, out_float.data_ptr(), out_u8.data_ptr())
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
     trace_ms = []
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     with ClockSampler(local) as clocks:
+        # clocks are sampled from the warm-up on, so short timed regions still get samples under load
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
         torch.cuda.synchronize()
         for k in range(args.steps):
             with torch.cuda.stream(stream):
@@ -320,10 +328,9 @@ def main():
                     ref_sd.meshes = sd.meshes
                     import tests.helpers as H
                     H.tlas_sah(ref_sd, "ref")
-                    rows = calibrated_reference(ref_sd, cam, threads, 15.0)
-                    rays, dt = cpu_reference_rows(ref_sd, cam, rows, threads)
+                    rays, dt, frames = cpu_reference_sample(ref_sd, cam, threads, 10.0)
                     cpu = {"value": rays / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "reference",
-                           "sample": f"{rows} of {HEIGHT + 1} QCAA rows spread evenly, same scene bytes, "
+                           "sample": f"{frames} whole 1921x1081 frames of the same scene bytes, "
                                      f"{dt:.1f} s on {threads} host threads"}
             except Exception as ex:  # the baseline is reported, never required
                 cpu = {"value": None, "unit": "Mrays/s", "cores": os.cpu_count(), "kind": "reference",

@@ -154,6 +154,31 @@ ST_API int st_render_scene(st_ctx *ctx, int slot, const Scene *scene, Viewport *
 ST_API int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *viewport,
                  st_render_options *options);
 
+/* ---- batched views: many views of resident scenes in one persistent launch --------------------- */
+typedef struct st_view {
+    int slot;                   /* resident scene */
+    const Scene *scene;         /* per-frame values (ambient light); NULL -> the uploaded ones */
+    const Viewport *viewport;   /* camera, projection plane (set by the caller), dims, mode, trace.depth */
+    FloatPixel *out_float;      /* optional (W+1)x(H+1) grid, host or device per device_outputs */
+    Pixel *out_u8;              /* optional W x H resolved BGRA */
+} st_view;
+
+typedef struct st_batch_options {
+    void *stream;               /* cudaStream_t; NULL -> the context's stream */
+    int device_outputs;         /* 1: out_* are device pointers */
+    int tile_shape;             /* -1: autotuned; 0: 8x4, 1: 16x2, 2: 32x1, 3: 4x8 grid points per warp */
+    int chunk;                  /* tiles a warp takes per queue fetch; 0: autotuned */
+    int use_graph;              /* 1: replay a captured CUDA graph while the batch's shape is unchanged */
+    float batch_ms;             /* out: CUDA-event time of the batch on the launch stream */
+    uint64_t rays;              /* out: primary rays traced */
+    int tile_shape_used, chunk_used, graph_replayed;   /* out */
+} st_batch_options;
+
+/* Render `view_count` views (different sizes, scenes, render modes and bounce counts) with one
+ * persistent kernel over a shared tile queue.  No reference counterpart: the reference renders one
+ * viewport per renderScene call (raytracer.h:302); each view's output equals st_render_ex's. */
+ST_API int st_render_batch(st_ctx *ctx, const st_view *views, int view_count, st_batch_options *options);
+
 #ifdef __cplusplus
 }
 #endif

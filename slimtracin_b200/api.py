@@ -33,6 +33,17 @@ class st_render_options(C.Structure):
                 ("total_ms", C.c_float)]
 
 
+class st_view(C.Structure):
+    _fields_ = [("slot", C.c_int), ("scene", C.c_void_p), ("viewport", C.c_void_p), ("out_float", C.c_void_p),
+                ("out_u8", C.c_void_p)]
+
+
+class st_batch_options(C.Structure):
+    _fields_ = [("stream", C.c_void_p), ("device_outputs", C.c_int), ("tile_shape", C.c_int), ("chunk", C.c_int),
+                ("use_graph", C.c_int), ("batch_ms", C.c_float), ("rays", C.c_uint64),
+                ("tile_shape_used", C.c_int), ("chunk_used", C.c_int), ("graph_replayed", C.c_int)]
+
+
 class STError(RuntimeError):
     def __init__(self, status, what, detail=""):
         self.status = status
@@ -72,6 +83,7 @@ def lib():
             "st_render_scene": (i, [vp, i, vp, vp]),
             "st_build_bvh": (i, [vp, i, vp, u32, u32, vp, vp, vp, vp]),
             "st_render_ex": (i, [vp, i, vp, vp, C.POINTER(st_render_options)]),
+            "st_render_batch": (i, [vp, vp, i, C.POINTER(st_batch_options)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -196,6 +208,25 @@ class Renderer:
         self._check(self.L.st_render_ex(self.ctx, slot, C.byref(sc), C.byref(frame.viewport), C.byref(opt)),
                     "st_render_ex")
         return opt
+
+
+def render_batch(renderer, items, tile_shape=-1, chunk=0, use_graph=False, device_outputs=False):
+    """st_render_batch over items = [(slot, SceneData, Frame)]; outputs go to each Frame's buffers
+    (host) unless device_outputs, in which case Frame.grid pointers are used as device pointers."""
+    keep = []
+    views = (st_view * len(items))()
+    for k, (slot, sd, fr) in enumerate(items):
+        sc, kk = sd.to_ctypes()
+        keep += [sc, kk]
+        views[k].slot = slot
+        views[k].scene = C.addressof(sc)
+        views[k].viewport = C.addressof(fr.viewport)
+        views[k].out_float = fr.grid.float_pixels
+        views[k].out_u8 = fr.grid.pixels
+    opt = st_batch_options()
+    opt.tile_shape, opt.chunk, opt.use_graph, opt.device_outputs = tile_shape, chunk, int(use_graph), int(device_outputs)
+    renderer._check(renderer.L.st_render_batch(renderer.ctx, views, len(items), C.byref(opt)), "st_render_batch")
+    return opt
 
 
 def counters_dict(opt):

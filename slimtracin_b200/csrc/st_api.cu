@@ -5,6 +5,10 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <cstdlib>
+#include <fstream>
+#include <map>
+#include <sstream>
 #include "slimtracin_b200.h"
 #include "slimtracin_layout.h"
 #include "st_kernels.h"
@@ -42,8 +46,21 @@ struct SceneSlot {
 
 }  // namespace
 
+struct BatchState {
+    DevBuf table, ssb, seg, out_float, out_u8, counter;
+    BatchView *staging = nullptr;       // pinned host copy of the view table
+    size_t staging_cap = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::string graph_key;
+    std::map<std::string, std::pair<int, int>> tuned;   // scene-class key -> (tile shape, chunk)
+};
+
 struct st_ctx {
     int device = 0;
+    int sm_count = 148;
+    int blocks_per_sm[TILE_SHAPES] = {1, 1, 1, 1};
+    BatchState batch;
     cudaStream_t stream = nullptr;
     uint64_t budget = 0, in_use = 0;
     std::vector<SceneSlot> slots;
@@ -59,6 +76,11 @@ int fail_cuda(st_ctx *ctx, cudaError_t e) {
     ctx->cuda_error = cudaGetErrorString(e);
     return e == cudaErrorMemoryAllocation ? ST_ERR_OUT_OF_MEMORY : ST_ERR_CUDA;
 }
+int ST_CUDA_LAST_impl(st_ctx *ctx) {
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ST_OK : fail_cuda(ctx, e);
+}
+#define ST_CUDA_LAST() ST_CUDA_LAST_impl(ctx)
 int ST_CUDA_SYNC(st_ctx *ctx) {
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
     return e == cudaSuccess ? ST_OK : fail_cuda(ctx, e);
@@ -233,6 +255,14 @@ int st_init(st_ctx **out, const st_config *cfg) {
         delete ctx;
         return ST_ERR_CUDA;
     }
+    cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+    for (int t = 0; t < TILE_SHAPES; t++) ctx->blocks_per_sm[t] = batch_blocks_per_sm(t);
+    if (const char *path = getenv("ST_AUTOTUNE_CACHE")) {
+        std::ifstream f(path);
+        std::string key;
+        int tile, chunk;
+        while (f >> key >> tile >> chunk) ctx->batch.tuned[key] = {tile, chunk};
+    }
     int s = reserve(ctx, ctx->status, 16);
     if (s == ST_OK) s = reserve(ctx, ctx->counters, sizeof(unsigned long long) * 16);
     if (s != ST_OK) {
@@ -251,6 +281,12 @@ void st_shutdown(st_ctx *ctx) {
     for (DevBuf *b : {&ctx->ssb, &ctx->dirs, &ctx->out_float, &ctx->out_u8, &ctx->prim_ids, &ctx->status, &ctx->counters})
         release(ctx, *b);
     lbvh_release(ctx->lbvh);
+    for (DevBuf *b : {&ctx->batch.table, &ctx->batch.ssb, &ctx->batch.seg, &ctx->batch.out_float, &ctx->batch.out_u8,
+                      &ctx->batch.counter})
+        release(ctx, *b);
+    if (ctx->batch.exec) cudaGraphExecDestroy(ctx->batch.exec);
+    if (ctx->batch.graph) cudaGraphDestroy(ctx->batch.graph);
+    if (ctx->batch.staging) cudaFreeHost(ctx->batch.staging);
     for (auto &e : ctx->ev) if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -720,7 +756,7 @@ int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *view
     const size_t grid = (size_t)v.grid_w * v.grid_h;
     const u32t W = v.grid_w - 1, H = v.grid_h - 1;
     ST_TRY(reserve(ctx, ctx->ssb, sizeof(int4) * std::max(S->n_prims, 1u)));
-    ST_TRY(reserve(ctx, ctx->dirs, sizeof(float) * 3 * grid));
+    ST_TRY(reserve(ctx, ctx->dirs, sizeof(float) * ray_rows_floats(v)));
     FloatPixel *host_float = o->out_float ? o->out_float : viewport->frame_buffer->float_pixels;
     Pixel *host_u8 = o->out_u8 ? o->out_u8 : viewport->frame_buffer->pixels;
     FloatPixel *dev_float;
@@ -778,6 +814,233 @@ int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *view
     ST_CUDA(cudaStreamSynchronize(st));
     cudaEventElapsedTime(&o->trace_ms, ctx->ev[1], ctx->ev[2]);
     cudaEventElapsedTime(&o->total_ms, ctx->ev[0], ctx->ev[3]);
+    if (status[0] & S_STACK_OVERFLOW) return ST_ERR_STACK_OVERFLOW;
+    return ST_OK;
+}
+
+// ---- batched views ---------------------------------------------------------------------------
+namespace {
+
+struct BatchPlan {
+    std::vector<BatchView> table;
+    std::vector<size_t> ssb_off, seg_off, float_off, u8_off;   // element offsets into the batch arena
+    std::vector<bool> want_u8;
+    size_t ssb_total = 0, seg_total = 0, float_total = 0, u8_total = 0;
+    u32t total_tiles = 0;
+    uint64_t rays = 0;
+    std::string shape_key, class_key;
+};
+
+int plan_batch(st_ctx *ctx, const st_view *views, int n, int tile, const st_batch_options &o, BatchPlan &p) {
+    u32t tw, th;
+    tile_dims(tile, tw, th);
+    p = BatchPlan();
+    std::ostringstream shape, cls;
+    shape << "t" << tile << "n" << n;
+    for (int i = 0; i < n; i++) {
+        const st_view &V = views[i];
+        SceneSlot *S = slot_of(ctx, V.slot);
+        if (!S || !V.viewport) return ST_ERR_INVALID_ARG;
+        if (!S->allocated || !S->tlas_valid || !S->n_prims) return ST_ERR_NOT_RESIDENT;
+        BatchView b;
+        memset(&b, 0, sizeof(b));
+        ST_TRY(make_view(V.viewport, b.view));
+        b.view.primary_tlas = S->n_prims > 64 ? 1 : 0;
+        b.scene = scene_view(*S, V.scene);
+        b.tiles_x = (b.view.grid_w + tw - 1) / tw;
+        const u32t tiles_y = (b.view.grid_h + th - 1) / th;
+        b.tile_begin = p.total_tiles;
+        p.total_tiles += b.tiles_x * tiles_y;
+        const size_t grid = (size_t)b.view.grid_w * b.view.grid_h;
+        p.ssb_off.push_back(p.ssb_total);
+        p.ssb_total += std::max(S->n_prims, 1u);
+        p.seg_off.push_back(p.seg_total);
+        p.seg_total += ray_rows_floats(b.view);
+        p.float_off.push_back(p.float_total);
+        if (!(o.device_outputs && V.out_float)) p.float_total += grid;
+        const bool u8 = V.out_u8 != nullptr;
+        p.want_u8.push_back(u8);
+        p.u8_off.push_back(p.u8_total);
+        if (u8 && !o.device_outputs) p.u8_total += (size_t)(b.view.grid_w - 1) * (b.view.grid_h - 1);
+        p.rays += grid;
+        p.table.push_back(b);
+        shape << "_" << V.slot << ":" << b.view.grid_w << "x" << b.view.grid_h << "m" << b.view.mode << "d"
+              << b.view.depth << "u" << (V.out_u8 != nullptr);
+        // device outputs are baked into the captured launches; host outputs are copied after them
+        if (o.device_outputs) shape << "o" << (const void *)V.out_float << "/" << (const void *)V.out_u8;
+        // the scene class: primitive and triangle counts (log2 buckets) and the bounce count
+        u32t tris = 0;
+        for (const MeshDev &m : S->mesh_host) tris += m.triangle_count;
+        int pb = 0, tb = 0;
+        for (u32t x = S->n_prims; x > 1; x >>= 1) pb++;
+        for (u32t x = tris; x > 1; x >>= 1) tb++;
+        cls << "p" << pb << "t" << tb << "d" << b.view.depth << ";";
+    }
+    p.shape_key = shape.str();
+    p.class_key = cls.str();
+    return ST_OK;
+}
+
+int enqueue_batch(st_ctx *ctx, const st_view *views, int n, BatchPlan &p, int tile, u32t chunk, cudaStream_t st,
+                  const st_batch_options &o) {
+    BatchState &B = ctx->batch;
+    // per-view pointers into the arena (or the caller's device outputs)
+    for (int i = 0; i < n; i++) {
+        BatchView &b = p.table[i];
+        b.ssb = P<int4>(B.ssb) + p.ssb_off[i];
+        b.dirs = P<float>(B.seg) + p.seg_off[i];
+        b.out = (o.device_outputs && views[i].out_float) ? views[i].out_float : P<FloatPixel>(B.out_float) + p.float_off[i];
+        b.prim_ids = nullptr;
+    }
+    memcpy(B.staging, p.table.data(), sizeof(BatchView) * n);
+    ST_CUDA(cudaMemcpyAsync(B.table.ptr, B.staging, sizeof(BatchView) * n, cudaMemcpyHostToDevice, st));
+    ST_CUDA(cudaMemsetAsync(B.counter.ptr, 0, 16, st));
+    ST_CUDA(cudaMemsetAsync(ctx->status.ptr, 0, 16, st));
+    for (int i = 0; i < n; i++) {
+        BatchView &b = p.table[i];
+        launch_ssb(b.scene, b.view, const_cast<int4 *>(b.ssb), st);
+        launch_ray_rows(b.view, const_cast<float *>(b.dirs), st);
+    }
+    const u32t blocks = (u32t)(ctx->sm_count * ctx->blocks_per_sm[tile]);
+    if (launch_batch(P<BatchView>(B.table), (u32t)n, p.total_tiles, tile, chunk, blocks, P<u32t>(B.counter),
+                     P<unsigned>(ctx->status), P<unsigned long long>(ctx->counters), false, st) != 0)
+        return ST_ERR_INVALID_ARG;
+    for (int i = 0; i < n; i++) {
+        if (!p.want_u8[i]) continue;
+        const BatchView &b = p.table[i];
+        uint32_t *u8 = o.device_outputs ? reinterpret_cast<uint32_t *>(views[i].out_u8) : P<uint32_t>(B.out_u8) + p.u8_off[i];
+        launch_resolve(b.out, b.view.grid_w, b.view.grid_w - 1, b.view.grid_h - 1, u8, st);
+    }
+    return ST_CUDA_LAST();
+}
+
+int batch_reserve(st_ctx *ctx, const BatchPlan &p, int n) {
+    BatchState &B = ctx->batch;
+    ST_TRY(reserve(ctx, B.table, sizeof(BatchView) * n));
+    ST_TRY(reserve(ctx, B.ssb, sizeof(int4) * p.ssb_total));
+    ST_TRY(reserve(ctx, B.seg, sizeof(float) * p.seg_total));
+    ST_TRY(reserve(ctx, B.out_float, sizeof(FloatPixel) * std::max(p.float_total, (size_t)1)));
+    ST_TRY(reserve(ctx, B.out_u8, sizeof(uint32_t) * std::max(p.u8_total, (size_t)1)));
+    ST_TRY(reserve(ctx, B.counter, 16));
+    if (B.staging_cap < (size_t)n) {
+        if (B.staging) cudaFreeHost(B.staging);
+        B.staging = nullptr;
+        B.staging_cap = 0;
+        ST_CUDA(cudaMallocHost((void **)&B.staging, sizeof(BatchView) * n));
+        B.staging_cap = n;
+    }
+    return ST_OK;
+}
+
+}  // namespace
+
+int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *opt) {
+    if (!ctx || !views || n <= 0) return ST_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    st_batch_options dflt;
+    memset(&dflt, 0, sizeof(dflt));
+    dflt.tile_shape = -1;
+    st_batch_options &o = opt ? *opt : dflt;
+    cudaStream_t st = o.stream ? (cudaStream_t)o.stream : ctx->stream;
+    BatchState &B = ctx->batch;
+    // the tile shape and queue chunk: given, cached for this scene class, or tuned now
+    BatchPlan p;
+    int tile = o.tile_shape;
+    u32t chunk = o.chunk > 0 ? (u32t)o.chunk : 0;
+    ST_TRY(plan_batch(ctx, views, n, tile >= 0 ? tile : 0, o, p));
+    if (tile < 0 || chunk == 0) {
+        auto it = B.tuned.find(p.class_key);
+        if (it != B.tuned.end()) {
+            if (tile < 0) tile = it->second.first;
+            if (!chunk) chunk = (u32t)it->second.second;
+        } else {
+            const int shapes[4] = {TILE_8x4, TILE_16x2, TILE_4x8, TILE_32x1};
+            const u32t chunks[2] = {1, 4};
+            float best = INFINITY;
+            int best_tile = TILE_8x4;
+            u32t best_chunk = 1;
+            for (int si = 0; si < 4; si++) {
+                if (tile >= 0 && shapes[si] != tile) continue;
+                for (u32t c : chunks) {
+                    if (chunk && c != chunk) continue;
+                    BatchPlan q;
+                    ST_TRY(plan_batch(ctx, views, n, shapes[si], o, q));
+                    ST_TRY(batch_reserve(ctx, q, n));
+                    ST_CUDA(cudaEventRecord(ctx->ev[0], st));
+                    ST_TRY(enqueue_batch(ctx, views, n, q, shapes[si], c, st, o));
+                    ST_CUDA(cudaEventRecord(ctx->ev[1], st));
+                    ST_CUDA(cudaStreamSynchronize(st));
+                    float ms = 0;
+                    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+                    if (ms < best) { best = ms; best_tile = shapes[si]; best_chunk = c; }
+                }
+            }
+            B.tuned[p.class_key] = {best_tile, (int)best_chunk};
+            if (const char *path = getenv("ST_AUTOTUNE_CACHE")) {
+                std::ofstream f(path, std::ios::app);
+                f << p.class_key << " " << best_tile << " " << best_chunk << "\n";
+            }
+            if (tile < 0) tile = best_tile;
+            if (!chunk) chunk = best_chunk;
+        }
+        ST_TRY(plan_batch(ctx, views, n, tile, o, p));
+    }
+    ST_TRY(batch_reserve(ctx, p, n));
+    o.graph_replayed = 0;
+    ST_CUDA(cudaEventRecord(ctx->ev[0], st));
+    if (o.use_graph) {
+        std::ostringstream key;
+        key << p.shape_key << "c" << chunk << "s" << (const void *)st;
+        if (B.exec && B.graph_key == key.str()) {
+            // same shape: refresh the view table the graph's copy node reads, then replay
+            for (int i = 0; i < n; i++) {
+                BatchView &b = p.table[i];
+                b.ssb = P<int4>(B.ssb) + p.ssb_off[i];
+                b.dirs = P<float>(B.seg) + p.seg_off[i];
+                b.out = (o.device_outputs && views[i].out_float) ? views[i].out_float : P<FloatPixel>(B.out_float) + p.float_off[i];
+                b.prim_ids = nullptr;
+            }
+            memcpy(B.staging, p.table.data(), sizeof(BatchView) * n);
+            ST_CUDA(cudaGraphLaunch(B.exec, st));
+            o.graph_replayed = 1;
+        } else {
+            if (B.exec) { cudaGraphExecDestroy(B.exec); B.exec = nullptr; }
+            if (B.graph) { cudaGraphDestroy(B.graph); B.graph = nullptr; }
+            ST_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            int s = enqueue_batch(ctx, views, n, p, tile, chunk, st, o);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(st, &g);
+            if (s != ST_OK) { if (g) cudaGraphDestroy(g); return s; }
+            if (e != cudaSuccess) return fail_cuda(ctx, e);
+            B.graph = g;
+            ST_CUDA(cudaGraphInstantiate(&B.exec, g, 0));
+            B.graph_key = key.str();
+            ST_CUDA(cudaGraphLaunch(B.exec, st));
+        }
+    } else {
+        ST_TRY(enqueue_batch(ctx, views, n, p, tile, chunk, st, o));
+    }
+    ST_CUDA(cudaEventRecord(ctx->ev[1], st));
+    if (!o.device_outputs) {
+        for (int i = 0; i < n; i++) {
+            const BatchView &b = p.table[i];
+            const size_t grid = (size_t)b.view.grid_w * b.view.grid_h;
+            if (views[i].out_float)
+                ST_CUDA(cudaMemcpyAsync(views[i].out_float, P<FloatPixel>(B.out_float) + p.float_off[i],
+                                        sizeof(FloatPixel) * grid, cudaMemcpyDeviceToHost, st));
+            if (views[i].out_u8)
+                ST_CUDA(cudaMemcpyAsync(views[i].out_u8, P<uint32_t>(B.out_u8) + p.u8_off[i],
+                                        sizeof(uint32_t) * (size_t)(b.view.grid_w - 1) * (b.view.grid_h - 1),
+                                        cudaMemcpyDeviceToHost, st));
+        }
+    }
+    unsigned status[4] = {0, 0, 0, 0};
+    ST_CUDA(cudaMemcpyAsync(status, ctx->status.ptr, 16, cudaMemcpyDeviceToHost, st));
+    ST_CUDA(cudaStreamSynchronize(st));
+    cudaEventElapsedTime(&o.batch_ms, ctx->ev[0], ctx->ev[1]);
+    o.rays = p.rays;
+    o.tile_shape_used = tile;
+    o.chunk_used = (int)chunk;
     if (status[0] & S_STACK_OVERFLOW) return ST_ERR_STACK_OVERFLOW;
     return ST_OK;
 }

@@ -8,6 +8,8 @@ namespace st {
 
 // One view: what rayTrace / renderSceneOnCPU read from the Viewport and its Camera
 // (raytracer.h:136-170) and what computeSSB reads from the frame buffer's Dimensions (SSB.h:5).
+constexpr int kSegment = 8;        // grid points per stored row-segment start (row_segments_kernel)
+
 struct ViewDev {
     v3 cam_pos;
     q4 cam_rot_inv;                 // camera->transform.rotation_inverted
@@ -22,8 +24,27 @@ struct ViewDev {
     int primary_tlas;               // 1: primary rays walk the TLAS (with the SSB cull); 0: brute force
 };
 
+// One view of a batch: the scene it renders, the view, its per-view scratch and outputs, and where
+// its tiles start in the batch's tile numbering.
+struct BatchView {
+    SceneDev scene;
+    ViewDev view;
+    const int4 *ssb;
+    const float *dirs;             // row-segment starts (row_segments_kernel)
+    FloatPixel *out;
+    u32t *prim_ids;
+    u32t tile_begin, tiles_x;
+};
+enum TileShape { TILE_8x4 = 0, TILE_16x2 = 1, TILE_32x1 = 2, TILE_4x8 = 3, TILE_SHAPES = 4 };
+
 void launch_ssb(const SceneDev &S, const ViewDev &v, int4 *ssb, cudaStream_t st);
+int launch_batch(const BatchView *views, u32t n_views, u32t total_tiles, int tile_shape, u32t chunk, u32t grid_blocks,
+                 u32t *tile_counter, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st);
+void tile_dims(int tile_shape, u32t &tw, u32t &th);
+int batch_blocks_per_sm(int tile_shape);
+// Row-segment starts of the view's ray directions: (grid_h x ceil(grid_w / kSegment)) float3.
 void launch_ray_rows(const ViewDev &v, float *dirs, cudaStream_t st);
+inline size_t ray_rows_floats(const ViewDev &v) { return (size_t)v.grid_h * ((v.grid_w + kSegment - 1) / kSegment) * 3; }
 void launch_trace(const SceneDev &S, const ViewDev &v, const int4 *ssb, const float *dirs, FloatPixel *out,
                   u32t *prim_ids, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st);
 void launch_resolve(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out, cudaStream_t st);

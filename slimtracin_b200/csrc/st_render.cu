@@ -535,37 +535,125 @@ __global__ void ssb_kernel(SceneDev S, ViewDev v, int4 *ssb) {
 }
 
 // The reference walks each row of the QCAA grid by repeated addition (raytracer.h:156-170):
-// row y starts at start + down added y times, pixel x at that plus right added x times.  One lane
-// per row keeps that exact sequence; 32 consecutive values per lane go through shared memory so
-// the stores to the (W+1)x(H+1) grid stay coalesced.
-__global__ void ray_rows_kernel(ViewDev v, float *dirs) {
-    __shared__ float tile[32][32 * 3 + 1];
-    const int lane = threadIdx.x;
-    const u32t row = blockIdx.x * 32 + lane;
-    v3 start = v.pp_start;
-    for (u32t y = 0; y < row && y < v.grid_h; y++) start = start + v.pp_down;
-    v3 cur = start;
-    const u32t rows_here = min(32u, v.grid_h - blockIdx.x * 32);
-    for (u32t x0 = 0; x0 < v.grid_w; x0 += 32) {
-        for (int k = 0; k < 32; k++) {
-            tile[lane][3 * k + 0] = cur.x;
-            tile[lane][3 * k + 1] = cur.y;
-            tile[lane][3 * k + 2] = cur.z;
-            cur = cur + v.pp_right;
-        }
-        __syncwarp();
-        const u32t n = min(32u, v.grid_w - x0);
-        for (u32t r = 0; r < rows_here; r++) {
-            float *dst = dirs + ((size_t)(blockIdx.x * 32 + r) * v.grid_w + x0) * 3;
-            for (u32t k = lane; k < 3 * n; k += 32) dst[k] = tile[r][k];
-        }
-        __syncwarp();
+// row y starts at start + down added y times, pixel x at that plus right added x times.  That
+// sequence is kept exactly: one thread per row walks it and stores every kSegment-th value
+// ("segment starts", 3 MB at 1080p instead of a 25 MB direction table); the trace kernel adds
+// `right` the remaining x % kSegment times itself.
+__global__ void row_segments_kernel(ViewDev v, float *seg) {
+    const u32t row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= v.grid_h) return;
+    v3 cur = v.pp_start;
+    for (u32t y = 0; y < row; y++) cur = cur + v.pp_down;
+    const u32t nseg = (v.grid_w + kSegment - 1) / kSegment;
+    float *out = seg + (size_t)row * nseg * 3;
+    for (u32t k = 0; k < nseg; k++) {
+        out[3 * k] = cur.x;
+        out[3 * k + 1] = cur.y;
+        out[3 * k + 2] = cur.z;
+        for (int i = 0; i < kSegment; i++) cur = cur + v.pp_right;
     }
+}
+
+__device__ __forceinline__ v3 grid_direction(const ViewDev &v, const float *seg, u32t x, u32t y) {
+    const u32t nseg = (v.grid_w + kSegment - 1) / kSegment;
+    const float *s = seg + ((size_t)y * nseg + x / kSegment) * 3;
+    v3 cur = V(__ldg(s), __ldg(s + 1), __ldg(s + 2));
+    for (u32t i = 0; i < x % kSegment; i++) cur = cur + v.pp_right;
+    return cur;
 }
 
 // rayTrace render/raytracer.h:81 for one QCAA grid point, writing the FloatPixel the reference's
 // setPixel leaves after beginDrawing's clear (viewport.h:88): hit -> (color, 1, z), miss ->
 // (black, 0, +inf).
+template <bool CNT>
+__device__ __forceinline__ void trace_point(TState<CNT> &t, const SceneDev &S, const ViewDev &v, const int4 *ssb,
+                                            const float *dirs, u32t x, u32t y, FloatPixel *out, u32t *prim_ids) {
+    const size_t idx = (size_t)y * v.grid_w + x;
+    v3 current = grid_direction(v, dirs, x, y);
+    RayD ray;
+    ray.origin = v.cam_pos;
+    ray.direction = norm(current);
+    ray.rcp = rcp(ray.direction);
+    t.depth = v.depth;
+    t.closest.distance = t.closest.distance_squared = INFINITY;
+    t.closest.cone_width = 0;
+    t.mesh_closest.object_type = PrimitiveType_Mesh;
+    t.current.cone_width = 0;
+    t.count(C_PRIMARY);
+    v3 Ro = ray.origin, Rd = ray.direction, color = splat(0);
+    bool lights_shaded = false;
+    bool hit_found;
+    if (v.primary_tlas) {
+        RayD pr = ray;
+        pre_prep(pr);
+        hit_found = trace_scene(t, S, pr, false, ssb, (int)x, (int)y, v.cone_angle, true);
+    } else {
+        hit_found = hit_primitives(t, S, ray, S.tlas_leaf_ids, 0, S.n_prims, false, ssb, (int)x, (int)y, v.cone_angle);
+    }
+    Hit &hit = t.closest;
+    if (prim_ids) prim_ids[idx] = hit_found ? hit.object_id : 0xFFFFFFFFu;
+    float closest_distance = hit_found ? hit.distance : INFINITY;
+    float z = INFINITY;
+    if (hit_found) {
+        z = qrot(hit.position - v.cam_pos, v.cam_rot_inv).z;
+        switch (v.mode) {
+            case RenderMode_Beauty: color = shade_surface(t, S, ray, lights_shaded); break;
+            case RenderMode_Depth: color = splat(4 / hit.distance); break;
+            case RenderMode_Normals: {
+                const Material &M = S.materials[hit.material_id];
+                if (M.texture_count > 1 && (M.use & NORMAL_MAP)) {
+                    float u = hit.u * M.uv_repeat.x, vv = hit.v * M.uv_repeat.y;
+                    hit.uv_area /= M.uv_repeat.x / M.uv_repeat.y;
+                    float du = duv_ray_cone(hit.NdotV, hit.cone_width, hit.area, hit.uv_area);
+                    q4 rot = normal_rotation(sample_normal(t, S, M.texture_ids[1], u, vv, du, 0.0f));
+                    hit.normal = qrot(hit.normal, rot);
+                }
+                color = V(0.5f * (hit.normal.x + 1), 0.5f * (hit.normal.y + 1), 0.5f * (hit.normal.z + 1));
+            } break;
+            case RenderMode_UVs: color = V(0.5f * hit.u, 0.5f * hit.v, 0.5f); break;
+        }
+    }
+    if (v.mode == RenderMode_Beauty && S.lights && !lights_shaded) {
+        if (shade_lights(t, S, Ro, Rd, closest_distance, color)) {
+            hit_found = true;
+            z = t.sphere.closest_distance;
+        }
+    }
+    float4 c01;
+    double depth;
+    if (hit_found) {
+        if (v.mode == RenderMode_Beauty) {
+            color.x = tone_mapped(color.x);
+            color.y = tone_mapped(color.y);
+            color.z = tone_mapped(color.z);
+        }
+        color = vscale(color, 255.0f);
+        color = vmul(color, color);
+        c01 = make_float4(color.x, color.y, color.z, 1.0f);
+        depth = (double)z;
+    } else {
+        c01 = make_float4(0, 0, 0, 0);
+        depth = (double)INFINITY;
+    }
+    float2 *o = reinterpret_cast<float2 *>(out + idx);
+    o[0] = make_float2(c01.x, c01.y);
+    o[1] = make_float2(c01.z, c01.w);
+    reinterpret_cast<double *>(o)[2] = depth;
+}
+
+template <bool CNT>
+__device__ __forceinline__ void flush_counters(TState<CNT> &t, unsigned *status, unsigned long long *counters) {
+    if (t.status) atomicOr(status, t.status);
+    if (CNT) {
+        const u32t lane = threadIdx.x & 31;
+        for (int k = 0; k < C_COUNT; k++) {
+            unsigned long long s = t.cnt[k];
+            for (int off = 16; off; off >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, off);
+            if (lane == 0 && s) atomicAdd(counters + k, s);
+        }
+    }
+}
+
 template <bool CNT>
 __global__ void __launch_bounds__(128) trace_kernel(SceneDev S, ViewDev v, const int4 *ssb, const float *dirs,
                                                     FloatPixel *out, u32t *prim_ids, unsigned *status,
@@ -574,91 +662,44 @@ __global__ void __launch_bounds__(128) trace_kernel(SceneDev S, ViewDev v, const
     // a block covers 16x8 grid points; each warp an 8x4 tile
     const u32t x = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
     const u32t y = blockIdx.y * 8 + (warp >> 1) * 4 + (lane >> 3);
-    const bool active = x < v.grid_w && y < v.grid_h;
     TState<CNT> t;
     t.status = 0;
     if (CNT) for (int k = 0; k < C_COUNT; k++) t.cnt[k] = 0;
-    if (active) {
-        const size_t idx = (size_t)y * v.grid_w + x;
-        v3 current = V(dirs[3 * idx], dirs[3 * idx + 1], dirs[3 * idx + 2]);
-        RayD ray;
-        ray.origin = v.cam_pos;
-        ray.direction = norm(current);
-        ray.rcp = rcp(ray.direction);
-        t.depth = v.depth;
-        t.closest.distance = t.closest.distance_squared = INFINITY;
-        t.closest.cone_width = 0;
-        t.mesh_closest.object_type = PrimitiveType_Mesh;
-        t.current.cone_width = 0;
-        t.count(C_PRIMARY);
-        v3 Ro = ray.origin, Rd = ray.direction, color = splat(0);
-        bool lights_shaded = false;
-        bool hit_found;
-        if (v.primary_tlas) {
-            RayD pr = ray;
-            pre_prep(pr);
-            hit_found = trace_scene(t, S, pr, false, ssb, (int)x, (int)y, v.cone_angle, true);
-        } else {
-            hit_found = hit_primitives(t, S, ray, S.tlas_leaf_ids, 0, S.n_prims, false, ssb, (int)x, (int)y, v.cone_angle);
-        }
-        Hit &hit = t.closest;
-        if (prim_ids) prim_ids[idx] = hit_found ? hit.object_id : 0xFFFFFFFFu;
-        float closest_distance = hit_found ? hit.distance : INFINITY;
-        float z = INFINITY;
-        if (hit_found) {
-            z = qrot(hit.position - v.cam_pos, v.cam_rot_inv).z;
-            switch (v.mode) {
-                case RenderMode_Beauty: color = shade_surface(t, S, ray, lights_shaded); break;
-                case RenderMode_Depth: color = splat(4 / hit.distance); break;
-                case RenderMode_Normals: {
-                    const Material &M = S.materials[hit.material_id];
-                    if (M.texture_count > 1 && (M.use & NORMAL_MAP)) {
-                        float u = hit.u * M.uv_repeat.x, vv = hit.v * M.uv_repeat.y;
-                        hit.uv_area /= M.uv_repeat.x / M.uv_repeat.y;
-                        float du = duv_ray_cone(hit.NdotV, hit.cone_width, hit.area, hit.uv_area);
-                        q4 rot = normal_rotation(sample_normal(t, S, M.texture_ids[1], u, vv, du, 0.0f));
-                        hit.normal = qrot(hit.normal, rot);
-                    }
-                    color = V(0.5f * (hit.normal.x + 1), 0.5f * (hit.normal.y + 1), 0.5f * (hit.normal.z + 1));
-                } break;
-                case RenderMode_UVs: color = V(0.5f * hit.u, 0.5f * hit.v, 0.5f); break;
-            }
-        }
-        if (v.mode == RenderMode_Beauty && S.lights && !lights_shaded) {
-            if (shade_lights(t, S, Ro, Rd, closest_distance, color)) {
-                hit_found = true;
-                z = t.sphere.closest_distance;
-            }
-        }
-        float4 c01;
-        double depth;
-        if (hit_found) {
-            if (v.mode == RenderMode_Beauty) {
-                color.x = tone_mapped(color.x);
-                color.y = tone_mapped(color.y);
-                color.z = tone_mapped(color.z);
-            }
-            color = vscale(color, 255.0f);
-            color = vmul(color, color);
-            c01 = make_float4(color.x, color.y, color.z, 1.0f);
-            depth = (double)z;
-        } else {
-            c01 = make_float4(0, 0, 0, 0);
-            depth = (double)INFINITY;
-        }
-        float2 *o = reinterpret_cast<float2 *>(out + idx);
-        o[0] = make_float2(c01.x, c01.y);
-        o[1] = make_float2(c01.z, c01.w);
-        reinterpret_cast<double *>(o)[2] = depth;
-    }
-    if (t.status) atomicOr(status, t.status);
-    if (CNT) {
-        for (int k = 0; k < C_COUNT; k++) {
-            unsigned long long s = t.cnt[k];
-            for (int off = 16; off; off >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, off);
-            if (lane == 0 && s) atomicAdd(counters + k, s);
+    if (x < v.grid_w && y < v.grid_h) trace_point(t, S, v, ssb, dirs, x, y, out, prim_ids);
+    flush_counters(t, status, counters);
+}
+
+// ---- batched views: one persistent launch over the tiles of many views ------------------------
+// Every view is cut into tiles of tile_w x tile_h grid points (one warp per tile when the tile has
+// 32 points); warps take tiles from one global counter, `chunk` tiles at a time, so views of
+// different sizes, scenes and bounce counts share the launch and no warp idles while work is left.
+template <bool CNT, int TW, int TH>
+__global__ void __launch_bounds__(128) batch_kernel(const BatchView *views, u32t n_views, u32t total_tiles, u32t chunk,
+                                                    u32t *tile_counter, unsigned *status, unsigned long long *counters) {
+    static_assert(TW * TH == 32, "one warp per tile");
+    const u32t lane = threadIdx.x & 31;
+    TState<CNT> t;
+    t.status = 0;
+    if (CNT) for (int k = 0; k < C_COUNT; k++) t.cnt[k] = 0;
+    for (;;) {
+        u32t first = 0;
+        if (lane == 0) first = atomicAdd(tile_counter, chunk);
+        first = __shfl_sync(0xFFFFFFFFu, first, 0);
+        if (first >= total_tiles) break;
+        const u32t last = min(first + chunk, total_tiles);
+        for (u32t tile = first; tile < last; tile++) {
+            // the view owning this tile: views are few, a linear search over their tile offsets
+            u32t vi = 0;
+            while (vi + 1 < n_views && views[vi + 1].tile_begin <= tile) vi++;
+            const BatchView &B = views[vi];
+            const u32t local = tile - B.tile_begin;
+            const u32t tx = local % B.tiles_x, ty = local / B.tiles_x;
+            const u32t x = tx * TW + (lane % TW), y = ty * TH + (lane / TW);
+            if (x < B.view.grid_w && y < B.view.grid_h)
+                trace_point(t, B.scene, B.view, B.ssb, B.dirs, x, y, B.out, B.prim_ids);
         }
     }
+    flush_counters(t, status, counters);
 }
 
 // drawViewportToWindowContent viewport/viewport.h:12 (QCAA branch): the 2x2 corners' colour times
@@ -689,13 +730,44 @@ void launch_ssb(const SceneDev &S, const ViewDev &v, int4 *ssb, cudaStream_t st)
     ssb_kernel<<<(S.n_prims + 127) / 128, 128, 0, st>>>(S, v, ssb);
 }
 void launch_ray_rows(const ViewDev &v, float *dirs, cudaStream_t st) {
-    ray_rows_kernel<<<(v.grid_h + 31) / 32, 32, 0, st>>>(v, dirs);
+    row_segments_kernel<<<(v.grid_h + 63) / 64, 64, 0, st>>>(v, dirs);
 }
 void launch_trace(const SceneDev &S, const ViewDev &v, const int4 *ssb, const float *dirs, FloatPixel *out,
                   u32t *prim_ids, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st) {
     dim3 grid((v.grid_w + 15) / 16, (v.grid_h + 7) / 8);
     if (count) trace_kernel<true><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters);
     else trace_kernel<false><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters);
+}
+int launch_batch(const BatchView *views, u32t n_views, u32t total_tiles, int tile_shape, u32t chunk, u32t grid_blocks,
+                 u32t *tile_counter, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st) {
+#define ST_BATCH(TW, TH) (count ? (batch_kernel<true, TW, TH><<<grid_blocks, 128, 0, st>>>(views, n_views, total_tiles, chunk, tile_counter, status, counters), 0) \
+                               : (batch_kernel<false, TW, TH><<<grid_blocks, 128, 0, st>>>(views, n_views, total_tiles, chunk, tile_counter, status, counters), 0))
+    switch (tile_shape) {
+        case TILE_8x4: return ST_BATCH(8, 4);
+        case TILE_16x2: return ST_BATCH(16, 2);
+        case TILE_32x1: return ST_BATCH(32, 1);
+        case TILE_4x8: return ST_BATCH(4, 8);
+    }
+#undef ST_BATCH
+    return -1;
+}
+int batch_blocks_per_sm(int tile_shape) {
+    int n = 0;
+    switch (tile_shape) {
+        case TILE_16x2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<false, 16, 2>, 128, 0); break;
+        case TILE_32x1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<false, 32, 1>, 128, 0); break;
+        case TILE_4x8: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<false, 4, 8>, 128, 0); break;
+        default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<false, 8, 4>, 128, 0); break;
+    }
+    return n > 0 ? n : 1;
+}
+void tile_dims(int tile_shape, u32t &tw, u32t &th) {
+    switch (tile_shape) {
+        case TILE_16x2: tw = 16; th = 2; return;
+        case TILE_32x1: tw = 32; th = 1; return;
+        case TILE_4x8: tw = 4; th = 8; return;
+        default: tw = 8; th = 4; return;
+    }
 }
 void launch_resolve(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out, cudaStream_t st) {
     dim3 grid((width + 127) / 128, height);

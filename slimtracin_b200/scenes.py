@@ -550,11 +550,11 @@ def value_noise3(p, rng_seed, frequency=4.0, octaves=3):
     return out / norm * 2 - 1
 
 
-def displaced_icosphere(subdivisions, seed, amplitude=0.1):
+def displaced_icosphere(subdivisions, seed, amplitude=0.1, radius=1.0):
     """Icosphere with vertices displaced along the normal by value noise; area-weighted vertex
     normals; spherical UVs; centred on its AABB like obj2mesh does (obj2mesh.c:25)."""
     v, f = icosphere(subdivisions)
-    v = v * (1.0 + amplitude * value_noise3(v, seed))[:, None]
+    v = radius * v * (1.0 + amplitude * value_noise3(v, seed))[:, None]
     e1 = v[f[:, 1]] - v[f[:, 0]]
     e2 = v[f[:, 2]] - v[f[:, 0]]
     fn = np.cross(e1, e2)  # length = 2 * area: area weighting
@@ -667,10 +667,12 @@ def bake_texture(rgb, wrap=True, mipmap=True):
     return TextureData(width, height, wrap, mipmap, mips)
 
 
-def config1(seed_offset=0, subdivisions=8, texture_size=1024, instances=8):
-    """The 1080p PBR mesh scene (sizes at the defaults)."""
+def config1(seed_offset=0, subdivisions=8, texture_size=1024, instances=8, radius=2.5):
+    """The 1080p PBR mesh scene (sizes at the defaults).  The icosphere has radius 2.5 and the camera
+    frames the instances (about 42% of primary rays hit, 27% a mesh instance at 1080p); neither is
+    fixed by the benchmark's description."""
     rng = PCG32(0x5EED0000 + 1 + seed_offset)
-    mesh = displaced_icosphere(subdivisions, seed=rng.next_u32())
+    mesh = displaced_icosphere(subdivisions, seed=rng.next_u32(), radius=radius)
     n_prims = instances + 2
     prims = default_primitives(n_prims)
     for i in range(instances):
@@ -725,7 +727,7 @@ def config1(seed_offset=0, subdivisions=8, texture_size=1024, instances=8):
     textures = [bake_texture(albedo, True, True), bake_texture(normal, True, True)]
     sd = SceneData(prims, mats, default_lights(0), ambient=(0.004, 0.004, 0.007),
                    meshes=[mesh], textures=textures, name="config1")
-    cam = look_at((0.0, 9.0, -21.0), (0.0, 1.5, 0.0))
+    cam = look_at((0.0, 8.0, -15.0), (0.0, 1.5, 0.0))
     return sd, cam
 
 

@@ -238,3 +238,31 @@ def test_binned_sah_tlas_and_blas_render(renderer):
     g = H.gpu_frame(renderer, 10, sd1, cam1, 320, 180, depth=4)
     o = H.oracle_frame(sd1, cam1, 320, 180, depth=4)
     H.assert_parity(H.compare(g, o, S.RM_BEAUTY), S.RM_BEAUTY)
+
+
+def test_batch_equals_per_frame_renders(renderer):
+    """st_render_batch over views of different scenes, sizes, modes and bounce counts: every view's
+    float grid and u8 frame equal the per-frame render's, for every tile shape, with and without
+    the CUDA graph (the second graph call replays the captured graph)."""
+    c0, cam0 = scenes.config0()
+    H.tlas_sah(c0)
+    renderer.upload(11, c0, tlas="host")
+    c1, cam1 = H.small_config1(subdivisions=3, texture_size=64, blas="orc")
+    H.tlas_sah(c1)
+    renderer.upload(12, c1, tlas="host")
+    c2, cam2 = scenes.config2(count=300)
+    H.tlas_sah(c2)
+    renderer.upload(13, c2, tlas="host")
+    specs = [(11, c0, cam0, 96, 64, 2, S.RM_BEAUTY), (12, c1, cam1, 160, 90, 4, S.RM_BEAUTY),
+             (13, c2, cam2, 64, 48, 1, S.RM_BEAUTY), (12, c1, cam1, 80, 60, 6, S.RM_NORMALS),
+             (11, c0, cam0, 33, 17, 3, S.RM_DEPTH)]
+    singles = [H.gpu_frame(renderer, slot, sd, cam, w, h, depth=d, mode=m) for slot, sd, cam, w, h, d, m in specs]
+    for tile in (0, 1, 2, 3, -1):
+        for graph in (False, True, True):
+            frames = [scenes.Frame(w, h, cam, depth=d, mode=m) for slot, sd, cam, w, h, d, m in specs]
+            opt = api.render_batch(renderer, [(sp[0], sp[1], fr) for sp, fr in zip(specs, frames)],
+                                   tile_shape=tile, use_graph=graph)
+            for a, b in zip(frames, singles):
+                assert np.array_equal(a.float_pixels.view(np.uint8), b.float_pixels.view(np.uint8)), (tile, graph)
+                assert np.array_equal(a.pixels.view(np.uint8), b.pixels.view(np.uint8))
+            assert opt.rays == sum(fr.rays for fr in frames)
