@@ -179,6 +179,52 @@ typedef struct st_batch_options {
  * viewport per renderScene call (raytracer.h:302); each view's output equals st_render_ex's. */
 ST_API int st_render_batch(st_ctx *ctx, const st_view *views, int view_count, st_batch_options *options);
 
+/* ---- serving: continuous batching of render requests ---------------------------------------------
+ * A worker thread inside the library takes submitted requests in order, admits them while the
+ * device-memory budget for in-flight frame/ray buffers allows, applies their transform updates,
+ * refits (few moved primitives) or rebuilds (many) the TLAS of exactly the scenes that changed,
+ * and launches each batch with the persistent multi-view kernel on one of `max_in_flight` streams,
+ * so requests that arrive while other batches run are launched beside them.  A request never
+ * shares a batch with a request that changes its scene after it, so every result equals the
+ * result of the same request rendered alone after the same sequence of updates.
+ * While serving, only st_submit / st_poll / st_wait / st_serve_stop may be called on the context
+ * (from any one host thread); the scenes must already be resident.  No reference counterpart. */
+typedef struct st_serve_config {
+    int max_in_flight;          /* batches on the device at once; 0 -> 3 */
+    int max_views_per_batch;    /* 0 -> 64 */
+    uint64_t frame_budget;      /* device bytes for in-flight frame/ray buffers; 0 -> budget - resident scenes */
+    int tile_shape, chunk;      /* -1 / 0: the autotuned choice for the scene class, else 8x4 and 1 */
+    double refit_fraction;      /* moved/total below which the TLAS is refit, else rebuilt (LBVH30); 0 -> 0.25 */
+} st_serve_config;
+
+typedef struct st_request {
+    st_view view;               /* host outputs; they must stay valid until the request completes */
+    const Primitive *moved;     /* transform updates applied before this view renders (copied at submit) */
+    const uint32_t *moved_ids;
+    uint32_t moved_count;
+    double arrival_time;        /* carried to the result; use st_clock() for the library's clock */
+} st_request;
+
+typedef struct st_result {
+    int status;                 /* ST_OK, or the error that failed the request */
+    double arrival_time, launch_time, completion_time;   /* st_clock() seconds */
+    uint64_t rays;
+    int batch_size;             /* requests in the batch that rendered it */
+} st_result;
+
+typedef uint64_t st_ticket;
+
+ST_API int st_serve_start(st_ctx *ctx, const st_serve_config *config);
+ST_API int st_submit(st_ctx *ctx, const st_request *request, st_ticket *ticket);
+/* ST_OK with *result filled once the request has completed (the ticket is then released),
+ * ST_ERR_NOT_READY before that, ST_ERR_INVALID_ARG for an unknown ticket. */
+ST_API int st_poll(st_ctx *ctx, st_ticket ticket, st_result *result);
+ST_API int st_wait(st_ctx *ctx, st_ticket ticket, st_result *result, double timeout_s);
+/* Finish every submitted request, then stop the worker. */
+ST_API int st_serve_stop(st_ctx *ctx);
+/* The library's steady clock, in seconds. */
+ST_API double st_clock(void);
+
 #ifdef __cplusplus
 }
 #endif

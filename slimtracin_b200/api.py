@@ -44,6 +44,24 @@ class st_batch_options(C.Structure):
                 ("tile_shape_used", C.c_int), ("chunk_used", C.c_int), ("graph_replayed", C.c_int)]
 
 
+class st_serve_config(C.Structure):
+    _fields_ = [("max_in_flight", C.c_int), ("max_views_per_batch", C.c_int), ("frame_budget", C.c_uint64),
+                ("tile_shape", C.c_int), ("chunk", C.c_int), ("refit_fraction", C.c_double)]
+
+
+class st_request(C.Structure):
+    _fields_ = [("view", st_view), ("moved", C.c_void_p), ("moved_ids", C.c_void_p), ("moved_count", C.c_uint32),
+                ("arrival_time", C.c_double)]
+
+
+class st_result(C.Structure):
+    _fields_ = [("status", C.c_int), ("arrival_time", C.c_double), ("launch_time", C.c_double),
+                ("completion_time", C.c_double), ("rays", C.c_uint64), ("batch_size", C.c_int)]
+
+
+ST_ERR_NOT_READY, ST_ERR_TIMEOUT = 11, 7
+
+
 class STError(RuntimeError):
     def __init__(self, status, what, detail=""):
         self.status = status
@@ -84,6 +102,12 @@ def lib():
             "st_build_bvh": (i, [vp, i, vp, u32, u32, vp, vp, vp, vp]),
             "st_render_ex": (i, [vp, i, vp, vp, C.POINTER(st_render_options)]),
             "st_render_batch": (i, [vp, vp, i, C.POINTER(st_batch_options)]),
+            "st_serve_start": (i, [vp, C.POINTER(st_serve_config)]),
+            "st_submit": (i, [vp, C.POINTER(st_request), C.POINTER(u64)]),
+            "st_poll": (i, [vp, u64, C.POINTER(st_result)]),
+            "st_wait": (i, [vp, u64, C.POINTER(st_result), C.c_double]),
+            "st_serve_stop": (i, [vp]),
+            "st_clock": (C.c_double, []),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -231,3 +255,66 @@ def render_batch(renderer, items, tile_shape=-1, chunk=0, use_graph=False, devic
 
 def counters_dict(opt):
     return {k: int(opt.counters[i]) for i, k in enumerate(COUNTER_NAMES)}
+
+
+class Server:
+    """The serving loop of a Renderer (st_serve_start .. st_serve_stop): requests are views of resident
+    scenes, optionally carrying transform updates that apply before the view renders.  While it runs,
+    the Renderer takes no other calls."""
+
+    def __init__(self, renderer, max_in_flight=3, max_views_per_batch=64, frame_budget=0, tile_shape=-1, chunk=0,
+                 refit_fraction=0.25):
+        self.r = renderer
+        self.L = renderer.L
+        cfg = st_serve_config(max_in_flight, max_views_per_batch, frame_budget, tile_shape, chunk, refit_fraction)
+        renderer._check(self.L.st_serve_start(renderer.ctx, C.byref(cfg)), "st_serve_start")
+        self._keep = {}
+        self.running = True
+
+    def submit(self, slot, sd, frame, moved=None, moved_ids=None, arrival_time=None):
+        """Queue a view; `moved` (PRIMITIVE_DT records) replaces primitives `moved_ids` before it renders.
+        The frame's host buffers receive the outputs; they stay referenced until the request completes."""
+        sc, kk = sd.to_ctypes()
+        req = st_request()
+        req.view.slot = slot
+        req.view.scene = C.addressof(sc)
+        req.view.viewport = C.addressof(frame.viewport)
+        req.view.out_float = frame.grid.float_pixels
+        req.view.out_u8 = frame.grid.pixels
+        keep = [sc, kk, frame]
+        if moved is not None and len(moved):
+            arr = np.ascontiguousarray(moved, dtype=S.PRIMITIVE_DT)
+            ids = np.ascontiguousarray(moved_ids, dtype=np.uint32)
+            req.moved, req.moved_ids, req.moved_count = arr.ctypes.data, ids.ctypes.data, len(ids)
+            keep += [arr, ids]
+        req.arrival_time = self.L.st_clock() if arrival_time is None else arrival_time
+        t = C.c_uint64()
+        self.r._check(self.L.st_submit(self.r.ctx, C.byref(req), C.byref(t)), "st_submit")
+        self._keep[t.value] = keep
+        return t.value
+
+    def poll(self, ticket):
+        """The st_result of a finished request, or None while it is still running."""
+        res = st_result()
+        s = self.L.st_poll(self.r.ctx, ticket, C.byref(res))
+        if s == ST_ERR_NOT_READY:
+            return None
+        self.r._check(s, "st_poll")
+        self._keep.pop(ticket, None)
+        return res
+
+    def wait(self, ticket, timeout=60.0):
+        res = st_result()
+        self.r._check(self.L.st_wait(self.r.ctx, ticket, C.byref(res), float(timeout)), "st_wait")
+        self._keep.pop(ticket, None)
+        return res
+
+    def stop(self):
+        if self.running:
+            self.r._check(self.L.st_serve_stop(self.r.ctx), "st_serve_stop")
+            self.running = False
+            self._keep.clear()
+
+
+def clock():
+    return lib().st_clock()

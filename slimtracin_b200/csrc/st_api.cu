@@ -9,6 +9,13 @@
 #include <fstream>
 #include <map>
 #include <sstream>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <set>
+#include <thread>
 #include "slimtracin_b200.h"
 #include "slimtracin_layout.h"
 #include "st_kernels.h"
@@ -56,8 +63,54 @@ struct BatchState {
     std::map<std::string, std::pair<int, int>> tuned;   // scene-class key -> (tile shape, chunk)
 };
 
+struct ServeReq {
+    uint64_t id = 0;
+    int slot = 0;
+    ViewDev view{};
+    bool has_scene_values = false;
+    vec3 ambient{};
+    bool lights_present = false;
+    FloatPixel *out_float = nullptr;
+    Pixel *out_u8 = nullptr;
+    std::vector<Primitive> moved;
+    std::vector<uint32_t> moved_ids;
+    double arrival = 0, launch = 0, done = 0;
+    int status = ST_ERR_NOT_READY;
+    uint64_t rays = 0;
+    int batch_size = 0;
+    size_t dev_float = 0, dev_ssb = 0, dev_seg = 0, dev_u8 = 0;   // byte offsets in the batch's device arena
+    size_t host_float = 0, host_u8 = 0;                           // byte offsets in the flight's pinned staging
+};
+
+struct InFlight {
+    bool busy = false;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done_ev = nullptr;
+    BatchState B;
+    DevBuf status;
+    char *pinned = nullptr;            // host staging of the batch's outputs and status word
+    size_t pinned_cap = 0;
+    size_t bytes = 0;                  // device bytes this batch holds against the frame budget
+    std::vector<std::shared_ptr<ServeReq>> reqs;
+    std::set<int> scenes;
+};
+
+struct Server {
+    std::thread worker;
+    std::mutex m;
+    std::condition_variable cv_work, cv_done;
+    bool running = false, stop = false;
+    std::deque<std::shared_ptr<ServeReq>> pending;
+    std::map<uint64_t, std::shared_ptr<ServeReq>> tickets;
+    std::vector<InFlight> flights;
+    st_serve_config cfg{};
+    uint64_t frame_budget = 0, inflight_bytes = 0;
+    uint64_t next_id = 1;
+};
+
 struct st_ctx {
     int device = 0;
+    Server server;
     int sm_count = 148;
     int blocks_per_sm[TILE_SHAPES] = {1, 1, 1, 1};
     BatchState batch;
@@ -275,6 +328,7 @@ int st_init(st_ctx **out, const st_config *cfg) {
 
 void st_shutdown(st_ctx *ctx) {
     if (!ctx) return;
+    st_serve_stop(ctx);
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (int i = 0; i < (int)ctx->slots.size(); i++) st_free_scene(ctx, i);
@@ -881,9 +935,8 @@ int plan_batch(st_ctx *ctx, const st_view *views, int n, int tile, const st_batc
     return ST_OK;
 }
 
-int enqueue_batch(st_ctx *ctx, const st_view *views, int n, BatchPlan &p, int tile, u32t chunk, cudaStream_t st,
-                  const st_batch_options &o) {
-    BatchState &B = ctx->batch;
+int enqueue_batch(st_ctx *ctx, BatchState &B, unsigned *status, const st_view *views, int n, BatchPlan &p, int tile,
+                  u32t chunk, cudaStream_t st, const st_batch_options &o) {
     // per-view pointers into the arena (or the caller's device outputs)
     for (int i = 0; i < n; i++) {
         BatchView &b = p.table[i];
@@ -895,7 +948,7 @@ int enqueue_batch(st_ctx *ctx, const st_view *views, int n, BatchPlan &p, int ti
     memcpy(B.staging, p.table.data(), sizeof(BatchView) * n);
     ST_CUDA(cudaMemcpyAsync(B.table.ptr, B.staging, sizeof(BatchView) * n, cudaMemcpyHostToDevice, st));
     ST_CUDA(cudaMemsetAsync(B.counter.ptr, 0, 16, st));
-    ST_CUDA(cudaMemsetAsync(ctx->status.ptr, 0, 16, st));
+    ST_CUDA(cudaMemsetAsync(status, 0, 16, st));
     for (int i = 0; i < n; i++) {
         BatchView &b = p.table[i];
         launch_ssb(b.scene, b.view, const_cast<int4 *>(b.ssb), st);
@@ -903,7 +956,7 @@ int enqueue_batch(st_ctx *ctx, const st_view *views, int n, BatchPlan &p, int ti
     }
     const u32t blocks = (u32t)(ctx->sm_count * ctx->blocks_per_sm[tile]);
     if (launch_batch(P<BatchView>(B.table), (u32t)n, p.total_tiles, tile, chunk, blocks, P<u32t>(B.counter),
-                     P<unsigned>(ctx->status), P<unsigned long long>(ctx->counters), false, st) != 0)
+                     status, P<unsigned long long>(ctx->counters), false, st) != 0)
         return ST_ERR_INVALID_ARG;
     for (int i = 0; i < n; i++) {
         if (!p.want_u8[i]) continue;
@@ -914,8 +967,7 @@ int enqueue_batch(st_ctx *ctx, const st_view *views, int n, BatchPlan &p, int ti
     return ST_CUDA_LAST();
 }
 
-int batch_reserve(st_ctx *ctx, const BatchPlan &p, int n) {
-    BatchState &B = ctx->batch;
+int batch_reserve(st_ctx *ctx, BatchState &B, const BatchPlan &p, int n) {
     ST_TRY(reserve(ctx, B.table, sizeof(BatchView) * n));
     ST_TRY(reserve(ctx, B.ssb, sizeof(int4) * p.ssb_total));
     ST_TRY(reserve(ctx, B.seg, sizeof(float) * p.seg_total));
@@ -965,9 +1017,9 @@ int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *
                     if (chunk && c != chunk) continue;
                     BatchPlan q;
                     ST_TRY(plan_batch(ctx, views, n, shapes[si], o, q));
-                    ST_TRY(batch_reserve(ctx, q, n));
+                    ST_TRY(batch_reserve(ctx, B, q, n));
                     ST_CUDA(cudaEventRecord(ctx->ev[0], st));
-                    ST_TRY(enqueue_batch(ctx, views, n, q, shapes[si], c, st, o));
+                    ST_TRY(enqueue_batch(ctx, B, P<unsigned>(ctx->status), views, n, q, shapes[si], c, st, o));
                     ST_CUDA(cudaEventRecord(ctx->ev[1], st));
                     ST_CUDA(cudaStreamSynchronize(st));
                     float ms = 0;
@@ -985,7 +1037,7 @@ int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *
         }
         ST_TRY(plan_batch(ctx, views, n, tile, o, p));
     }
-    ST_TRY(batch_reserve(ctx, p, n));
+    ST_TRY(batch_reserve(ctx, B, p, n));
     o.graph_replayed = 0;
     ST_CUDA(cudaEventRecord(ctx->ev[0], st));
     if (o.use_graph) {
@@ -1007,7 +1059,7 @@ int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *
             if (B.exec) { cudaGraphExecDestroy(B.exec); B.exec = nullptr; }
             if (B.graph) { cudaGraphDestroy(B.graph); B.graph = nullptr; }
             ST_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            int s = enqueue_batch(ctx, views, n, p, tile, chunk, st, o);
+            int s = enqueue_batch(ctx, B, P<unsigned>(ctx->status), views, n, p, tile, chunk, st, o);
             cudaGraph_t g = nullptr;
             cudaError_t e = cudaStreamEndCapture(st, &g);
             if (s != ST_OK) { if (g) cudaGraphDestroy(g); return s; }
@@ -1018,7 +1070,7 @@ int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *
             ST_CUDA(cudaGraphLaunch(B.exec, st));
         }
     } else {
-        ST_TRY(enqueue_batch(ctx, views, n, p, tile, chunk, st, o));
+        ST_TRY(enqueue_batch(ctx, B, P<unsigned>(ctx->status), views, n, p, tile, chunk, st, o));
     }
     ST_CUDA(cudaEventRecord(ctx->ev[1], st));
     if (!o.device_outputs) {
@@ -1052,4 +1104,379 @@ int st_render_scene(st_ctx *ctx, int slot, const Scene *scene, Viewport *viewpor
     return st_render_ex(ctx, slot, scene, viewport, &o);
 }
 
+// ---- serving ---------------------------------------------------------------------------------
+double st_clock(void) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 }  // extern "C"
+
+namespace {
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+size_t request_bytes(const ServeReq &r, u32t n_prims) {
+    const size_t grid = (size_t)r.view.grid_w * r.view.grid_h;
+    size_t b = align256(sizeof(FloatPixel) * grid) + align256(sizeof(int4) * std::max(n_prims, 1u)) +
+               align256(sizeof(float) * ray_rows_floats(r.view));
+    if (r.out_u8) b += align256(sizeof(uint32_t) * (size_t)(r.view.grid_w - 1) * (r.view.grid_h - 1));
+    return b;
+}
+
+// Copy a finished batch's outputs to the requests' buffers and complete them.
+void finish_flight(st_ctx *ctx, InFlight &F) {
+    Server &V = ctx->server;
+    const unsigned status = *reinterpret_cast<unsigned *>(F.pinned);
+    const double now = st_clock();
+    for (auto &r : F.reqs) {
+        const size_t grid = (size_t)r->view.grid_w * r->view.grid_h;
+        if (r->out_float) memcpy(r->out_float, F.pinned + r->host_float, sizeof(FloatPixel) * grid);
+        if (r->out_u8) memcpy(r->out_u8, F.pinned + r->host_u8, sizeof(uint32_t) * (size_t)(r->view.grid_w - 1) * (r->view.grid_h - 1));
+    }
+    std::lock_guard<std::mutex> lk(V.m);
+    for (auto &r : F.reqs) {
+        r->done = now;
+        r->status = (status & S_STACK_OVERFLOW) ? ST_ERR_STACK_OVERFLOW : ST_OK;
+    }
+    V.inflight_bytes -= F.bytes;
+    F.reqs.clear();
+    F.scenes.clear();
+    F.busy = false;
+    V.cv_done.notify_all();
+}
+
+// Enqueue one admitted batch on its flight's stream: view table, per-view SSB and ray rows, the
+// persistent tile-queue kernel, resolves, and the copies of every output into pinned staging.
+int enqueue_flight(st_ctx *ctx, InFlight &F, BatchPlan &p, std::vector<std::shared_ptr<ServeReq>> &reqs, int tile,
+                   u32t chunk, char *arena) {
+    const int n = (int)reqs.size();
+    cudaStream_t st = F.stream;
+    for (int i = 0; i < n; i++) {
+        BatchView &b = p.table[i];
+        b.out = reinterpret_cast<FloatPixel *>(arena + reqs[i]->dev_float);
+        b.ssb = reinterpret_cast<int4 *>(arena + reqs[i]->dev_ssb);
+        b.dirs = reinterpret_cast<float *>(arena + reqs[i]->dev_seg);
+        b.prim_ids = nullptr;
+    }
+    memcpy(F.B.staging, p.table.data(), sizeof(BatchView) * n);
+    ST_CUDA(cudaMemcpyAsync(F.B.table.ptr, F.B.staging, sizeof(BatchView) * n, cudaMemcpyHostToDevice, st));
+    ST_CUDA(cudaMemsetAsync(F.B.counter.ptr, 0, 16, st));
+    ST_CUDA(cudaMemsetAsync(F.status.ptr, 0, 16, st));
+    for (int i = 0; i < n; i++) {
+        launch_ssb(p.table[i].scene, p.table[i].view, const_cast<int4 *>(p.table[i].ssb), st);
+        launch_ray_rows(p.table[i].view, const_cast<float *>(p.table[i].dirs), st);
+    }
+    const u32t blocks = (u32t)(ctx->sm_count * ctx->blocks_per_sm[tile]);
+    if (launch_batch(P<BatchView>(F.B.table), (u32t)n, p.total_tiles, tile, chunk, blocks, P<u32t>(F.B.counter),
+                     P<unsigned>(F.status), P<unsigned long long>(ctx->counters), false, st) != 0)
+        return ST_ERR_INVALID_ARG;
+    for (int i = 0; i < n; i++) {
+        const ServeReq &r = *reqs[i];
+        const BatchView &b = p.table[i];
+        const size_t grid = (size_t)b.view.grid_w * b.view.grid_h;
+        if (r.out_u8) {
+            uint32_t *u8 = reinterpret_cast<uint32_t *>(arena + r.dev_u8);
+            launch_resolve(b.out, b.view.grid_w, b.view.grid_w - 1, b.view.grid_h - 1, u8, st);
+            ST_CUDA(cudaMemcpyAsync(F.pinned + r.host_u8, u8, (size_t)(b.view.grid_w - 1) * (b.view.grid_h - 1) * 4,
+                                    cudaMemcpyDeviceToHost, st));
+        }
+        if (r.out_float)
+            ST_CUDA(cudaMemcpyAsync(F.pinned + r.host_float, b.out, sizeof(FloatPixel) * grid, cudaMemcpyDeviceToHost, st));
+    }
+    ST_CUDA(cudaMemcpyAsync(F.pinned, F.status.ptr, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    ST_CUDA(cudaEventRecord(F.done_ev, st));
+    return ST_CUDA_LAST();
+}
+
+// Apply the batch's transform updates and TLAS maintenance, then launch it on flight slot f.
+int launch_flight(st_ctx *ctx, int f, std::vector<std::shared_ptr<ServeReq>> &reqs) {
+    Server &V = ctx->server;
+    InFlight &F = V.flights[f];
+    // transform updates, in submission order; a scene read by an in-flight batch is waited for first
+    std::map<int, uint32_t> moved_count;
+    for (auto &r : reqs) {
+        if (r->moved.empty()) continue;
+        for (InFlight &G : V.flights)
+            if (G.busy && G.scenes.count(r->slot)) {
+                cudaEventSynchronize(G.done_ev);
+                finish_flight(ctx, G);
+            }
+        ST_TRY(st_update_primitives(ctx, r->slot, r->moved.data(), r->moved_ids.data(), (uint32_t)r->moved.size()));
+        moved_count[r->slot] += (uint32_t)r->moved.size();
+    }
+    for (auto &kv : moved_count) {
+        SceneSlot *S = slot_of(ctx, kv.first);
+        const int mode = (double)kv.second < V.cfg.refit_fraction * S->n_prims ? ST_BVH_REFIT : ST_BVH_LBVH30;
+        ST_TRY(st_update_scene_bvh(ctx, kv.first, nullptr, mode));
+    }
+    // view table and arena layout
+    const int n = (int)reqs.size();
+    BatchPlan p;
+    int tile = V.cfg.tile_shape >= 0 ? V.cfg.tile_shape : TILE_8x4;
+    u32t chunk = V.cfg.chunk > 0 ? (u32t)V.cfg.chunk : 1;
+    std::ostringstream cls;
+    size_t dev = 0, host = 64;
+    u32t tw, th;
+    for (auto &r : reqs) {
+        SceneSlot *S = slot_of(ctx, r->slot);
+        u32t tris = 0;
+        for (const MeshDev &m : S->mesh_host) tris += m.triangle_count;
+        int pb = 0, tb = 0;
+        for (u32t x = S->n_prims; x > 1; x >>= 1) pb++;
+        for (u32t x = tris; x > 1; x >>= 1) tb++;
+        cls << "p" << pb << "t" << tb << "d" << r->view.depth << ";";
+    }
+    if (V.cfg.tile_shape < 0 || V.cfg.chunk <= 0) {
+        auto it = ctx->batch.tuned.find(cls.str());
+        if (it != ctx->batch.tuned.end()) {
+            if (V.cfg.tile_shape < 0) tile = it->second.first;
+            if (V.cfg.chunk <= 0) chunk = (u32t)it->second.second;
+        }
+    }
+    tile_dims(tile, tw, th);
+    for (auto &r : reqs) {
+        SceneSlot *S = slot_of(ctx, r->slot);
+        BatchView b;
+        memset(&b, 0, sizeof(b));
+        b.view = r->view;
+        b.view.primary_tlas = S->n_prims > 64 ? 1 : 0;
+        b.scene = scene_view(*S, nullptr);
+        if (r->has_scene_values) {
+            b.scene.ambient = r->ambient;
+            b.scene.lights = r->lights_present ? P<Light>(S->lights) : nullptr;
+            b.scene.n_lights = r->lights_present ? S->n_lights : 0;
+        }
+        b.tiles_x = (b.view.grid_w + tw - 1) / tw;
+        b.tile_begin = p.total_tiles;
+        p.total_tiles += b.tiles_x * ((b.view.grid_h + th - 1) / th);
+        const size_t grid = (size_t)b.view.grid_w * b.view.grid_h;
+        r->dev_float = dev; dev += align256(sizeof(FloatPixel) * grid);
+        r->dev_ssb = dev; dev += align256(sizeof(int4) * std::max(S->n_prims, 1u));
+        r->dev_seg = dev; dev += align256(sizeof(float) * ray_rows_floats(b.view));
+        const size_t u8b = (size_t)(b.view.grid_w - 1) * (b.view.grid_h - 1) * sizeof(uint32_t);
+        if (r->out_u8) { r->dev_u8 = dev; dev += align256(u8b); }
+        r->rays = grid;
+        r->batch_size = n;
+        p.table.push_back(b);
+        F.scenes.insert(r->slot);
+    }
+    // host staging: the status word, then each request's float grid and u8 frame
+    for (auto &r : reqs) {
+        const size_t grid = (size_t)r->view.grid_w * r->view.grid_h;
+        if (r->out_float) { r->host_float = host; host += align256(sizeof(FloatPixel) * grid); }
+        if (r->out_u8) { r->host_u8 = host; host += align256((size_t)(r->view.grid_w - 1) * (r->view.grid_h - 1) * 4); }
+    }
+    if (F.pinned_cap < host) {
+        if (F.pinned) cudaFreeHost(F.pinned);
+        F.pinned = nullptr;
+        F.pinned_cap = 0;
+        ST_CUDA(cudaMallocHost((void **)&F.pinned, host));
+        F.pinned_cap = host;
+    }
+    ST_TRY(reserve(ctx, F.B.table, sizeof(BatchView) * n));
+    ST_TRY(reserve(ctx, F.B.counter, 16));
+    if (F.B.staging_cap < (size_t)n) {
+        if (F.B.staging) cudaFreeHost(F.B.staging);
+        F.B.staging = nullptr;
+        F.B.staging_cap = 0;
+        ST_CUDA(cudaMallocHost((void **)&F.B.staging, sizeof(BatchView) * n));
+        F.B.staging_cap = n;
+    }
+    cudaStream_t st = F.stream;
+    char *arena = nullptr;
+    ST_CUDA(cudaMallocAsync((void **)&arena, std::max(dev, (size_t)256), st));
+    const int s = enqueue_flight(ctx, F, p, reqs, tile, chunk, arena);
+    cudaFreeAsync(arena, st);   // stream-ordered: released once the batch's work has run
+    ST_TRY(s);
+    const double t = st_clock();
+    for (auto &r : reqs) r->launch = t;
+    F.bytes = dev;
+    F.reqs = reqs;
+    F.busy = true;
+    return ST_OK;
+}
+
+void serve_loop(st_ctx *ctx) {
+    Server &V = ctx->server;
+    cudaSetDevice(ctx->device);
+    for (;;) {
+        for (InFlight &F : V.flights)
+            if (F.busy && cudaEventQuery(F.done_ev) == cudaSuccess) finish_flight(ctx, F);
+        std::vector<std::shared_ptr<ServeReq>> batch;
+        int free_slot = -1;
+        {
+            std::unique_lock<std::mutex> lk(V.m);
+            bool any_busy = false;
+            for (size_t i = 0; i < V.flights.size(); i++) {
+                if (V.flights[i].busy) any_busy = true;
+                else if (free_slot < 0) free_slot = (int)i;
+            }
+            if (V.stop && V.pending.empty() && !any_busy) break;
+            if (free_slot >= 0 && !V.pending.empty()) {
+                // admit in order while the budget and the batch rules allow
+                uint64_t bytes = 0;
+                std::set<int> scenes;
+                while (!V.pending.empty() && (int)batch.size() < V.cfg.max_views_per_batch) {
+                    auto &r = V.pending.front();
+                    SceneSlot *S = slot_of(ctx, r->slot);
+                    const size_t need = request_bytes(*r, S->n_prims);
+                    if (!r->moved.empty() && scenes.count(r->slot)) break;   // it changes a scene this batch renders
+                    if (V.inflight_bytes + bytes + need > V.frame_budget) {
+                        if (batch.empty() && !any_busy) {                   // can never fit
+                            r->status = ST_ERR_BUDGET;
+                            r->done = st_clock();
+                            V.pending.pop_front();
+                            V.cv_done.notify_all();
+                            continue;
+                        }
+                        break;
+                    }
+                    bytes += need;
+                    scenes.insert(r->slot);
+                    batch.push_back(r);
+                    V.pending.pop_front();
+                }
+                V.inflight_bytes += bytes;
+                if (batch.empty()) free_slot = -1;
+            } else {
+                V.cv_work.wait_for(lk, std::chrono::microseconds(any_busy ? 50 : 2000));
+                continue;
+            }
+        }
+        if (free_slot >= 0 && !batch.empty()) {
+            uint64_t held = 0;
+            for (auto &r : batch) held += request_bytes(*r, slot_of(ctx, r->slot)->n_prims);
+            int s = launch_flight(ctx, free_slot, batch);
+            std::lock_guard<std::mutex> lk(V.m);
+            V.inflight_bytes -= held;                    // the flight now accounts its own bytes
+            if (s == ST_OK) V.inflight_bytes += V.flights[free_slot].bytes;
+            else {
+                V.flights[free_slot].scenes.clear();
+                for (auto &r : batch) { r->status = s; r->done = st_clock(); }
+                V.cv_done.notify_all();
+            }
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int st_serve_start(st_ctx *ctx, const st_serve_config *cfg) {
+    if (!ctx) return ST_ERR_INVALID_ARG;
+    Server &V = ctx->server;
+    if (V.running) return ST_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    V.cfg = cfg ? *cfg : st_serve_config{};
+    if (V.cfg.max_in_flight <= 0) V.cfg.max_in_flight = 3;
+    if (V.cfg.max_views_per_batch <= 0) V.cfg.max_views_per_batch = 64;
+    if (V.cfg.refit_fraction <= 0) V.cfg.refit_fraction = 0.25;
+    if (!cfg) { V.cfg.tile_shape = -1; V.cfg.chunk = 0; }
+    V.frame_budget = V.cfg.frame_budget ? V.cfg.frame_budget
+                                        : (ctx->budget > ctx->in_use ? ctx->budget - ctx->in_use : 0);
+    V.flights.resize(V.cfg.max_in_flight);
+    for (InFlight &F : V.flights) {
+        ST_CUDA(cudaStreamCreateWithFlags(&F.stream, cudaStreamNonBlocking));
+        ST_CUDA(cudaEventCreateWithFlags(&F.done_ev, cudaEventDisableTiming));
+        ST_TRY(reserve(ctx, F.status, 16));
+    }
+    V.stop = false;
+    V.running = true;
+    V.inflight_bytes = 0;
+    V.worker = std::thread(serve_loop, ctx);
+    return ST_OK;
+}
+
+int st_submit(st_ctx *ctx, const st_request *req, st_ticket *ticket) {
+    if (!ctx || !req || !ticket || !req->view.viewport) return ST_ERR_INVALID_ARG;
+    Server &V = ctx->server;
+    if (!V.running) return ST_ERR_INVALID_ARG;
+    SceneSlot *S = slot_of(ctx, req->view.slot);
+    if (!S || !S->allocated || !S->tlas_valid) return ST_ERR_NOT_RESIDENT;
+    auto r = std::make_shared<ServeReq>();
+    r->slot = req->view.slot;
+    ST_TRY(make_view(req->view.viewport, r->view));
+    if (req->view.scene) {
+        r->has_scene_values = true;
+        r->ambient = req->view.scene->ambient_light.color;
+        r->lights_present = req->view.scene->lights != nullptr && req->view.scene->settings.lights;
+    }
+    r->out_float = req->view.out_float;
+    r->out_u8 = req->view.out_u8;
+    if (req->moved_count) {
+        if (!req->moved || !req->moved_ids) return ST_ERR_INVALID_ARG;
+        for (uint32_t k = 0; k < req->moved_count; k++)
+            if (req->moved_ids[k] >= S->n_prims) return ST_ERR_INVALID_ARG;
+        r->moved.assign(req->moved, req->moved + req->moved_count);
+        r->moved_ids.assign(req->moved_ids, req->moved_ids + req->moved_count);
+    }
+    r->arrival = req->arrival_time;
+    std::lock_guard<std::mutex> lk(V.m);
+    r->id = V.next_id++;
+    V.tickets[r->id] = r;
+    V.pending.push_back(r);
+    *ticket = r->id;
+    V.cv_work.notify_one();
+    return ST_OK;
+}
+
+static void fill_result(const ServeReq &r, st_result *out) {
+    out->status = r.status;
+    out->arrival_time = r.arrival;
+    out->launch_time = r.launch;
+    out->completion_time = r.done;
+    out->rays = r.rays;
+    out->batch_size = r.batch_size;
+}
+
+int st_poll(st_ctx *ctx, st_ticket ticket, st_result *result) {
+    if (!ctx) return ST_ERR_INVALID_ARG;
+    Server &V = ctx->server;
+    std::lock_guard<std::mutex> lk(V.m);
+    auto it = V.tickets.find(ticket);
+    if (it == V.tickets.end()) return ST_ERR_INVALID_ARG;
+    if (it->second->status == ST_ERR_NOT_READY) return ST_ERR_NOT_READY;
+    if (result) fill_result(*it->second, result);
+    V.tickets.erase(it);
+    return ST_OK;
+}
+
+int st_wait(st_ctx *ctx, st_ticket ticket, st_result *result, double timeout_s) {
+    if (!ctx) return ST_ERR_INVALID_ARG;
+    Server &V = ctx->server;
+    std::unique_lock<std::mutex> lk(V.m);
+    auto it = V.tickets.find(ticket);
+    if (it == V.tickets.end()) return ST_ERR_INVALID_ARG;
+    auto r = it->second;
+    if (!V.cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] { return r->status != ST_ERR_NOT_READY; }))
+        return ST_ERR_TIMEOUT;
+    if (result) fill_result(*r, result);
+    V.tickets.erase(ticket);
+    return ST_OK;
+}
+
+int st_serve_stop(st_ctx *ctx) {
+    if (!ctx) return ST_ERR_INVALID_ARG;
+    Server &V = ctx->server;
+    if (!V.running) return ST_OK;
+    {
+        std::lock_guard<std::mutex> lk(V.m);
+        V.stop = true;
+        V.cv_work.notify_all();
+    }
+    V.worker.join();
+    for (InFlight &F : V.flights) {
+        if (F.pinned) cudaFreeHost(F.pinned);
+        if (F.B.staging) cudaFreeHost(F.B.staging);
+        for (DevBuf *b : {&F.B.table, &F.B.counter, &F.status}) release(ctx, *b);
+        if (F.done_ev) cudaEventDestroy(F.done_ev);
+        if (F.stream) cudaStreamDestroy(F.stream);
+    }
+    V.flights.clear();
+    V.running = false;
+    return ST_OK;
+}
+
+}  // extern "C"
+
