@@ -179,6 +179,21 @@ typedef struct st_batch_options {
  * viewport per renderScene call (raytracer.h:302); each view's output equals st_render_ex's. */
 ST_API int st_render_batch(st_ctx *ctx, const st_view *views, int view_count, st_batch_options *options);
 
+/* LBVH30 over device-resident boxes with no allocation.  No counterpart in the reference: its
+ * builders run on the CPU (builder_top_down.h:272,366).  Same inputs and outputs as st_build_bvh
+ * (ST_BVH_LBVH30), but every pointer is DEVICE memory: aabbs (6 floats per item), codes (n, may be
+ * null), order (n), nodes (2n BVHNodes); info[2] is host memory.  The scratch is a static device array
+ * sized for ST_NOALLOC_LBVH_MAX_ITEMS items (about 4.8 MB), so the call makes no cudaMalloc/cudaFree
+ * and grows no pool: for hosts that must not allocate while other streams are busy or whose budget is
+ * reserved up front.  n > ST_NOALLOC_LBVH_MAX_ITEMS returns ST_ERR_INVALID_ARG before any work.
+ * The first call on a device looks up the array's address (and may load the module): make it once at
+ * set-up, before any stream capture.  Calls on one device share the array: overlapping calls (threads,
+ * streams or contexts of one process) race and must be serialised by the caller.  Returns after
+ * `stream` (null: the context's stream) has finished the build. */
+#define ST_NOALLOC_LBVH_MAX_ITEMS 65536u
+ST_API int st_build_lbvh_noalloc(st_ctx *ctx, const float *aabbs, uint32_t n, uint32_t max_leaf, uint32_t *codes,
+                                 uint32_t *order, BVHNode *nodes, uint32_t info[2], void *stream);
+
 /* ---- serving: continuous batching of render requests ---------------------------------------------
  * A worker thread inside the library takes submitted requests in order, admits them while the
  * device-memory budget for in-flight frame/ray buffers allows, applies their transform updates,

@@ -1480,3 +1480,68 @@ int st_serve_stop(st_ctx *ctx) {
 
 }  // extern "C"
 
+
+// ---- LBVH30 build that allocates nothing ---------------------------------------------------------
+// st_build_bvh and updateSceneBVH take their scratch from a per-context pool that grows with
+// cudaMalloc, and cudaMalloc/cudaFree can wait for work queued on every stream of the device.  A
+// host that rebuilds a TLAS between batches still running on other streams (a serving worker), or
+// one whose memory budget is fully reserved up front, cannot afford that wait or that growth.  This
+// variant keeps its scratch in one static device array sized for ST_NOALLOC_LBVH_MAX_ITEMS items.
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = lbvh_scratch_bytes(ST_NOALLOC_LBVH_MAX_ITEMS);
+// Nothing here has to start at zero: every word a build reads was written earlier in the same
+// build (bounds_init_kernel, the radix histograms, cudaMemsetAsync of the arrival counters and of
+// the height word).  Calls that overlap on one device share this array and race.
+static __device__ __align__(256) unsigned char g_lbvh_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// The array's device address on the current device, looked up once per device (the first call
+// may load the module); the symbol itself is never handed to a kernel.
+int noalloc_scratch(st_ctx *ctx, void **out) {
+    if (ctx->device < 0 || ctx->device >= kNoAllocMaxDevices) return ST_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+    if (!g_noalloc_ptr[ctx->device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_lbvh_noalloc_scratch);
+        if (e != cudaSuccess) return fail_cuda(ctx, e);
+        if (!p || (reinterpret_cast<uintptr_t>(p) & 255)) return fail_cuda(ctx, cudaErrorInvalidSymbol);
+        g_noalloc_ptr[ctx->device] = p;
+    }
+    *out = g_noalloc_ptr[ctx->device];
+    return ST_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int st_build_lbvh_noalloc(st_ctx *ctx, const float *aabbs, uint32_t n, uint32_t max_leaf, uint32_t *codes,
+                          uint32_t *order, BVHNode *nodes, uint32_t info[2], void *stream) {
+    if (!ctx || !aabbs || !order || !nodes || !info || n == 0 || max_leaf == 0 || max_leaf > 0xFFFF)
+        return ST_ERR_INVALID_ARG;
+    if (n > ST_NOALLOC_LBVH_MAX_ITEMS) return ST_ERR_INVALID_ARG;   // beyond the static scratch
+    ST_CUDA(cudaSetDevice(ctx->device));
+    void *scratch = nullptr;
+    ST_TRY(noalloc_scratch(ctx, &scratch));
+    LbvhScratch s;
+    lbvh_carve(s, scratch, ST_NOALLOC_LBVH_MAX_ITEMS);
+    s.aabbs = const_cast<float *>(aabbs);   // only read by the build
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    u32t inf[2];
+    cudaError_t e = lbvh_build(s, n, max_leaf, nodes, order, inf, st);
+    if (e == cudaSuccess && codes) {
+        launch_codes_by_item(s, n, codes, st);
+        e = cudaStreamSynchronize(st);
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(ctx, e);
+    info[0] = inf[0];
+    info[1] = inf[1];
+    return ST_OK;
+}
+
+}  // extern "C"

@@ -403,6 +403,23 @@ cudaError_t lbvh_reserve(LbvhScratch &s, u32t n) {
     s.capacity = cap;
     return cudaSuccess;
 }
+static_assert(RS_TILE == 2048 && SCAN_BLOCK == 1024, "lbvh_scratch_bytes assumes these tile sizes");
+void lbvh_carve(LbvhScratch &s, void *base, u32t cap) {
+    char *p = static_cast<char *>(base);
+    auto take = [&](size_t bytes) { char *q = p; p += lbvh_align(bytes); return q; };
+    const u32t nblocks = (cap + RS_TILE - 1) / RS_TILE;
+    const size_t hist = (size_t)256 * nblocks + 2 * ((cap + SCAN_BLOCK - 1) / SCAN_BLOCK) + 64;
+    s = LbvhScratch();
+    s.bounds = reinterpret_cast<unsigned *>(take(sizeof(unsigned) * 8));
+    u32t **arrays[] = {&s.codes, &s.codes_alt, &s.order, &s.order_alt, &s.first, &s.last, &s.lchild, &s.rchild,
+                       &s.parent, &s.leaf_parent, &s.rank, &s.flags};
+    for (u32t **a : arrays) *a = reinterpret_cast<u32t *>(take(sizeof(u32t) * (size_t)cap));
+    s.kbox = reinterpret_cast<unsigned *>(take(sizeof(unsigned) * 6 * (size_t)cap));
+    s.info = reinterpret_cast<u32t *>(take(sizeof(u32t) * 4));
+    s.hist = reinterpret_cast<u32t *>(take(sizeof(u32t) * hist * 2));
+    s.capacity = cap;
+}
+
 void lbvh_release(LbvhScratch &s) {
     void *ptrs[] = {s.aabbs, s.bounds, s.codes, s.codes_alt, s.order, s.order_alt, s.hist, s.first, s.last, s.lchild,
                     s.rchild, s.parent, s.leaf_parent, s.rank, s.flags, s.kbox, s.info};

@@ -66,6 +66,16 @@ struct LbvhScratch {
 
 cudaError_t lbvh_reserve(LbvhScratch &s, u32t n);
 void lbvh_release(LbvhScratch &s);
+// Bytes of one caller-provided block holding every LbvhScratch array except aabbs for builds of up
+// to `cap` items (radix tiles of 2048 items, scan blocks of 1024 elements; arrays 256-byte aligned).
+constexpr size_t lbvh_align(size_t b) { return (b + 255) & ~(size_t)255; }
+constexpr size_t lbvh_scratch_bytes(u32t cap) {
+    return lbvh_align(32) + 12 * lbvh_align(4 * (size_t)cap) + lbvh_align(24 * (size_t)cap) + lbvh_align(16) +
+           lbvh_align(8 * (256 * (((size_t)cap + 2047) / 2048) + 2 * (((size_t)cap + 1023) / 1024) + 64));
+}
+// Point the arrays of `s` (aabbs excepted) into `base`, a 256-byte aligned block of
+// lbvh_scratch_bytes(cap) bytes; s.capacity = cap.
+void lbvh_carve(LbvhScratch &s, void *base, u32t cap);
 // Items' world boxes -> Morton codes -> stable radix sort -> Karras tree -> leaf collapse ->
 // reference-layout BVHNode array (1 + 2*kept nodes) + leaf order.  Synchronous w.r.t. `st`.
 // out_nodes must hold 2n nodes; out_order n ids.  info (host) receives node_count, height.
