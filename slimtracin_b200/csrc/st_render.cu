@@ -50,7 +50,7 @@ __device__ __forceinline__ NodePair load_pair(const NodePair *p) {
 }
 
 template <bool CNT>
-__device__ bool trace_mesh(TState<CNT> &t, const SceneDev &S, const MeshDev &M, bool any_hit) {   // mesh.h:38
+__device__ __forceinline__ bool trace_mesh(TState<CNT> &t, const SceneDev &S, const MeshDev &M, bool any_hit) {   // mesh.h:38
     const RayD &ray = t.local;
     Hit &closest = t.mesh_closest;
     float ld, rd;
@@ -58,46 +58,49 @@ __device__ bool trace_mesh(TState<CNT> &t, const SceneDev &S, const MeshDev &M, 
     t.count(C_AABB);
     if (!hit_aabb(V(M.aabb[0], M.aabb[1], M.aabb[2]), V(M.aabb[3], M.aabb[4], M.aabb[5]), ray, closest.distance, ld))
         return false;
-    if (M.root_count) return hit_triangles(t, S, M.tri_offset, M.triangle_count, any_hit);
+    // Leaves met at a node are tested (left, then right) before the walk moves on, as in the
+    // reference; they are queued so that the triangle loop has a single call site.
+    u32t leaf_first[2], leaf_count[2];
+    int leaves = 0;
     const NodePair *pairs = S.mesh_pairs + M.pair_offset;
-    u32t pair = (M.root_first - 1) >> 1;
+    u32t pair = kNoPair;
+    if (M.root_count) { leaf_first[0] = 0; leaf_count[0] = M.triangle_count; leaves = 1; }
+    else pair = (M.root_first - 1) >> 1;
     u32t sp = 0;
     bool found = false;
     for (;;) {
+#pragma unroll 1
+        for (int k = 0; k < leaves; k++)
+            if (hit_triangles(t, S, M.tri_offset + leaf_first[k], leaf_count[k], any_hit)) {
+                closest.object_id += leaf_first[k];
+                found = true;
+                if (any_hit) return true;
+            }
+        leaves = 0;
+        if (pair == kNoPair) break;
         const NodePair P = load_pair(pairs + pair);
         t.count(C_AABB, 2);
         bool hl = hit_aabb(V(P.a.x, P.a.y, P.a.z), V(P.a.w, P.b.x, P.b.y), ray, closest.distance, ld);
         bool hr = hit_aabb(V(P.b.z, P.b.w, P.c.x), V(P.c.y, P.c.z, P.c.w), ray, closest.distance, rd);
         bool lgo = hl, rgo = hr;
-        if (hl && P.d.y) {
-            if (hit_triangles(t, S, M.tri_offset + P.d.x, P.d.y, any_hit)) {
-                closest.object_id += P.d.x;
-                found = true;
-                if (any_hit) break;
-            }
-            lgo = false;
-        }
-        if (hr && P.d.w) {
-            if (hit_triangles(t, S, M.tri_offset + P.d.z, P.d.w, any_hit)) {
-                closest.object_id += P.d.z;
-                found = true;
-                if (any_hit) break;
-            }
-            rgo = false;
-        }
+        if (hl && P.d.y) { leaf_first[leaves] = P.d.x; leaf_count[leaves] = P.d.y; leaves++; lgo = false; }
+        if (hr && P.d.w) { leaf_first[leaves] = P.d.z; leaf_count[leaves] = P.d.w; leaves++; rgo = false; }
         if (lgo) {
             u32t near_pair = P.d.x, far_pair = P.d.z;
             if (rgo) {
                 if (!any_hit && ld > rd) { near_pair = P.d.z; far_pair = P.d.x; }
-                if (sp >= kStack) { t.status |= S_STACK_OVERFLOW; return false; }
+                if (sp >= kStack) {               // the queued leaves still run, then the walk ends
+                    t.status |= S_STACK_OVERFLOW;
+                    pair = kNoPair;
+                    continue;
+                }
                 t.mesh_stack[sp++] = far_pair;
             }
             pair = near_pair;
         } else if (rgo) {
             pair = P.d.z;
         } else {
-            if (sp == 0) break;
-            pair = t.mesh_stack[--sp];
+            pair = sp ? t.mesh_stack[--sp] : kNoPair;
         }
     }
     return found;
@@ -106,7 +109,7 @@ __device__ bool trace_mesh(TState<CNT> &t, const SceneDev &S, const MeshDev &M, 
 // ---- hitPrimitives intersection/primitives.h:9 ----------------------------------------------------
 // ids == nullptr: the candidates are primitives first..first+count-1 in index order.
 template <bool CNT>
-__device__ bool hit_primitives(TState<CNT> &t, const SceneDev &S, const RayD &ray, const u32t *ids, u32t first,
+__device__ __forceinline__ bool hit_primitives(TState<CNT> &t, const SceneDev &S, const RayD &ray, const u32t *ids, u32t first,
                                u32t count, bool any_hit, const int4 *ssb, int x, int y, float cone_angle) {
     Hit &hit = t.current, &closest = t.closest;
     bool found = false;
@@ -186,56 +189,63 @@ __device__ bool hit_primitives(TState<CNT> &t, const SceneDev &S, const RayD &ra
 }
 
 // ---- traceScene shaders/trace.h:8 (TLAS walk); with ssb != null it also serves primary rays ----
+// The primitive loop, the BLAS walk and the triangle loop each have one call site here, so every
+// inlined copy of the walk carries one copy of them (the instruction footprint of the megakernel).
+// all_prims: test every primitive in leaf-id order without the root box (the primary-ray path of
+// scenes with few primitives, raytracer.h:100).
 template <bool CNT>
-__device__ bool trace_scene(TState<CNT> &t, const SceneDev &S, RayD &ray, bool any_hit, const int4 *ssb, int x,
-                            int y, float cone_angle, bool prepped) {
+__device__ __forceinline__ bool trace_scene(TState<CNT> &t, const SceneDev &S, RayD &ray, bool any_hit, const int4 *ssb,
+                                            int x, int y, float cone_angle, bool prepped, bool all_prims) {
     if (!prepped) {
         ray.rcp = rcp(ray.direction);
         pre_prep(ray);
     }
     float ld, rd;
-    t.count(C_AABB);
-    if (!hit_aabb(V(S.tlas_root_aabb[0], S.tlas_root_aabb[1], S.tlas_root_aabb[2]),
-                  V(S.tlas_root_aabb[3], S.tlas_root_aabb[4], S.tlas_root_aabb[5]), ray, t.closest.distance, ld))
-        return false;
-    if (S.tlas_root_count)
-        return hit_primitives(t, S, ray, S.tlas_leaf_ids, 0, S.n_prims, any_hit, ssb, x, y, cone_angle);
-    u32t pair = (S.tlas_root_first - 1) >> 1;
+    u32t leaf_first[2], leaf_count[2];
+    int leaves = 0;
+    u32t pair = kNoPair;
+    if (!all_prims) {
+        t.count(C_AABB);
+        if (!hit_aabb(V(S.tlas_root_aabb[0], S.tlas_root_aabb[1], S.tlas_root_aabb[2]),
+                      V(S.tlas_root_aabb[3], S.tlas_root_aabb[4], S.tlas_root_aabb[5]), ray, t.closest.distance, ld))
+            return false;
+    }
+    if (all_prims || S.tlas_root_count) { leaf_first[0] = 0; leaf_count[0] = S.n_prims; leaves = 1; }
+    else pair = (S.tlas_root_first - 1) >> 1;
     u32t sp = 0;
     bool found = false;
     for (;;) {
+#pragma unroll 1
+        for (int k = 0; k < leaves; k++)
+            if (hit_primitives(t, S, ray, S.tlas_leaf_ids, leaf_first[k], leaf_count[k], any_hit, ssb, x, y, cone_angle)) {
+                found = true;
+                if (any_hit) return true;
+            }
+        leaves = 0;
+        if (pair == kNoPair) break;
         const NodePair P = load_pair(S.tlas_pairs + pair);
         t.count(C_AABB, 2);
         bool hl = hit_aabb(V(P.a.x, P.a.y, P.a.z), V(P.a.w, P.b.x, P.b.y), ray, t.closest.distance, ld);
         bool hr = hit_aabb(V(P.b.z, P.b.w, P.c.x), V(P.c.y, P.c.z, P.c.w), ray, t.closest.distance, rd);
         bool lgo = hl, rgo = hr;
-        if (hl && P.d.y) {
-            if (hit_primitives(t, S, ray, S.tlas_leaf_ids, P.d.x, P.d.y, any_hit, ssb, x, y, cone_angle)) {
-                found = true;
-                if (any_hit) break;
-            }
-            lgo = false;
-        }
-        if (hr && P.d.w) {
-            if (hit_primitives(t, S, ray, S.tlas_leaf_ids, P.d.z, P.d.w, any_hit, ssb, x, y, cone_angle)) {
-                found = true;
-                if (any_hit) break;
-            }
-            rgo = false;
-        }
+        if (hl && P.d.y) { leaf_first[leaves] = P.d.x; leaf_count[leaves] = P.d.y; leaves++; lgo = false; }
+        if (hr && P.d.w) { leaf_first[leaves] = P.d.z; leaf_count[leaves] = P.d.w; leaves++; rgo = false; }
         if (lgo) {
             u32t near_pair = P.d.x, far_pair = P.d.z;
             if (rgo) {
                 if (!any_hit && ld > rd) { near_pair = P.d.z; far_pair = P.d.x; }
-                if (sp >= kStack) { t.status |= S_STACK_OVERFLOW; return found; }
+                if (sp >= kStack) {               // the queued leaves still run, then the walk ends
+                    t.status |= S_STACK_OVERFLOW;
+                    pair = kNoPair;
+                    continue;
+                }
                 t.scene_stack[sp++] = far_pair;
             }
             pair = near_pair;
         } else if (rgo) {
             pair = P.d.z;
         } else {
-            if (sp == 0) break;
-            pair = t.scene_stack[--sp];
+            pair = sp ? t.scene_stack[--sp] : kNoPair;
         }
     }
     return found;
@@ -258,7 +268,7 @@ __device__ v3 shade_from_lights(TState<CNT> &t, const SceneDev &S, Shaded &s, Ra
         ray.origin = s.position;
         ray.direction = s.light_direction;
         t.count(C_SHADOW);
-        if (trace_scene(t, S, ray, true, nullptr, 0, 0, 0.0f, false)) continue;       // inShadow trace.h:85
+        if (trace_scene(t, S, ray, true, nullptr, 0, 0, 0.0f, false, false)) continue;       // inShadow trace.h:85
         color = vvfma(shade_point(s, NdotL), vscale(from(light.color), li), color);
     }
     return color;
@@ -430,7 +440,7 @@ __device__ v3 shade_surface(TState<CNT> &t, const SceneDev &S, RayD &ray, bool &
             }
             t.count(C_BOUNCE);
             t.closest.distance = t.closest.distance_squared = INFINITY;       // traceRay trace.h:89
-            if (trace_scene(t, S, ray, false, nullptr, 0, 0, 0.0f, false)) {
+            if (trace_scene(t, S, ray, false, nullptr, 0, 0, 0.0f, false, false)) {
                 t.count(C_SHADE);
                 s.prim_index = hit.object_id;
                 s.material = M = S.materials + hit.material_id;
@@ -583,12 +593,10 @@ __device__ __forceinline__ void trace_point(TState<CNT> &t, const SceneDev &S, c
     v3 Ro = ray.origin, Rd = ray.direction, color = splat(0);
     bool lights_shaded = false;
     bool hit_found;
-    if (v.primary_tlas) {
+    {
         RayD pr = ray;
         pre_prep(pr);
-        hit_found = trace_scene(t, S, pr, false, ssb, (int)x, (int)y, v.cone_angle, true);
-    } else {
-        hit_found = hit_primitives(t, S, ray, S.tlas_leaf_ids, 0, S.n_prims, false, ssb, (int)x, (int)y, v.cone_angle);
+        hit_found = trace_scene(t, S, pr, false, ssb, (int)x, (int)y, v.cone_angle, true, !v.primary_tlas);
     }
     Hit &hit = t.closest;
     if (prim_ids) prim_ids[idx] = hit_found ? hit.object_id : 0xFFFFFFFFu;
