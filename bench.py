@@ -5,7 +5,7 @@
 Workload (one step = one frame): 1920x1080 viewport = 1921x1081 QCAA grid of primary rays,
 trace.depth 4, one displaced icosphere of 1,310,720 triangles in 8 instances (4 Cook-Torrance,
 2 glass, 2 mirror), two 1024^2 textures with 9-level mip chains, 2 emissive quads.  Seeded
-synthetic data (scenes.config1); the BLAS is built on the device (LBVH30) once, before timing.
+synthetic data (scenes.config1); the BLAS is built on the device (binned SAH) once, before timing.
 
 value      primary rays of all ranks / (max over ranks of the device time of K renders), inputs
            resident, outputs to device buffers; L2 flushed (256 MiB write) before every step,
@@ -18,6 +18,13 @@ roofline   the trace kernel: algorithmic bytes per frame (device event counters 
 cpu_baseline / --impl reference
            the reference's own renderer (oracle/_ref, compiled from the reference sources) on the
            same scene bytes, all host threads, over a bounded sample of rows
+batched    64 views (resolutions from 256x256 to 1920x1080, 1-6 bounces) over 8 resident scenes:
+           one st_render_batch call (persistent kernel, autotuned, CUDA graph) against one
+           st_render_ex call per view, both timed with device events around the whole sequence
+served     Poisson request streams (--rates) over the same 8 scenes, each request a view plus a
+           transform update of 0-64 primitives, u8 frames to host: the library's server against
+           the same requests one at a time; p50/p99 latency from arrival to completion (library
+           clock) and Mrays/s over the stream
 """
 import argparse
 import ctypes as C
@@ -177,12 +184,74 @@ def run_reference_arm(args):
     return 0
 
 
+def mixed_workloads(r, big_sd, stream, rates):
+    """The batched-views workload (64 views over 8 resident scenes, one graph-captured persistent
+    launch vs one st_render_ex per view) and the served stream (Poisson arrivals at `rates` with
+    transform updates, the library's server vs one request at a time), both with device-event or
+    library-clock timing."""
+    import torch
+    from slimtracin_b200 import api, mixed as MX
+    residents = MX.resident_scenes(big=big_sd)
+    slots = MX.upload(r, residents, first_slot=1)
+    rng = np.random.default_rng(1234)
+    views = []
+    for _ in range(64):
+        si, w, h, d = MX.random_view(rng, len(residents))
+        views.append((slots[si], residents[si], scenes.Frame(w, h, MX.random_camera(rng, residents[si]), depth=d,
+                                                             with_pixels=False, with_float=False)))
+    rays = sum(fr.rays for _, _, fr in views)
+    biggest = max(fr.rays for _, _, fr in views)
+    # per-view device outputs for the batch; one shared pair for the per-frame loop
+    f_sizes = [fr.rays * 24 for _, _, fr in views]
+    u_sizes = [fr.width * fr.height * 4 for _, _, fr in views]
+    fbuf = torch.empty(sum(f_sizes), dtype=torch.uint8, device="cuda")
+    ubuf = torch.empty(sum(u_sizes), dtype=torch.uint8, device="cuda")
+    fptr = fbuf.data_ptr() + np.concatenate([[0], np.cumsum(f_sizes)[:-1]]).astype(np.int64)
+    uptr = ubuf.data_ptr() + np.concatenate([[0], np.cumsum(u_sizes)[:-1]]).astype(np.int64)
+    one_f = torch.empty(biggest * 24, dtype=torch.uint8, device="cuda")
+    one_u = torch.empty(biggest * 4, dtype=torch.uint8, device="cuda")
+    per_frame = MX.PerFrame(r, views, one_f.data_ptr(), one_u.data_ptr())
+    batch = MX.Batch(r, views, [int(x) for x in fptr], [int(x) for x in uptr], use_graph=True)
+
+    def timed(fn, reps=3):
+        fn()                      # warm-up (and, for the batch, autotuning and graph capture)
+        torch.cuda.synchronize()
+        out = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+            fn()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            torch.cuda.synchronize()
+            out.append(e0.elapsed_time(e1))
+        return float(np.median(out))
+
+    pf_ms = timed(per_frame.run)
+    b_ms = timed(batch.run)
+    batched = {"views": len(views), "scenes": [x.name for x in residents], "rays": rays,
+               "per_frame_ms": pf_ms, "batch_ms": b_ms,
+               "per_frame_mrays_s": rays / pf_ms / 1e3, "batch_mrays_s": rays / b_ms / 1e3,
+               "speedup": pf_ms / b_ms, "tile_shape": batch.opt.tile_shape_used,
+               "chunk": batch.opt.chunk_used, "graph_replayed": batch.opt.graph_replayed}
+    del fbuf, ubuf, one_f, one_u
+    served = []
+    for k, rate in enumerate(rates):
+        count = int(min(max(rate * 3.0, 60), 1500))
+        stream_k = MX.Stream(residents, slots, rate, count, seed=500 + k)
+        srv = MX.latency_summary(stream_k.serve(r))
+        pf = MX.latency_summary(stream_k.per_frame(r))
+        served.append({"rate_req_s": rate, "requests": count, "served": srv, "per_frame": pf})
+    return {"batched": batched, "served": served}
+
+
 def blas_on_device(sd):
     from slimtracin_b200 import api
     r = api.Renderer(device=int(os.environ.get("LOCAL_RANK", 0)))
     try:
         for md in sd.meshes:
-            r.build_blas(md, api.ST_BVH_LBVH30)
+            r.build_blas(md, api.ST_BVH_BINNED_SAH)
     finally:
         r.close()
 
@@ -194,6 +263,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the batched-views and served-stream sections")
+    ap.add_argument("--rates", default="50,200,1000,2000", help="served-stream arrival rates (req/s)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -213,7 +284,8 @@ def main():
     sd, cam = build_scene()
     r = api.Renderer(device=local)
     for md in sd.meshes:
-        r.build_blas(md, api.ST_BVH_LBVH30)
+        r.build_blas(md, api.ST_BVH_BINNED_SAH)
+        md.device_built = True
     r.upload(0, sd, tlas=None)
     r.build_tlas(0, sd, api.ST_BVH_LBVH30)
     frame = scenes.Frame(WIDTH, HEIGHT, cam, depth=DEPTH)
@@ -303,6 +375,8 @@ def main():
     h2d = len(prim_view) * S.PRIMITIVE_DT.itemsize
     d2h = grid * 24 + WIDTH * HEIGHT * 4
 
+    mixed = None if args.no_mixed else mixed_workloads(r, sd, stream, [float(x) for x in args.rates.split(",") if x])
+
     # ---- roofline of the trace kernel -----------------------------------------------------------
     trace_avg_ms = sum(trace_ms) / len(trace_ms)
     peaks = measured_peaks()
@@ -344,7 +418,7 @@ def main():
                        "width": WIDTH, "height": HEIGHT, "depth": DEPTH, "rays_per_frame": grid,
                        "triangles": sd.meshes[0].triangle_count, "instances": 8, "parallelism": f"replicas x{world}",
                        "l2": "flushed before every step (256 MiB write, outside the timed events)",
-                       "blas": "LBVH30 on device", "tlas": "LBVH30 on device"},
+                       "blas": "binned SAH on device", "tlas": "LBVH30 on device"},
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "api": "st_upload_primitives + st_render_scene, pinned host buffers"},
             "gpu_launches": 4 * args.steps,
@@ -354,6 +428,8 @@ def main():
                          "bytes_alg_per_launch": bytes_alg,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6.65 TB/s"},
             "counters": counters,
+            "batched": mixed["batched"] if mixed else None,
+            "served": mixed["served"] if mixed else None,
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
         }

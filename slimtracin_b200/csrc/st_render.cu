@@ -662,8 +662,14 @@ __device__ __forceinline__ void flush_counters(TState<CNT> &t, unsigned *status,
     }
 }
 
+// ST_TRACE_MIN_BLOCKS (optional): resident 128-thread blocks per SM the register allocation must allow
+#ifdef ST_TRACE_MIN_BLOCKS
+#define ST_TRACE_BOUNDS __launch_bounds__(128, ST_TRACE_MIN_BLOCKS)
+#else
+#define ST_TRACE_BOUNDS __launch_bounds__(128)
+#endif
 template <bool CNT>
-__global__ void __launch_bounds__(128) trace_kernel(SceneDev S, ViewDev v, const int4 *ssb, const float *dirs,
+__global__ void ST_TRACE_BOUNDS trace_kernel(SceneDev S, ViewDev v, const int4 *ssb, const float *dirs,
                                                     FloatPixel *out, u32t *prim_ids, unsigned *status,
                                                     unsigned long long *counters) {
     const u32t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -682,7 +688,7 @@ __global__ void __launch_bounds__(128) trace_kernel(SceneDev S, ViewDev v, const
 // 32 points); warps take tiles from one global counter, `chunk` tiles at a time, so views of
 // different sizes, scenes and bounce counts share the launch and no warp idles while work is left.
 template <bool CNT, int TW, int TH>
-__global__ void __launch_bounds__(128) batch_kernel(const BatchView *views, u32t n_views, u32t total_tiles, u32t chunk,
+__global__ void ST_TRACE_BOUNDS batch_kernel(const BatchView *views, u32t n_views, u32t total_tiles, u32t chunk,
                                                     u32t *tile_counter, unsigned *status, unsigned long long *counters) {
     static_assert(TW * TH == 32, "one warp per tile");
     const u32t lane = threadIdx.x & 31;

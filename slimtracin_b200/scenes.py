@@ -194,7 +194,7 @@ class Frame:
     """A Viewport + Camera + PixelGrid + output buffers for one view (reference structs)."""
 
     def __init__(self, width, height, camera: CameraSpec, depth=2, mode=S.RM_BEAUTY, cone_angle=0.0,
-                 with_pixels=True):
+                 with_pixels=True, with_float=True):
         self.width, self.height = width, height
         self.grid_w, self.grid_h = width + 1, height + 1
         self.camera = S.Camera()
@@ -202,9 +202,9 @@ class Frame:
         self.grid = S.PixelGrid()
         update_dimensions(self.grid.dimensions, width, height, True)
         self.grid.QCAA = 1
-        self.float_pixels = np.zeros(self.grid_w * self.grid_h, dtype=S.FLOATPIXEL_DT)
+        self.float_pixels = np.zeros(self.grid_w * self.grid_h, dtype=S.FLOATPIXEL_DT) if with_float else None
         self.pixels = np.zeros(width * height, dtype=S.PIXEL_DT) if with_pixels else None
-        self.grid.float_pixels = self.float_pixels.ctypes.data
+        self.grid.float_pixels = self.float_pixels.ctypes.data if with_float else None
         self.grid.pixels = self.pixels.ctypes.data if with_pixels else None
         self.viewport = S.Viewport()
         vp = self.viewport
