@@ -49,6 +49,25 @@ struct TState {
     __device__ __forceinline__ void count(int k, unsigned n = 1) { if (CNT) cnt[k] += n; }
 };
 
+// A ray that does not move along an axis (a zero direction component, or one so small that
+// -origin * rcp overflows) makes hitAABB compute inf - inf = NaN on that axis.  Its min/max chain
+// then drops the NaN together with a neighbouring axis, the ray accepts boxes nowhere near it and
+// walks nearly every node of a BVH: one such ray through a 1.3M-triangle BLAS made hundreds of
+// thousands of box and triangle tests and held its warp for hundreds of milliseconds.  For those
+// axes the reciprocal is replaced by +-2^100: the slab then yields a huge negative entry (origin
+// inside the slab, no constraint) or a huge positive one (outside, the box is refused), exactly,
+// since scaling by a power of two is exact.  The walk visits only boxes that hold points of the
+// ray, so it finds the same hits; among boxes the ray crosses it orders children by their true
+// entry distances, where hitAABB's NaN chain would have dropped an axis, so of two hits at exactly
+// the same distance, or of two occluders of a shadow ray, another may be found first.  Every other
+// ray keeps the reference's arithmetic unchanged.
+__device__ __forceinline__ void parallel_axis(float dir, float org, float &rcp, float &so) {
+    if (!(fabsf(rcp) < INFINITY && fabsf(so) < INFINITY)) {
+        rcp = copysignf(0x1p100f, dir);
+        so = -org * rcp;
+    }
+}
+
 // prePrepRay core/init.h:536
 __device__ __forceinline__ void pre_prep(RayD &r) {
     r.ox = signbit(r.direction.x);
@@ -57,6 +76,9 @@ __device__ __forceinline__ void pre_prep(RayD &r) {
     r.scaled_origin.x = -r.origin.x * r.rcp.x;
     r.scaled_origin.y = -r.origin.y * r.rcp.y;
     r.scaled_origin.z = -r.origin.z * r.rcp.z;
+    parallel_axis(r.direction.x, r.origin.x, r.rcp.x, r.scaled_origin.x);
+    parallel_axis(r.direction.y, r.origin.y, r.rcp.y, r.scaled_origin.y);
+    parallel_axis(r.direction.z, r.origin.z, r.rcp.z, r.scaled_origin.z);
 }
 
 // hitAABB render/AABB.h:6 (the octant offset selects max for the entry plane when negative)
