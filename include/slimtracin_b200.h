@@ -199,9 +199,12 @@ ST_API int st_build_lbvh_noalloc(st_ctx *ctx, const float *aabbs, uint32_t n, ui
  * device-memory budget for in-flight frame/ray buffers allows, applies their transform updates,
  * refits (few moved primitives) or rebuilds (many) the TLAS of exactly the scenes that changed,
  * and launches each batch with the persistent multi-view kernel on one of `max_in_flight` streams,
- * so requests that arrive while other batches run are launched beside them.  A request never
- * shares a batch with a request that changes its scene after it, so every result equals the
- * result of the same request rendered alone after the same sequence of updates.
+ * so requests that arrive while other batches run are launched beside them.  An update to a scene
+ * that batches in flight still read goes to a new copy of the scene's primitive and TLAS arrays
+ * (a scene version; at most one per batch in flight, counted against the context's budget), so it
+ * never waits for them.  A request never shares a batch with a request that changes its scene
+ * after it, so every result equals the result of the same request rendered alone after the same
+ * sequence of updates.
  * While serving, only st_submit / st_poll / st_wait / st_serve_stop may be called on the context
  * (from any one host thread); the scenes must already be resident.  No reference counterpart. */
 typedef struct st_serve_config {

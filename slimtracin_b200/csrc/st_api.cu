@@ -29,6 +29,12 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
+// The arrays a transform update rewrites: primitive records and the TLAS.  The serving loop gives a
+// scene a fresh copy of them when batches still in flight read the current one (scene versions).
+struct MotionBufs {
+    DevBuf prims_raw, prims, tlas_nodes, tlas_leaf_ids, tlas_pairs, tlas_aabbs, tlas_scratch;
+};
+
 struct SceneSlot {
     bool allocated = false;
     u32t n_prims = 0, n_materials = 0, n_lights = 0, n_meshes = 0, n_textures = 0;
@@ -49,7 +55,15 @@ struct SceneSlot {
     bool lights_present = false;
     std::vector<Primitive> prims_host;    // host copy for the emissive/occluder lists
     std::vector<Material> materials_host;
+    std::vector<MotionBufs> spare;        // released scene versions, reused by the next update
 };
+
+DevBuf *motion_field(SceneSlot &S, MotionBufs &m, int k, DevBuf **mine) {
+    DevBuf *a[7] = {&S.prims_raw, &S.prims, &S.tlas_nodes, &S.tlas_leaf_ids, &S.tlas_pairs, &S.tlas_aabbs, &S.tlas_scratch};
+    DevBuf *b[7] = {&m.prims_raw, &m.prims, &m.tlas_nodes, &m.tlas_leaf_ids, &m.tlas_pairs, &m.tlas_aabbs, &m.tlas_scratch};
+    *mine = a[k];
+    return b[k];
+}
 
 }  // namespace
 
@@ -93,6 +107,15 @@ struct InFlight {
     size_t bytes = 0;                  // device bytes this batch holds against the frame budget
     std::vector<std::shared_ptr<ServeReq>> reqs;
     std::set<int> scenes;
+    uint64_t launch_id = 0;
+};
+
+// A scene version replaced while batches in flight still read it; it returns to the scene's
+// spare list once every one of those batches has finished.
+struct RetiredVersion {
+    int slot = 0;
+    MotionBufs bufs;
+    std::vector<std::pair<int, uint64_t>> readers;   // (flight, launch id)
 };
 
 struct Server {
@@ -105,7 +128,9 @@ struct Server {
     std::vector<InFlight> flights;
     st_serve_config cfg{};
     uint64_t frame_budget = 0, inflight_bytes = 0;
-    uint64_t next_id = 1;
+    uint64_t next_id = 1, next_launch = 1;
+    std::vector<RetiredVersion> retired;
+    cudaMemPool_t pool = nullptr;       // per-batch arenas; keeps freed memory for the next batch
 };
 
 struct st_ctx {
@@ -357,6 +382,11 @@ int st_free_scene(st_ctx *ctx, int slot) {
                       &S->tlas_pairs, &S->tlas_aabbs, &S->tlas_scratch, &S->meshes, &S->mesh_pairs, &S->tri_hot,
                       &S->tri_full, &S->textures, &S->mips, &S->quads, &S->emissive, &S->occluders})
         release(ctx, *b);
+    for (MotionBufs &m : S->spare)
+        for (int k = 0; k < 7; k++) {
+            DevBuf *mine;
+            release(ctx, *motion_field(*S, m, k, &mine));
+        }
     *S = SceneSlot();
     return ST_OK;
 }
@@ -1143,6 +1173,56 @@ void finish_flight(st_ctx *ctx, InFlight &F) {
     F.scenes.clear();
     F.busy = false;
     V.cv_done.notify_all();
+    // scene versions this batch was the last reader of go back to their scenes' spare lists
+    const int me = (int)(&F - V.flights.data());
+    for (size_t i = 0; i < V.retired.size();) {
+        auto &rd = V.retired[i].readers;
+        rd.erase(std::remove(rd.begin(), rd.end(), std::make_pair(me, F.launch_id)), rd.end());
+        if (rd.empty()) {
+            slot_of(ctx, V.retired[i].slot)->spare.push_back(V.retired[i].bufs);
+            V.retired.erase(V.retired.begin() + i);
+        } else {
+            i++;
+        }
+    }
+}
+
+// Give scene `slot` a private copy of its primitive and TLAS arrays when batches in flight still
+// read the current ones, so that a transform update can proceed at once: those batches keep the
+// version they were launched with.  The copy is device to device on the context's stream, which
+// the update that follows also uses.
+int new_scene_version(st_ctx *ctx, int slot) {
+    Server &V = ctx->server;
+    SceneSlot *S = slot_of(ctx, slot);
+    RetiredVersion old;
+    old.slot = slot;
+    for (size_t i = 0; i < V.flights.size(); i++)
+        if (V.flights[i].busy && V.flights[i].scenes.count(slot)) old.readers.push_back({(int)i, V.flights[i].launch_id});
+    if (old.readers.empty()) return ST_OK;
+    MotionBufs m;
+    if (!S->spare.empty()) {
+        m = S->spare.back();
+        S->spare.pop_back();
+    }
+    for (int k = 0; k < 7; k++) {
+        DevBuf *mine;
+        DevBuf *copy = motion_field(*S, m, k, &mine);
+        if (!mine->ptr) continue;
+        const int e = reserve(ctx, *copy, mine->bytes);
+        if (e != ST_OK) {
+            S->spare.push_back(m);
+            return e;
+        }
+        ST_CUDA(cudaMemcpyAsync(copy->ptr, mine->ptr, mine->bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    for (int k = 0; k < 7; k++) {
+        DevBuf *mine;
+        DevBuf *copy = motion_field(*S, m, k, &mine);
+        std::swap(*mine, *copy);
+    }
+    old.bufs = m;                       // after the swap: the buffers the readers hold
+    V.retired.push_back(old);
+    return ST_OK;
 }
 
 // Enqueue one admitted batch on its flight's stream: view table, per-view SSB and ray rows, the
@@ -1192,15 +1272,11 @@ int enqueue_flight(st_ctx *ctx, InFlight &F, BatchPlan &p, std::vector<std::shar
 int launch_flight(st_ctx *ctx, int f, std::vector<std::shared_ptr<ServeReq>> &reqs) {
     Server &V = ctx->server;
     InFlight &F = V.flights[f];
-    // transform updates, in submission order; a scene read by an in-flight batch is waited for first
+    // transform updates, in submission order; a scene read by a batch in flight gets a new version
     std::map<int, uint32_t> moved_count;
     for (auto &r : reqs) {
         if (r->moved.empty()) continue;
-        for (InFlight &G : V.flights)
-            if (G.busy && G.scenes.count(r->slot)) {
-                cudaEventSynchronize(G.done_ev);
-                finish_flight(ctx, G);
-            }
+        ST_TRY(new_scene_version(ctx, r->slot));
         ST_TRY(st_update_primitives(ctx, r->slot, r->moved.data(), r->moved_ids.data(), (uint32_t)r->moved.size()));
         moved_count[r->slot] += (uint32_t)r->moved.size();
     }
@@ -1266,30 +1342,33 @@ int launch_flight(st_ctx *ctx, int f, std::vector<std::shared_ptr<ServeReq>> &re
         if (r->out_float) { r->host_float = host; host += align256(sizeof(FloatPixel) * grid); }
         if (r->out_u8) { r->host_u8 = host; host += align256((size_t)(r->view.grid_w - 1) * (r->view.grid_h - 1) * 4); }
     }
-    if (F.pinned_cap < host) {
+    if (F.pinned_cap < host) {                  // grows geometrically: cudaFreeHost waits for the device
+        const size_t cap = std::max(host, 2 * F.pinned_cap);
         if (F.pinned) cudaFreeHost(F.pinned);
         F.pinned = nullptr;
         F.pinned_cap = 0;
-        ST_CUDA(cudaMallocHost((void **)&F.pinned, host));
-        F.pinned_cap = host;
+        ST_CUDA(cudaMallocHost((void **)&F.pinned, cap));
+        F.pinned_cap = cap;
     }
     ST_TRY(reserve(ctx, F.B.table, sizeof(BatchView) * n));
     ST_TRY(reserve(ctx, F.B.counter, 16));
     if (F.B.staging_cap < (size_t)n) {
+        const size_t cap = std::max((size_t)n, (size_t)std::max(V.cfg.max_views_per_batch, 1));
         if (F.B.staging) cudaFreeHost(F.B.staging);
         F.B.staging = nullptr;
         F.B.staging_cap = 0;
-        ST_CUDA(cudaMallocHost((void **)&F.B.staging, sizeof(BatchView) * n));
-        F.B.staging_cap = n;
+        ST_CUDA(cudaMallocHost((void **)&F.B.staging, sizeof(BatchView) * cap));
+        F.B.staging_cap = cap;
     }
     cudaStream_t st = F.stream;
     char *arena = nullptr;
-    ST_CUDA(cudaMallocAsync((void **)&arena, std::max(dev, (size_t)256), st));
+    ST_CUDA(cudaMallocFromPoolAsync((void **)&arena, std::max(dev, (size_t)256), V.pool, st));
     const int s = enqueue_flight(ctx, F, p, reqs, tile, chunk, arena);
     cudaFreeAsync(arena, st);   // stream-ordered: released once the batch's work has run
     ST_TRY(s);
     const double t = st_clock();
     for (auto &r : reqs) r->launch = t;
+    F.launch_id = V.next_launch++;
     F.bytes = dev;
     F.reqs = reqs;
     F.busy = true;
@@ -1380,7 +1459,19 @@ int st_serve_start(st_ctx *ctx, const st_serve_config *cfg) {
         ST_CUDA(cudaStreamCreateWithFlags(&F.stream, cudaStreamNonBlocking));
         ST_CUDA(cudaEventCreateWithFlags(&F.done_ev, cudaEventDisableTiming));
         ST_TRY(reserve(ctx, F.status, 16));
+        F.pinned_cap = 64u << 20;              // output staging; grows if a batch needs more
+        ST_CUDA(cudaMallocHost((void **)&F.pinned, F.pinned_cap));
     }
+    // batch arenas come from a pool that keeps what batches free (the default pool would hand
+    // memory back at every synchronisation and map it again for the next batch)
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = ctx->device;
+    ST_CUDA(cudaMemPoolCreate(&V.pool, &props));
+    uint64_t keep = UINT64_MAX;
+    ST_CUDA(cudaMemPoolSetAttribute(V.pool, cudaMemPoolAttrReleaseThreshold, &keep));
     V.stop = false;
     V.running = true;
     V.inflight_bytes = 0;
@@ -1474,6 +1565,13 @@ int st_serve_stop(st_ctx *ctx) {
         if (F.stream) cudaStreamDestroy(F.stream);
     }
     V.flights.clear();
+    for (RetiredVersion &rv : V.retired) slot_of(ctx, rv.slot)->spare.push_back(rv.bufs);
+    V.retired.clear();
+    if (V.pool) {
+        cudaDeviceSynchronize();
+        cudaMemPoolDestroy(V.pool);
+        V.pool = nullptr;
+    }
     V.running = false;
     return ST_OK;
 }
