@@ -69,6 +69,35 @@ __device__ __forceinline__ bool trace_mesh(TState<CNT> &t, const SceneDev &S, co
     u32t sp = 0;
     bool found = false;
     for (;;) {
+        // inner nodes until this lane has leaves queued ("while-while": lanes of a warp walk nodes
+        // together and test triangles together; each lane's own order of tests is unchanged)
+        while (leaves == 0 && pair != kNoPair) {
+            const NodePair P = load_pair(pairs + pair);
+            t.count(C_AABB, 2);
+            bool hl = hit_aabb(V(P.a.x, P.a.y, P.a.z), V(P.a.w, P.b.x, P.b.y), ray, closest.distance, ld);
+            bool hr = hit_aabb(V(P.b.z, P.b.w, P.c.x), V(P.c.y, P.c.z, P.c.w), ray, closest.distance, rd);
+            bool lgo = hl, rgo = hr;
+            if (hl && P.d.y) { leaf_first[leaves] = P.d.x; leaf_count[leaves] = P.d.y; leaves++; lgo = false; }
+            if (hr && P.d.w) { leaf_first[leaves] = P.d.z; leaf_count[leaves] = P.d.w; leaves++; rgo = false; }
+            if (lgo) {
+                u32t near_pair = P.d.x, far_pair = P.d.z;
+                if (rgo) {
+                    if (!any_hit && ld > rd) { near_pair = P.d.z; far_pair = P.d.x; }
+                    if (sp >= kStack) {           // the queued leaves still run, then the walk ends
+                        t.status |= S_STACK_OVERFLOW;
+                        pair = kNoPair;
+                        continue;
+                    }
+                    t.mesh_stack[sp++] = far_pair;
+                }
+                pair = near_pair;
+            } else if (rgo) {
+                pair = P.d.z;
+            } else {
+                pair = sp ? t.mesh_stack[--sp] : kNoPair;
+            }
+        }
+        if (!leaves) break;
 #pragma unroll 1
         for (int k = 0; k < leaves; k++)
             if (hit_triangles(t, S, M.tri_offset + leaf_first[k], leaf_count[k], any_hit)) {
@@ -78,30 +107,6 @@ __device__ __forceinline__ bool trace_mesh(TState<CNT> &t, const SceneDev &S, co
             }
         leaves = 0;
         if (pair == kNoPair) break;
-        const NodePair P = load_pair(pairs + pair);
-        t.count(C_AABB, 2);
-        bool hl = hit_aabb(V(P.a.x, P.a.y, P.a.z), V(P.a.w, P.b.x, P.b.y), ray, closest.distance, ld);
-        bool hr = hit_aabb(V(P.b.z, P.b.w, P.c.x), V(P.c.y, P.c.z, P.c.w), ray, closest.distance, rd);
-        bool lgo = hl, rgo = hr;
-        if (hl && P.d.y) { leaf_first[leaves] = P.d.x; leaf_count[leaves] = P.d.y; leaves++; lgo = false; }
-        if (hr && P.d.w) { leaf_first[leaves] = P.d.z; leaf_count[leaves] = P.d.w; leaves++; rgo = false; }
-        if (lgo) {
-            u32t near_pair = P.d.x, far_pair = P.d.z;
-            if (rgo) {
-                if (!any_hit && ld > rd) { near_pair = P.d.z; far_pair = P.d.x; }
-                if (sp >= kStack) {               // the queued leaves still run, then the walk ends
-                    t.status |= S_STACK_OVERFLOW;
-                    pair = kNoPair;
-                    continue;
-                }
-                t.mesh_stack[sp++] = far_pair;
-            }
-            pair = near_pair;
-        } else if (rgo) {
-            pair = P.d.z;
-        } else {
-            pair = sp ? t.mesh_stack[--sp] : kNoPair;
-        }
     }
     return found;
 }
@@ -215,6 +220,33 @@ __device__ __forceinline__ bool trace_scene(TState<CNT> &t, const SceneDev &S, R
     u32t sp = 0;
     bool found = false;
     for (;;) {
+        while (leaves == 0 && pair != kNoPair) {      // inner nodes until leaves are queued
+            const NodePair P = load_pair(S.tlas_pairs + pair);
+            t.count(C_AABB, 2);
+            bool hl = hit_aabb(V(P.a.x, P.a.y, P.a.z), V(P.a.w, P.b.x, P.b.y), ray, t.closest.distance, ld);
+            bool hr = hit_aabb(V(P.b.z, P.b.w, P.c.x), V(P.c.y, P.c.z, P.c.w), ray, t.closest.distance, rd);
+            bool lgo = hl, rgo = hr;
+            if (hl && P.d.y) { leaf_first[leaves] = P.d.x; leaf_count[leaves] = P.d.y; leaves++; lgo = false; }
+            if (hr && P.d.w) { leaf_first[leaves] = P.d.z; leaf_count[leaves] = P.d.w; leaves++; rgo = false; }
+            if (lgo) {
+                u32t near_pair = P.d.x, far_pair = P.d.z;
+                if (rgo) {
+                    if (!any_hit && ld > rd) { near_pair = P.d.z; far_pair = P.d.x; }
+                    if (sp >= kStack) {           // the queued leaves still run, then the walk ends
+                        t.status |= S_STACK_OVERFLOW;
+                        pair = kNoPair;
+                        continue;
+                    }
+                    t.scene_stack[sp++] = far_pair;
+                }
+                pair = near_pair;
+            } else if (rgo) {
+                pair = P.d.z;
+            } else {
+                pair = sp ? t.scene_stack[--sp] : kNoPair;
+            }
+        }
+        if (!leaves) break;
 #pragma unroll 1
         for (int k = 0; k < leaves; k++)
             if (hit_primitives(t, S, ray, S.tlas_leaf_ids, leaf_first[k], leaf_count[k], any_hit, ssb, x, y, cone_angle)) {
@@ -223,30 +255,6 @@ __device__ __forceinline__ bool trace_scene(TState<CNT> &t, const SceneDev &S, R
             }
         leaves = 0;
         if (pair == kNoPair) break;
-        const NodePair P = load_pair(S.tlas_pairs + pair);
-        t.count(C_AABB, 2);
-        bool hl = hit_aabb(V(P.a.x, P.a.y, P.a.z), V(P.a.w, P.b.x, P.b.y), ray, t.closest.distance, ld);
-        bool hr = hit_aabb(V(P.b.z, P.b.w, P.c.x), V(P.c.y, P.c.z, P.c.w), ray, t.closest.distance, rd);
-        bool lgo = hl, rgo = hr;
-        if (hl && P.d.y) { leaf_first[leaves] = P.d.x; leaf_count[leaves] = P.d.y; leaves++; lgo = false; }
-        if (hr && P.d.w) { leaf_first[leaves] = P.d.z; leaf_count[leaves] = P.d.w; leaves++; rgo = false; }
-        if (lgo) {
-            u32t near_pair = P.d.x, far_pair = P.d.z;
-            if (rgo) {
-                if (!any_hit && ld > rd) { near_pair = P.d.z; far_pair = P.d.x; }
-                if (sp >= kStack) {               // the queued leaves still run, then the walk ends
-                    t.status |= S_STACK_OVERFLOW;
-                    pair = kNoPair;
-                    continue;
-                }
-                t.scene_stack[sp++] = far_pair;
-            }
-            pair = near_pair;
-        } else if (rgo) {
-            pair = P.d.z;
-        } else {
-            pair = sp ? t.scene_stack[--sp] : kNoPair;
-        }
     }
     return found;
 }
