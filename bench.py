@@ -18,6 +18,8 @@ roofline   the trace kernel: algorithmic bytes per frame (device event counters 
 cpu_baseline / --impl reference
            the reference's own renderer (oracle/_ref, compiled from the reference sources) on the
            same scene bytes, all host threads, over a bounded sample of rows
+dynamic    config 2: 4096 moving primitives, TLAS rebuilt (LBVH30, binned SAH) or refit every frame,
+           1280x720 depth 2, 300 frames: build ms (API wall time) and trace ms (device events)
 batched    64 views (resolutions from 256x256 to 1920x1080, 1-6 bounces) over 8 resident scenes:
            one st_render_batch call (persistent kernel, autotuned, CUDA graph) against one
            st_render_ex call per view, both timed with device events around the whole sequence
@@ -237,6 +239,9 @@ def mixed_workloads(r, big_sd, stream, rates):
                "chunk": batch.opt.chunk_used, "graph_replayed": batch.opt.graph_replayed}
     del fbuf, ubuf, one_f, one_u
     served = []
+    if rates:
+        # a short stream first: the server's staging, arenas and scene versions reach their sizes
+        MX.Stream(residents, slots, 200.0, 60, seed=499).serve(r)
     for k, rate in enumerate(rates):
         count = int(min(max(rate * 3.0, 60), 1500))
         stream_k = MX.Stream(residents, slots, rate, count, seed=500 + k)
@@ -244,6 +249,81 @@ def mixed_workloads(r, big_sd, stream, rates):
         pf = MX.latency_summary(stream_k.per_frame(r))
         served.append({"rate_req_s": rate, "requests": count, "served": srv, "per_frame": pf})
     return {"batched": batched, "served": served}
+
+
+def dynamic_tlas(r, frames, cpu_reference):
+    """Config 2: 4096 moving implicit primitives, the TLAS rebuilt (LBVH30 or binned SAH) or refit
+    every frame, 1280x720 depth 2.  Per frame: the primitive records go up (whole array), the TLAS
+    is updated through st_update_scene_bvh (wall time of the call, which includes its validity
+    check of the new node array), and the frame is traced (device events)."""
+    import torch
+    from slimtracin_b200 import api
+    L = api.lib()
+    out = {"primitives": 4096, "frames": frames, "width": 1280, "height": 720, "depth": 2}
+    slot = 12
+    for name, mode in (("lbvh30", api.ST_BVH_LBVH30), ("binned_sah", api.ST_BVH_BINNED_SAH),
+                       ("refit", api.ST_BVH_REFIT)):
+        sd, cam = scenes.config2()
+        r.upload(slot, sd, tlas=None)
+        r.build_tlas(slot, sd, api.ST_BVH_LBVH30)     # the topology a refit keeps
+        fr = scenes.Frame(1280, 720, cam, depth=2, with_pixels=False, with_float=False)
+        dev_f = torch.empty(fr.rays * 24, dtype=torch.uint8, device="cuda")
+        dev_u = torch.empty(1280 * 720 * 4, dtype=torch.uint8, device="cuda")
+        sc, keep = sd.to_ctypes()
+        opt = api.st_render_options()
+        opt.device_outputs, opt.out_float, opt.out_u8 = 1, dev_f.data_ptr(), dev_u.data_ptr()
+        up_ms, build_ms, trace_ms = [], [], []
+        for _ in range(frames):
+            scenes.advance_config2(sd, 1)           # in place: sc.primitives sees the new records
+            t0 = time.perf_counter()
+            r._check(L.st_upload_primitives(r.ctx, slot, C.byref(sc)), "st_upload_primitives")
+            t1 = time.perf_counter()
+            r._check(L.st_update_scene_bvh(r.ctx, slot, None, mode), "st_update_scene_bvh")
+            t2 = time.perf_counter()
+            r._check(L.st_render_ex(r.ctx, slot, C.byref(sc), C.byref(fr.viewport), C.byref(opt)), "st_render_ex")
+            up_ms.append((t1 - t0) * 1e3)
+            build_ms.append((t2 - t1) * 1e3)
+            trace_ms.append(opt.trace_ms)
+        out[name] = {"build_ms_p50": float(np.median(build_ms)), "build_ms_p99": float(np.percentile(build_ms, 99)),
+                     "upload_ms_p50": float(np.median(up_ms)),
+                     "trace_ms_p50": float(np.median(trace_ms)), "trace_ms_last": float(trace_ms[-1]),
+                     "mrays_s": fr.rays / (float(np.median(trace_ms)) / 1e3) / 1e6}
+        r.free(slot)
+    if cpu_reference:
+        # the reference's own updateSceneBVH (top-down SAH on one host thread), a bounded sample
+        try:
+            import oracle
+            if oracle.reference_available():
+                ref = oracle.reference()
+                sd, _ = scenes.config2()
+                sc, keep = sd.to_ctypes()
+                ts = []
+                for _ in range(5):
+                    scenes.advance_config2(sd, 1)
+                    t = time.perf_counter()
+                    ref.ref_update_scene_bvh(C.byref(sc))
+                    ts.append((time.perf_counter() - t) * 1e3)
+                out["reference_cpu_build_ms_p50"] = float(np.median(ts))
+        except Exception as ex:  # reported, never required
+            out["reference_cpu_build_ms_p50"] = f"failed: {ex}"
+    return out
+
+
+def measure_l2_gbs():
+    """Read bandwidth of a 48 MB float32 array that stays in the 126 MB L2 (torch.sum, CUDA events):
+    the denominator of the trace kernel's L2 fraction."""
+    import torch
+    x = torch.ones(12 << 20, dtype=torch.float32, device="cuda")
+    for _ in range(5):
+        x.sum()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 200
+    e0.record()
+    for _ in range(reps):
+        x.sum()
+    e1.record()
+    torch.cuda.synchronize()
+    return x.numel() * 4 * reps / (e0.elapsed_time(e1) / 1e3) / 1e9
 
 
 def blas_on_device(sd):
@@ -265,6 +345,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the batched-views and served-stream sections")
     ap.add_argument("--rates", default="50,200,1000,2000", help="served-stream arrival rates (req/s)")
+    ap.add_argument("--dynamic-frames", type=int, default=300, help="config-2 frames (0 skips the section)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -376,6 +457,9 @@ def main():
     d2h = grid * 24 + WIDTH * HEIGHT * 4
 
     mixed = None if args.no_mixed else mixed_workloads(r, sd, stream, [float(x) for x in args.rates.split(",") if x])
+    dynamic = dynamic_tlas(r, args.dynamic_frames, rank == 0 and world == 1 and not args.no_cpu_baseline) \
+        if args.dynamic_frames > 0 else None
+    l2_gbs = measure_l2_gbs()
 
     # ---- roofline of the trace kernel -----------------------------------------------------------
     trace_avg_ms = sum(trace_ms) / len(trace_ms)
@@ -426,8 +510,11 @@ def main():
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "trace_kernel", "kernel_ms": trace_avg_ms,
                          "bytes_alg_per_launch": bytes_alg,
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6.65 TB/s"},
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6.65 TB/s",
+                         "l2_peak": l2_gbs, "l2_frac": achieved / l2_gbs,
+                         "l2_peak_source": "48 MB L2-resident read (torch.sum), measured in this run"},
             "counters": counters,
+            "dynamic_tlas": dynamic,
             "batched": mixed["batched"] if mixed else None,
             "served": mixed["served"] if mixed else None,
             "clocks": clocks.summary(),

@@ -117,8 +117,10 @@ ST_API int st_upload_lights(st_ctx *ctx, int slot, const Scene *scene);
 ST_API int st_upload_scene_bvh(st_ctx *ctx, int slot, const Scene *scene);
 /* uploadMeshBVHs (core/init.h:111): every mesh's BLAS nodes and BVH-ordered Triangles as-is. */
 ST_API int st_upload_mesh_bvhs(st_ctx *ctx, int slot, const Scene *scene);
-/* Primitives whose transform changed since the last upload: re-upload only those records and mark
- * the TLAS dirty (serving path; the reference re-uploads the whole array, core/init.h:74). */
+/* Primitives whose transform changed since the last upload: primitives[k] replaces primitive
+ * ids[k]; the ids must be distinct and below the scene's primitive count (else ST_ERR_INVALID_ARG,
+ * nothing changed).  Only those records cross to the device, in one copy; the TLAS is then stale
+ * until st_update_scene_bvh (the reference re-uploads the whole array, core/init.h:74). */
 ST_API int st_update_primitives(st_ctx *ctx, int slot, const Primitive *primitives,
                          const uint32_t *ids, uint32_t count);
 ST_API int st_free_scene(st_ctx *ctx, int slot);

@@ -143,6 +143,9 @@ struct st_ctx {
     uint64_t budget = 0, in_use = 0;
     std::vector<SceneSlot> slots;
     DevBuf ssb, dirs, out_float, out_u8, prim_ids, status, counters;
+    DevBuf upd_host_dev;                 // st_update_primitives: records and ids on the device
+    char *upd_pinned = nullptr;          // ... and their pinned staging
+    size_t upd_pinned_cap = 0;
     LbvhScratch lbvh;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     std::string cuda_error;
@@ -357,8 +360,10 @@ void st_shutdown(st_ctx *ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (int i = 0; i < (int)ctx->slots.size(); i++) st_free_scene(ctx, i);
-    for (DevBuf *b : {&ctx->ssb, &ctx->dirs, &ctx->out_float, &ctx->out_u8, &ctx->prim_ids, &ctx->status, &ctx->counters})
+    for (DevBuf *b : {&ctx->ssb, &ctx->dirs, &ctx->out_float, &ctx->out_u8, &ctx->prim_ids, &ctx->status, &ctx->counters,
+                      &ctx->upd_host_dev})
         release(ctx, *b);
+    if (ctx->upd_pinned) cudaFreeHost(ctx->upd_pinned);
     lbvh_release(ctx->lbvh);
     for (DevBuf *b : {&ctx->batch.table, &ctx->batch.ssb, &ctx->batch.seg, &ctx->batch.out_float, &ctx->batch.out_u8,
                       &ctx->batch.counter})
@@ -596,12 +601,32 @@ int st_update_primitives(st_ctx *ctx, int slot, const Primitive *primitives, con
     SceneSlot *S = slot_of(ctx, slot);
     if (!S || !S->allocated || (count && (!primitives || !ids))) return ST_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
+    if (!count) return ST_OK;
+    // ids must be in range and distinct (the last write to an id would otherwise be undefined)
+    std::vector<uint8_t> seen(S->n_prims, 0);
     for (uint32_t k = 0; k < count; k++) {
-        if (ids[k] >= S->n_prims) return ST_ERR_INVALID_ARG;
-        S->prims_host[ids[k]] = primitives[k];
-        ST_CUDA(cudaMemcpyAsync(P<Primitive>(S->prims_raw) + ids[k], primitives + k, sizeof(Primitive), cudaMemcpyHostToDevice, ctx->stream));
+        if (ids[k] >= S->n_prims || seen[ids[k]]) return ST_ERR_INVALID_ARG;
+        seen[ids[k]] = 1;
     }
-    if (count) launch_make_primdev(P<Primitive>(S->prims_raw), S->n_prims, P<PrimDev>(S->prims), ctx->stream);
+    // one copy of the records and ids, then a scatter kernel (not one copy per primitive)
+    const size_t rec_bytes = sizeof(Primitive) * count, id_off = (rec_bytes + 255) & ~(size_t)255;
+    ST_TRY(reserve(ctx, ctx->upd_host_dev, id_off + sizeof(u32t) * count));
+    if (ctx->upd_pinned_cap < id_off + sizeof(u32t) * count) {
+        if (ctx->upd_pinned) cudaFreeHost(ctx->upd_pinned);
+        ctx->upd_pinned = nullptr;
+        ctx->upd_pinned_cap = 0;
+        const size_t cap = std::max(id_off + sizeof(u32t) * count, (size_t)1 << 20);
+        ST_CUDA(cudaMallocHost((void **)&ctx->upd_pinned, cap));
+        ctx->upd_pinned_cap = cap;
+    }
+    memcpy(ctx->upd_pinned, primitives, rec_bytes);
+    memcpy(ctx->upd_pinned + id_off, ids, sizeof(u32t) * count);
+    ST_CUDA(cudaMemcpyAsync(ctx->upd_host_dev.ptr, ctx->upd_pinned, id_off + sizeof(u32t) * count, cudaMemcpyHostToDevice,
+                            ctx->stream));
+    char *d = static_cast<char *>(ctx->upd_host_dev.ptr);
+    launch_scatter_prims(reinterpret_cast<const Primitive *>(d), reinterpret_cast<const u32t *>(d + id_off), count,
+                         P<Primitive>(S->prims_raw), P<PrimDev>(S->prims), ctx->stream);
+    for (uint32_t k = 0; k < count; k++) S->prims_host[ids[k]] = primitives[k];
     return ST_CUDA_SYNC(ctx);
 }
 

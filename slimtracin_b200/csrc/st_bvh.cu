@@ -592,17 +592,27 @@ __global__ void make_trihot_kernel(const Triangle *tris, u32t n, TriHot *hot) {
     h.s = make_float4(m.Z.x, m.Z.y, m.Z.z, 0.0f);
     hot[i] = h;
 }
-__global__ void make_primdev_kernel(const Primitive *prims, u32t n, PrimDev *out) {
-    u32t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const Primitive p = prims[i];
+__device__ __forceinline__ PrimDev primdev_of(const Primitive &p) {
     PrimDev d;
     unsigned bits = (unsigned)p.flags | ((unsigned)p.type << 8) | ((unsigned)p.material_id << 16);
     d.pos_bits = make_float4(p.position.x, p.position.y, p.position.z, __uint_as_float(bits));
     d.rot = make_float4(p.rotation.axis.x, p.rotation.axis.y, p.rotation.axis.z, p.rotation.amount);
     d.scale_id = make_float4(p.scale.x, p.scale.y, p.scale.z, __uint_as_float(p.id));
     d.inv_scale = make_float4(1.0f / p.scale.x, 1.0f / p.scale.y, 1.0f / p.scale.z, 0.0f);
-    out[i] = d;
+    return d;
+}
+__global__ void make_primdev_kernel(const Primitive *prims, u32t n, PrimDev *out) {
+    u32t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = primdev_of(prims[i]);
+}
+// Moved primitives: record k replaces primitive ids[k] (raw record and its PrimDev).  Ids are
+// distinct within one call (the host checks), so no two threads write the same slot.
+__global__ void scatter_prims_kernel(const Primitive *recs, const u32t *ids, u32t count, Primitive *raw, PrimDev *dev) {
+    u32t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const Primitive p = recs[k];
+    raw[ids[k]] = p;
+    dev[ids[k]] = primdev_of(p);
 }
 
 void launch_prim_aabbs(const Primitive *prims, const MeshDev *meshes, u32t n, float *aabbs, cudaStream_t st) {
@@ -625,6 +635,10 @@ void launch_make_trihot(const Triangle *tris, u32t n, TriHot *hot, cudaStream_t 
 }
 void launch_make_primdev(const Primitive *prims, u32t n, PrimDev *out, cudaStream_t st) {
     if (n) make_primdev_kernel<<<(n + 127) / 128, 128, 0, st>>>(prims, n, out);
+}
+void launch_scatter_prims(const Primitive *recs, const u32t *ids, u32t count, Primitive *raw, PrimDev *dev,
+                          cudaStream_t st) {
+    if (count) scatter_prims_kernel<<<(count + 127) / 128, 128, 0, st>>>(recs, ids, count, raw, dev);
 }
 
 }  // namespace st

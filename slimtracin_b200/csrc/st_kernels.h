@@ -104,5 +104,8 @@ void launch_make_pairs(const BVHNode *nodes, u32t node_count, NodePair *pairs, c
 void launch_make_trihot(const Triangle *tris, u32t n, TriHot *hot, cudaStream_t st);
 // Primitive -> PrimDev
 void launch_make_primdev(const Primitive *prims, u32t n, PrimDev *out, cudaStream_t st);
+// recs[k] replaces primitive ids[k] (distinct ids): raw record and PrimDev
+void launch_scatter_prims(const Primitive *recs, const u32t *ids, u32t count, Primitive *raw, PrimDev *dev,
+                          cudaStream_t st);
 
 }  // namespace st
