@@ -214,7 +214,8 @@ typedef struct st_serve_config {
     int max_views_per_batch;    /* 0 -> 64 */
     uint64_t frame_budget;      /* device bytes for in-flight frame/ray buffers; 0 -> budget - resident scenes */
     int tile_shape, chunk;      /* -1 / 0: the autotuned choice for the scene class, else 8x4 and 1 */
-    double refit_fraction;      /* moved/total below which the TLAS is refit, else rebuilt (LBVH30); 0 -> 0.25 */
+    double refit_fraction;      /* primitives moved since the scene's last full TLAS build, as a fraction of
+                                   all, below which the TLAS is refit, else rebuilt (LBVH30); 0 -> 0.25 */
 } st_serve_config;
 
 typedef struct st_request {

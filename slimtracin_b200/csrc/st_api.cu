@@ -43,6 +43,7 @@ struct SceneSlot {
     DevBuf prims_raw, prims, materials, lights;
     DevBuf tlas_nodes, tlas_leaf_ids, tlas_pairs, tlas_aabbs, tlas_scratch;
     u32t tlas_node_count = 0, tlas_height = 0;
+    u32t moved_since_build = 0;            // primitives moved since the TLAS was last built in full
     bool tlas_valid = false;
     BVHNode tlas_root{};
     DevBuf meshes, mesh_pairs, tri_hot, tri_full;
@@ -144,6 +145,7 @@ struct st_ctx {
     std::vector<SceneSlot> slots;
     DevBuf ssb, dirs, out_float, out_u8, prim_ids, status, counters;
     DevBuf upd_host_dev;                 // st_update_primitives: records and ids on the device
+    DevBuf sah_scratch;                  // binned-SAH builds (kept between builds)
     char *upd_pinned = nullptr;          // ... and their pinned staging
     size_t upd_pinned_cap = 0;
     LbvhScratch lbvh;
@@ -361,7 +363,7 @@ void st_shutdown(st_ctx *ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (int i = 0; i < (int)ctx->slots.size(); i++) st_free_scene(ctx, i);
     for (DevBuf *b : {&ctx->ssb, &ctx->dirs, &ctx->out_float, &ctx->out_u8, &ctx->prim_ids, &ctx->status, &ctx->counters,
-                      &ctx->upd_host_dev})
+                      &ctx->upd_host_dev, &ctx->sah_scratch})
         release(ctx, *b);
     if (ctx->upd_pinned) cudaFreeHost(ctx->upd_pinned);
     lbvh_release(ctx->lbvh);
@@ -549,6 +551,7 @@ int st_upload_scene_bvh(st_ctx *ctx, int slot, const Scene *scene) {
     S->tlas_height = scene->bvh.height;
     ST_CUDA(cudaMemcpyAsync(S->tlas_nodes.ptr, scene->bvh.nodes, sizeof(BVHNode) * S->tlas_node_count, cudaMemcpyHostToDevice, ctx->stream));
     ST_CUDA(cudaMemcpyAsync(S->tlas_leaf_ids.ptr, scene->bvh.leaf_ids, sizeof(u32t) * n, cudaMemcpyHostToDevice, ctx->stream));
+    S->moved_since_build = 0;
     return finish_tlas(ctx, *S);
 }
 
@@ -653,8 +656,9 @@ int st_update_scene_bvh(st_ctx *ctx, int slot, Scene *scene, int mode) {
         if (lbvh_reserve(ctx->lbvh, n) != cudaSuccess) return ST_ERR_OUT_OF_MEMORY;
         launch_prim_aabbs(P<Primitive>(S->prims_raw), P<MeshDev>(S->meshes), n, ctx->lbvh.aabbs, ctx->stream);
         u32t info[2];
+        ST_TRY(reserve(ctx, ctx->sah_scratch, sah_scratch_bytes(n)));
         cudaError_t e = sah_build(ctx->lbvh.aabbs, n, MAX_OBJS_PER_SCENE_BVH_NODE, P<BVHNode>(S->tlas_nodes),
-                                  P<u32t>(S->tlas_leaf_ids), info, ctx->stream);
+                                  P<u32t>(S->tlas_leaf_ids), info, ctx->stream, ctx->sah_scratch.ptr, ctx->sah_scratch.bytes);
         if (e != cudaSuccess) return fail_cuda(ctx, e);
         S->tlas_node_count = info[0];
         S->tlas_height = info[1];
@@ -680,6 +684,7 @@ int st_update_scene_bvh(st_ctx *ctx, int slot, Scene *scene, int mode) {
     if (!check_bvh(host.data(), S->tlas_node_count, n, S->tlas_height)) return ST_ERR_BAD_SCENE;
     for (u32t i = 0; i < n; i++) if (ids[i] >= n) return ST_ERR_BAD_SCENE;
     ST_TRY(finish_tlas(ctx, *S));
+    if (mode != ST_BVH_REFIT) S->moved_since_build = 0;
     if (scene && scene->bvh.nodes && scene->bvh.leaf_ids) {
         ST_CUDA(cudaMemcpyAsync(scene->bvh.nodes, S->tlas_nodes.ptr, sizeof(BVHNode) * S->tlas_node_count, cudaMemcpyDeviceToHost, ctx->stream));
         ST_CUDA(cudaMemcpyAsync(scene->bvh.leaf_ids, S->tlas_leaf_ids.ptr, sizeof(u32t) * n, cudaMemcpyDeviceToHost, ctx->stream));
@@ -735,7 +740,8 @@ int st_update_mesh_bvh(st_ctx *ctx, Mesh *mesh, int mode) {
     u32t info[2];
     cudaError_t e = mode == ST_BVH_LBVH30
         ? lbvh_build(ctx->lbvh, n, MAX_TRIANGLES_PER_MESH_BVH_NODE, nodes, order, info, st)
-        : sah_build(ctx->lbvh.aabbs, n, MAX_TRIANGLES_PER_MESH_BVH_NODE, nodes, order, info, st);
+        : sah_build(ctx->lbvh.aabbs, n, MAX_TRIANGLES_PER_MESH_BVH_NODE, nodes, order, info, st,
+                    ctx->sah_scratch.ptr, ctx->sah_scratch.bytes);
     if (e == cudaSuccess) {
         launch_tri_records(pos, nrm, uv, pidx, nidx, uidx, mesh->uvs_count ? 1 : 0, order, n, tris, inverse, st);
         cudaMemcpyAsync(mesh->bvh.nodes, nodes, sizeof(BVHNode) * info[0], cudaMemcpyDeviceToHost, st);
@@ -771,7 +777,8 @@ int st_build_bvh(st_ctx *ctx, int mode, const float *aabbs, uint32_t n, uint32_t
     cudaMemcpyAsync(ctx->lbvh.aabbs, aabbs, sizeof(float) * 6 * (size_t)n, cudaMemcpyHostToDevice, st);
     u32t inf[2];
     cudaError_t e = mode == ST_BVH_LBVH30 ? lbvh_build(ctx->lbvh, n, max_leaf, d_nodes, d_order, inf, st)
-                                          : sah_build(ctx->lbvh.aabbs, n, max_leaf, d_nodes, d_order, inf, st);
+                                          : sah_build(ctx->lbvh.aabbs, n, max_leaf, d_nodes, d_order, inf, st, ctx->sah_scratch.ptr,
+                                                    ctx->sah_scratch.bytes);
     if (e == cudaSuccess) {
         if (mode == ST_BVH_LBVH30) launch_codes_by_item(ctx->lbvh, n, d_codes, st);
         else codes = nullptr;
@@ -1307,7 +1314,10 @@ int launch_flight(st_ctx *ctx, int f, std::vector<std::shared_ptr<ServeReq>> &re
     }
     for (auto &kv : moved_count) {
         SceneSlot *S = slot_of(ctx, kv.first);
-        const int mode = (double)kv.second < V.cfg.refit_fraction * S->n_prims ? ST_BVH_REFIT : ST_BVH_LBVH30;
+        // refit while the primitives moved since the last full build stay below the fraction: a
+        // refit keeps the topology, whose quality decays as motion accumulates
+        S->moved_since_build += kv.second;
+        const int mode = (double)S->moved_since_build < V.cfg.refit_fraction * S->n_prims ? ST_BVH_REFIT : ST_BVH_LBVH30;
         ST_TRY(st_update_scene_bvh(ctx, kv.first, nullptr, mode));
     }
     // view table and arena layout

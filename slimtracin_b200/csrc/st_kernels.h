@@ -82,8 +82,10 @@ void lbvh_carve(LbvhScratch &s, void *base, u32t cap);
 cudaError_t lbvh_build(LbvhScratch &s, u32t n, u32t max_leaf, BVHNode *out_nodes, u32t *out_order,
                        u32t info[2], cudaStream_t st);
 // Binned SAH over n device boxes (st_sah.cu): reference-layout nodes (2n capacity) + leaf order.
+// scratch (optional, sah_scratch_bytes(n) bytes): used instead of a stream-ordered allocation
 cudaError_t sah_build(const float *aabbs, u32t n, u32t max_leaf, BVHNode *out_nodes, u32t *out_order, u32t info[2],
-                      cudaStream_t st);
+                      cudaStream_t st, void *scratch = nullptr, size_t scratch_bytes = 0);
+size_t sah_scratch_bytes(u32t n);
 // After lbvh_build: the Morton code of every item, by item index.
 void launch_codes_by_item(const LbvhScratch &s, u32t n, u32t *out, cudaStream_t st);
 // World boxes of primitives as updateSceneBVH computes them (builder_top_down.h:370-377).

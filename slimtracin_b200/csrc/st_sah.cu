@@ -485,26 +485,46 @@ struct SahScratch {
 
 void scan_exclusive_u32(const u32t *in, u32t *out, u32t n, u32t *sums, u32t *total, cudaStream_t st);
 
-cudaError_t sah_build(const float *aabbs, u32t n, u32t max_leaf, BVHNode *out_nodes, u32t *out_order, u32t info[2],
-                      cudaStream_t st) {
-    if (n == 0) { info[0] = info[1] = 0; return cudaSuccess; }
-    // scratch: centroids, tmp ids, two task lists, flags/scans (3n each), large lists, bins, decisions
+namespace {
+struct SahLayout {
+    size_t o_cent, o_tmp, o_ta, o_tb, o_flags, o_scan, o_sums, o_large, o_ctask, o_cleft, o_bins, o_ldec, o_sdec, o_misc;
+    size_t bytes = 0;
+};
+// scratch: centroids, tmp ids, two task lists, flags/scans (3n each), large lists, bins, decisions
+SahLayout sah_layout(u32t n) {
+    SahLayout L;
     const size_t nb = n;
     const u32t max_large = (u32t)(n / kSmall + 2);
     const size_t max_chunks = n / kChunk + max_large + 2;
-    size_t bytes = 0;
-    auto add = [&](size_t b) { size_t off = bytes; bytes += (b + 255) & ~(size_t)255; return off; };
-    size_t o_cent = add(sizeof(float) * 3 * nb), o_tmp = add(sizeof(u32t) * nb);
-    size_t o_ta = add(sizeof(SahTask) * nb), o_tb = add(sizeof(SahTask) * nb);
-    size_t o_flags = add(sizeof(u32t) * 3 * nb + 64), o_scan = add(sizeof(u32t) * 3 * nb + 64);
-    size_t o_sums = add(sizeof(u32t) * (3 * nb / 1024 + 64));
-    size_t o_large = add(sizeof(u32t) * max_large), o_ctask = add(sizeof(u32t) * max_chunks);
-    size_t o_cleft = add(sizeof(u32t) * max_chunks);
-    size_t o_bins = add(sizeof(unsigned) * (size_t)max_large * 3 * kBins * kBinWords);
-    size_t o_ldec = add(sizeof(SahDecision) * max_large), o_sdec = add(sizeof(SahDecision) * nb);
-    size_t o_misc = add(sizeof(u32t) * 64);
+    auto add = [&](size_t b) { size_t off = L.bytes; L.bytes += (b + 255) & ~(size_t)255; return off; };
+    L.o_cent = add(sizeof(float) * 3 * nb); L.o_tmp = add(sizeof(u32t) * nb);
+    L.o_ta = add(sizeof(SahTask) * nb); L.o_tb = add(sizeof(SahTask) * nb);
+    L.o_flags = add(sizeof(u32t) * 3 * nb + 64); L.o_scan = add(sizeof(u32t) * 3 * nb + 64);
+    L.o_sums = add(sizeof(u32t) * (3 * nb / 1024 + 64));
+    L.o_large = add(sizeof(u32t) * max_large); L.o_ctask = add(sizeof(u32t) * max_chunks);
+    L.o_cleft = add(sizeof(u32t) * max_chunks);
+    L.o_bins = add(sizeof(unsigned) * (size_t)max_large * 3 * kBins * kBinWords);
+    L.o_ldec = add(sizeof(SahDecision) * max_large); L.o_sdec = add(sizeof(SahDecision) * nb);
+    L.o_misc = add(sizeof(u32t) * 64);
+    return L;
+}
+}  // namespace
+
+size_t sah_scratch_bytes(u32t n) { return sah_layout(n).bytes; }
+
+cudaError_t sah_build(const float *aabbs, u32t n, u32t max_leaf, BVHNode *out_nodes, u32t *out_order, u32t info[2],
+                      cudaStream_t st, void *scratch, size_t scratch_bytes) {
+    if (n == 0) { info[0] = info[1] = 0; return cudaSuccess; }
+    const SahLayout Lo = sah_layout(n);
+    const size_t o_cent = Lo.o_cent, o_tmp = Lo.o_tmp, o_ta = Lo.o_ta, o_tb = Lo.o_tb, o_flags = Lo.o_flags,
+                 o_scan = Lo.o_scan, o_sums = Lo.o_sums, o_large = Lo.o_large, o_ctask = Lo.o_ctask,
+                 o_cleft = Lo.o_cleft, o_bins = Lo.o_bins, o_ldec = Lo.o_ldec, o_sdec = Lo.o_sdec, o_misc = Lo.o_misc;
+    // the caller's scratch when it is large enough, else a stream-ordered allocation
     char *base = nullptr;
-    cudaError_t e = cudaMallocAsync((void **)&base, bytes, st);
+    const bool own = !(scratch && scratch_bytes >= Lo.bytes);
+    cudaError_t e = cudaSuccess;
+    if (own) e = cudaMallocAsync((void **)&base, Lo.bytes, st);
+    else base = static_cast<char *>(scratch);
     if (e != cudaSuccess) return e;
     float *cent = (float *)(base + o_cent);
     u32t *tmp = (u32t *)(base + o_tmp);
@@ -556,7 +576,7 @@ cudaError_t sah_build(const float *aabbs, u32t n, u32t max_leaf, BVHNode *out_no
         cudaMemcpyAsync(&h, misc + 20, sizeof(u32t), cudaMemcpyDeviceToHost, st);
         e = cudaStreamSynchronize(st);
     }
-    cudaFreeAsync(base, st);
+    if (own) cudaFreeAsync(base, st);
     cudaError_t e2 = cudaStreamSynchronize(st);
     info[0] = 1 + 2 * pairs;
     info[1] = h < 1 ? 1 : h;

@@ -213,6 +213,7 @@ class Stream:
         opt = api.st_render_options()
         opt.skip_float_copy = 1
         res = []
+        moved_since = {}
         t0 = L.st_clock() + 0.02
         for (si, w, h, fr, upd, ids, req), a in zip(self.requests, self.arrivals):
             arrival = t0 + a
@@ -222,7 +223,10 @@ class Stream:
                 renderer._check(L.st_update_primitives(ctx, slot, upd.ctypes.data, ids.ctypes.data, len(ids)),
                                 "st_update_primitives")
                 n = len(self.residents[si].sd.primitives)
-                mode = api.ST_BVH_REFIT if len(ids) < self.refit_fraction * n else api.ST_BVH_LBVH30
+                moved_since[si] = moved_since.get(si, 0) + len(ids)
+                mode = api.ST_BVH_REFIT if moved_since[si] < self.refit_fraction * n else api.ST_BVH_LBVH30
+                if mode != api.ST_BVH_REFIT:
+                    moved_since[si] = 0
                 renderer._check(L.st_update_scene_bvh(ctx, slot, None, mode), "st_update_scene_bvh")
             opt.out_u8 = self.out[(w, h)].ctypes.data
             renderer._check(L.st_render_ex(ctx, slot, C.byref(self.residents[si].sc), C.byref(fr.viewport),

@@ -76,11 +76,15 @@ def test_served_views_equal_views_rendered_alone():
             assert r.arrival_time <= r.launch_time <= r.completion_time
         # the same sequence, one request at a time
         n2 = len(scn[2][0].primitives)
+        moved_since_build = 0          # the server refits while this stays below the fraction
         for (si, w, h, d, m, moved), upd, fr, res in zip(reqs, updates, frames, results):
             sd, cam, _ = scn[si]
             if moved is not None:
                 alone.update_primitives(2, upd, moved)
-                mode = api.ST_BVH_REFIT if len(moved) < REFIT_FRACTION * n2 else api.ST_BVH_LBVH30
+                moved_since_build += len(moved)
+                mode = api.ST_BVH_REFIT if moved_since_build < REFIT_FRACTION * n2 else api.ST_BVH_LBVH30
+                if mode != api.ST_BVH_REFIT:
+                    moved_since_build = 0
                 alone.build_tlas(2, sd.copy(), mode)
             ref = scenes.Frame(w, h, cam, depth=d, mode=m)
             alone.render(si, sd, ref)
