@@ -397,78 +397,6 @@ __device__ __forceinline__ void apply_textures(TState<CNT> &t, const SceneDev &S
     }
 }
 
-template <bool CNT>
-__device__ v3 shade_surface(TState<CNT> &t, const SceneDev &S, RayD &ray, bool &lights_shaded) {   // surface.h:146
-    Hit &hit = t.closest;
-    v3 color = splat(0);
-    const Material *M = S.materials + hit.material_id;
-    t.count(C_SHADE);
-    if (M->is & EMISSIVE) return hit.from_behind ? color : from(M->emission);
-    float du = 0, dv = 0;
-    Shaded s;
-    s.viewing_origin = ray.origin;
-    s.viewing_direction = ray.direction;
-    s.prim_index = hit.object_id;
-    s.material = M;
-    s.albedo = from(M->albedo);
-    s.reflected_direction = splat(0);
-    if (M->use && M->texture_count) apply_textures(t, S, s, hit, *M, du, dv, true);
-    float NdotRd = 0, ior, max_distance = hit.distance;
-    v3 throughput = splat(1);
-    u32t depth = t.depth;
-    while (depth) {
-        s.position = ray.origin = hit.position;
-        s.normal = hit.from_behind ? neg(hit.normal) : hit.normal;
-        ior = hit.from_behind ? s.material->n2_over_n1 : s.material->n1_over_n2;
-        bool is_ref = (M->is & REFLECTIVE) || (M->is & REFRACTIVE);
-        if (is_ref || M->brdf == BRDF_Phong) {
-            NdotRd = -clamp01(-dot(s.normal, s.viewing_direction));      // invDotVec3 common.h:97
-            s.reflected_direction = vsfma(s.normal, -2.0f * NdotRd, s.viewing_direction);  // reflectWithDot :101
-        }
-        v3 current = is_ref ? splat(0) : from(S.ambient);
-        if (S.lights) current = shade_from_lights(t, S, s, ray, current);
-        if (S.n_emissive)
-            if (shade_from_emissive_quads(t, S, s, ray, current)) max_distance = hit.distance;
-        color = vvfma(current, throughput, color);
-        if (S.lights && shade_lights(t, S, s.viewing_origin, s.viewing_direction, max_distance, color))
-            lights_shaded = true;
-        if (is_ref && --depth) {
-            if (M->is & REFLECTIVE) ray.direction = s.reflected_direction;
-            else {                                                     // refract common.h:105
-                v3 Vv = s.viewing_direction, N = s.normal;
-                float c = ior * ior * (1 - (NdotRd * NdotRd));
-                if (c > 1) ray.direction = splat(0);
-                else {
-                    Vv = vscale(Vv, ior);
-                    Vv = vsfma(N, ior * -NdotRd - sqrtf(1 - c), Vv);
-                    ray.direction = norm(Vv);
-                }
-                if (ray.direction.x == 0 && ray.direction.y == 0 && ray.direction.z == 0)
-                    ray.direction = s.reflected_direction;
-            }
-            t.count(C_BOUNCE);
-            t.closest.distance = t.closest.distance_squared = INFINITY;       // traceRay trace.h:89
-            if (trace_scene(t, S, ray, false, nullptr, 0, 0, 0.0f, false, false)) {
-                t.count(C_SHADE);
-                s.prim_index = hit.object_id;
-                s.material = M = S.materials + hit.material_id;
-                s.albedo = from(M->albedo);
-                if (M->use && M->texture_count) apply_textures(t, S, s, hit, *M, du, dv, false);
-                if (hit.object_type == PrimitiveType_Quad && (M->is & EMISSIVE)) {
-                    color = hit.from_behind ? splat(0) : from(M->emission);
-                    break;
-                }
-                if (M->brdf != BRDF_CookTorrance) throughput = vmul(throughput, from(M->reflectivity));
-                s.viewing_origin = ray.origin;
-                s.viewing_direction = ray.direction;
-                continue;
-            }
-        }
-        break;
-    }
-    return color;
-}
-
 // ---- the frame kernels -----------------------------------------------------------------------
 // computeSSB render/SSB.h:5 for one primitive; the result is folded with IS_VISIBLE into one rect
 // (an invisible primitive gets an empty rect) so that the primary-ray cull is a single test.
@@ -592,42 +520,119 @@ __device__ __forceinline__ void trace_point(TState<CNT> &t, const SceneDev &S, c
     ray.origin = v.cam_pos;
     ray.direction = norm(current);
     ray.rcp = rcp(ray.direction);
+    pre_prep(ray);      // only the walk reads the prepared fields; every bounce ray prepares its own
     t.depth = v.depth;
     t.closest.distance = t.closest.distance_squared = INFINITY;
     t.closest.cone_width = 0;
     t.mesh_closest.object_type = PrimitiveType_Mesh;
     t.current.cone_width = 0;
     t.count(C_PRIMARY);
-    v3 Ro = ray.origin, Rd = ray.direction, color = splat(0);
-    bool lights_shaded = false;
-    bool hit_found;
-    {
-        RayD pr = ray;
-        pre_prep(pr);
-        hit_found = trace_scene(t, S, pr, false, ssb, (int)x, (int)y, v.cone_angle, true, !v.primary_tlas);
-    }
+    const v3 Ro = ray.origin, Rd = ray.direction;
+    v3 color = splat(0);
+    bool lights_shaded = false, hit_found = false;
+    float closest_distance = INFINITY, z = INFINITY;
     Hit &hit = t.closest;
-    if (prim_ids) prim_ids[idx] = hit_found ? hit.object_id : 0xFFFFFFFFu;
-    float closest_distance = hit_found ? hit.distance : INFINITY;
-    float z = INFINITY;
-    if (hit_found) {
-        z = qrot(hit.position - v.cam_pos, v.cam_rot_inv).z;
-        switch (v.mode) {
-            case RenderMode_Beauty: color = shade_surface(t, S, ray, lights_shaded); break;
-            case RenderMode_Depth: color = splat(4 / hit.distance); break;
-            case RenderMode_Normals: {
-                const Material &M = S.materials[hit.material_id];
-                if (M.texture_count > 1 && (M.use & NORMAL_MAP)) {
-                    float u = hit.u * M.uv_repeat.x, vv = hit.v * M.uv_repeat.y;
-                    hit.uv_area /= M.uv_repeat.x / M.uv_repeat.y;
-                    float du = duv_ray_cone(hit.NdotV, hit.cone_width, hit.area, hit.uv_area);
-                    q4 rot = normal_rotation(sample_normal(t, S, M.texture_ids[1], u, vv, du, 0.0f));
-                    hit.normal = qrot(hit.normal, rot);
+    // shadeSurface's state (surface.h:146)
+    Shaded s;
+    const Material *M = nullptr;
+    float du = 0, dv = 0, NdotRd = 0, ior = 0, max_distance = 0;
+    v3 throughput = splat(1);
+    u32t bounces = 0;                                       // shadeSurface's `depth`
+    bool primary = true;
+    // The primary ray and every bounce ray of shadeSurface's loop share this one trace site, so the
+    // kernel carries one inlined copy of the walk for both (shadow rays keep theirs).
+    for (;;) {
+        const bool found = trace_scene(t, S, ray, false, primary ? ssb : nullptr, (int)x, (int)y,
+                                       primary ? v.cone_angle : 0.0f, primary, primary && !v.primary_tlas);
+        if (primary) {                                      // rayTrace after the hit test (raytracer.h:89)
+            primary = false;
+            hit_found = found;
+            if (prim_ids) prim_ids[idx] = found ? hit.object_id : 0xFFFFFFFFu;
+            closest_distance = found ? hit.distance : INFINITY;
+            if (!found) break;
+            z = qrot(hit.position - v.cam_pos, v.cam_rot_inv).z;
+            if (v.mode != RenderMode_Beauty) {
+                switch (v.mode) {
+                    case RenderMode_Depth: color = splat(4 / hit.distance); break;
+                    case RenderMode_Normals: {
+                        const Material &NM = S.materials[hit.material_id];
+                        if (NM.texture_count > 1 && (NM.use & NORMAL_MAP)) {
+                            float u = hit.u * NM.uv_repeat.x, vv = hit.v * NM.uv_repeat.y;
+                            hit.uv_area /= NM.uv_repeat.x / NM.uv_repeat.y;
+                            float ndu = duv_ray_cone(hit.NdotV, hit.cone_width, hit.area, hit.uv_area);
+                            q4 rot = normal_rotation(sample_normal(t, S, NM.texture_ids[1], u, vv, ndu, 0.0f));
+                            hit.normal = qrot(hit.normal, rot);
+                        }
+                        color = V(0.5f * (hit.normal.x + 1), 0.5f * (hit.normal.y + 1), 0.5f * (hit.normal.z + 1));
+                    } break;
+                    case RenderMode_UVs: color = V(0.5f * hit.u, 0.5f * hit.v, 0.5f); break;
                 }
-                color = V(0.5f * (hit.normal.x + 1), 0.5f * (hit.normal.y + 1), 0.5f * (hit.normal.z + 1));
-            } break;
-            case RenderMode_UVs: color = V(0.5f * hit.u, 0.5f * hit.v, 0.5f); break;
+                break;
+            }
+            // shadeSurface (surface.h:146) up to its bounce loop
+            M = S.materials + hit.material_id;
+            t.count(C_SHADE);
+            if (M->is & EMISSIVE) {
+                if (!hit.from_behind) color = from(M->emission);
+                break;
+            }
+            s.viewing_origin = ray.origin;
+            s.viewing_direction = ray.direction;
+            s.prim_index = hit.object_id;
+            s.material = M;
+            s.albedo = from(M->albedo);
+            s.reflected_direction = splat(0);
+            if (M->use && M->texture_count) apply_textures(t, S, s, hit, *M, du, dv, true);
+            max_distance = hit.distance;
+            bounces = t.depth;
+        } else {                                            // traceRay returned (surface.h:214-239)
+            if (!found) break;
+            t.count(C_SHADE);
+            s.prim_index = hit.object_id;
+            s.material = M = S.materials + hit.material_id;
+            s.albedo = from(M->albedo);
+            if (M->use && M->texture_count) apply_textures(t, S, s, hit, *M, du, dv, false);
+            if (hit.object_type == PrimitiveType_Quad && (M->is & EMISSIVE)) {
+                color = hit.from_behind ? splat(0) : from(M->emission);
+                break;
+            }
+            if (M->brdf != BRDF_CookTorrance) throughput = vmul(throughput, from(M->reflectivity));
+            s.viewing_origin = ray.origin;
+            s.viewing_direction = ray.direction;
         }
+        // one iteration of shadeSurface's bounce loop
+        if (!bounces) break;
+        s.position = ray.origin = hit.position;
+        s.normal = hit.from_behind ? neg(hit.normal) : hit.normal;
+        ior = hit.from_behind ? s.material->n2_over_n1 : s.material->n1_over_n2;
+        const bool is_ref = (M->is & REFLECTIVE) || (M->is & REFRACTIVE);
+        if (is_ref || M->brdf == BRDF_Phong) {
+            NdotRd = -clamp01(-dot(s.normal, s.viewing_direction));      // invDotVec3 common.h:97
+            s.reflected_direction = vsfma(s.normal, -2.0f * NdotRd, s.viewing_direction);  // reflectWithDot :101
+        }
+        v3 cur = is_ref ? splat(0) : from(S.ambient);
+        if (S.lights) cur = shade_from_lights(t, S, s, ray, cur);
+        if (S.n_emissive)
+            if (shade_from_emissive_quads(t, S, s, ray, cur)) max_distance = hit.distance;
+        color = vvfma(cur, throughput, color);
+        if (S.lights && shade_lights(t, S, s.viewing_origin, s.viewing_direction, max_distance, color))
+            lights_shaded = true;
+        if (!(is_ref && --bounces)) break;
+        if (M->is & REFLECTIVE) ray.direction = s.reflected_direction;
+        else {                                                         // refract common.h:105
+            v3 Vv = s.viewing_direction, N = s.normal;
+            float c = ior * ior * (1 - (NdotRd * NdotRd));
+            if (c > 1) ray.direction = splat(0);
+            else {
+                Vv = vscale(Vv, ior);
+                Vv = vsfma(N, ior * -NdotRd - sqrtf(1 - c), Vv);
+                ray.direction = norm(Vv);
+            }
+            if (ray.direction.x == 0 && ray.direction.y == 0 && ray.direction.z == 0)
+                ray.direction = s.reflected_direction;
+        }
+        t.count(C_BOUNCE);
+        t.closest.distance = t.closest.distance_squared = INFINITY;           // traceRay trace.h:89
     }
     if (v.mode == RenderMode_Beauty && S.lights && !lights_shaded) {
         if (shade_lights(t, S, Ro, Rd, closest_distance, color)) {
