@@ -675,14 +675,17 @@ int st_update_scene_bvh(st_ctx *ctx, int slot, Scene *scene, int mode) {
     } else {
         return ST_ERR_INVALID_ARG;
     }
-    // the walk trusts every index it reads: check the device-built array before first use
-    std::vector<BVHNode> host(S->tlas_node_count);
-    std::vector<u32t> ids(n);
-    ST_CUDA(cudaMemcpyAsync(host.data(), S->tlas_nodes.ptr, sizeof(BVHNode) * host.size(), cudaMemcpyDeviceToHost, ctx->stream));
-    ST_CUDA(cudaMemcpyAsync(ids.data(), S->tlas_leaf_ids.ptr, sizeof(u32t) * n, cudaMemcpyDeviceToHost, ctx->stream));
-    ST_TRY(ST_CUDA_SYNC(ctx));
-    if (!check_bvh(host.data(), S->tlas_node_count, n, S->tlas_height)) return ST_ERR_BAD_SCENE;
-    for (u32t i = 0; i < n; i++) if (ids[i] >= n) return ST_ERR_BAD_SCENE;
+    // the walk trusts every index it reads: check a newly built array before first use (a refit
+    // rewrites boxes only, so the topology checked when it was built still holds)
+    if (mode != ST_BVH_REFIT) {
+        std::vector<BVHNode> host(S->tlas_node_count);
+        std::vector<u32t> ids(n);
+        ST_CUDA(cudaMemcpyAsync(host.data(), S->tlas_nodes.ptr, sizeof(BVHNode) * host.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        ST_CUDA(cudaMemcpyAsync(ids.data(), S->tlas_leaf_ids.ptr, sizeof(u32t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        ST_TRY(ST_CUDA_SYNC(ctx));
+        if (!check_bvh(host.data(), S->tlas_node_count, n, S->tlas_height)) return ST_ERR_BAD_SCENE;
+        for (u32t i = 0; i < n; i++) if (ids[i] >= n) return ST_ERR_BAD_SCENE;
+    }
     ST_TRY(finish_tlas(ctx, *S));
     if (mode != ST_BVH_REFIT) S->moved_since_build = 0;
     if (scene && scene->bvh.nodes && scene->bvh.leaf_ids) {
@@ -1507,6 +1510,28 @@ int st_serve_start(st_ctx *ctx, const st_serve_config *cfg) {
     ST_CUDA(cudaMemPoolCreate(&V.pool, &props));
     uint64_t keep = UINT64_MAX;
     ST_CUDA(cudaMemPoolSetAttribute(V.pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    {   // grow the pool now (up to 2 GB of the frame budget) rather than under the first heavy load
+        const size_t warm = (size_t)std::min<uint64_t>(V.frame_budget, 2ull << 30);
+        void *p = nullptr;
+        if (warm && cudaMallocFromPoolAsync(&p, warm, V.pool, ctx->stream) == cudaSuccess) cudaFreeAsync(p, ctx->stream);
+        cudaGetLastError();
+        ST_TRY(ST_CUDA_SYNC(ctx));
+    }
+    // spare scene versions for the resident scenes, so that the first updates under load do not
+    // allocate (one per batch that can be in flight)
+    for (int slot = 0; slot < (int)ctx->slots.size(); slot++) {
+        SceneSlot &S = ctx->slots[slot];
+        if (!S.allocated || !S.tlas_valid) continue;
+        while ((int)S.spare.size() < V.cfg.max_in_flight) {
+            MotionBufs m;
+            for (int k = 0; k < 7; k++) {
+                DevBuf *mine;
+                DevBuf *copy = motion_field(S, m, k, &mine);
+                if (mine->ptr) ST_TRY(reserve(ctx, *copy, mine->bytes));
+            }
+            S.spare.push_back(m);
+        }
+    }
     V.stop = false;
     V.running = true;
     V.inflight_bytes = 0;

@@ -675,12 +675,13 @@ __device__ __forceinline__ void flush_counters(TState<CNT> &t, unsigned *status,
     }
 }
 
-// ST_TRACE_MIN_BLOCKS (optional): resident 128-thread blocks per SM the register allocation must allow
-#ifdef ST_TRACE_MIN_BLOCKS
-#define ST_TRACE_BOUNDS __launch_bounds__(128, ST_TRACE_MIN_BLOCKS)
-#else
-#define ST_TRACE_BOUNDS __launch_bounds__(128)
+// Resident 128-thread blocks per SM the register allocation must allow.  Six (85 registers, more
+// spills) beat the compiler's own choice of 128 registers (four blocks) on the 1080p mesh frame:
+// 2.44 vs 2.62 ms; 5, 7 and 8 blocks measured 2.52, 2.45 and 2.38 ms, 2 blocks 5.6 ms.
+#ifndef ST_TRACE_MIN_BLOCKS
+#define ST_TRACE_MIN_BLOCKS 6
 #endif
+#define ST_TRACE_BOUNDS __launch_bounds__(128, ST_TRACE_MIN_BLOCKS)
 template <bool CNT>
 __global__ void ST_TRACE_BOUNDS trace_kernel(SceneDev S, ViewDev v, const int4 *ssb, const float *dirs,
                                                     FloatPixel *out, u32t *prim_ids, unsigned *status,
