@@ -150,7 +150,9 @@ ST_API int st_build_bvh(st_ctx *ctx, int mode, const float *aabbs, uint32_t n, u
  * float_pixels ((W+1)x(H+1), as renderScene leaves them after beginDrawing) and, when
  * frame_buffer->pixels is non-null, the resolved W x H BGRA pixels.  `scene` supplies the per-frame
  * values the reference passes by value to its kernel (counts, ambient light); the arrays come from
- * the device copy.  viewport->trace.depth is the bounce count. */
+ * the device copy.  viewport->trace.depth is the bounce count.  Page-locked host buffers (pinned
+ * or registered) are written by the kernels while the frame is traced; pageable ones receive a
+ * copy once it is done. */
 ST_API int st_render_scene(st_ctx *ctx, int slot, const Scene *scene, Viewport *viewport);
 /* st_render_scene with explicit outputs, stream, counters and timings. */
 ST_API int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *viewport,

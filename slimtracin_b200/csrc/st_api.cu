@@ -829,6 +829,17 @@ static int make_view(const Viewport *vp, ViewDev &v) {
     return ST_OK;
 }
 
+// The device address of a page-locked (pinned or registered) host buffer, or null for pageable
+// memory, which the device cannot write.
+static void *device_view_of_host(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+}
+
 static SceneDev scene_view(SceneSlot &S, const Scene *scene) {
     SceneDev d;
     d.prims = P<PrimDev>(S.prims);
@@ -907,17 +918,26 @@ int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *view
     ST_CUDA(cudaEventRecord(ctx->ev[0], st));
     launch_ssb(sd, v, P<int4>(ctx->ssb), st);
     launch_ray_rows(v, P<float>(ctx->dirs), st);
+    // Page-locked host outputs are written by the kernels themselves (the float grid as it is traced,
+    // the resolved frame by the resolve kernel), so no copy follows the trace; pageable ones are
+    // copied at the end.
+    FloatPixel *mapped_float = nullptr;
+    uint32_t *mapped_u8 = nullptr;
+    if (!o->device_outputs) {
+        if (host_float && !o->skip_float_copy) mapped_float = static_cast<FloatPixel *>(device_view_of_host(host_float));
+        if (host_u8 && dev_u8) mapped_u8 = static_cast<uint32_t *>(device_view_of_host(host_u8));
+    }
     ST_CUDA(cudaEventRecord(ctx->ev[1], st));
     launch_trace(sd, v, P<int4>(ctx->ssb), P<float>(ctx->dirs), dev_float, dev_ids, P<unsigned>(ctx->status),
-                 P<unsigned long long>(ctx->counters), o->count_work != 0, st);
+                 P<unsigned long long>(ctx->counters), o->count_work != 0, st, mapped_float);
     ST_CUDA(cudaGetLastError());
     ST_CUDA(cudaEventRecord(ctx->ev[2], st));
-    if (dev_u8) launch_resolve(dev_float, v.grid_w, W, H, dev_u8, st);
+    if (dev_u8) launch_resolve(dev_float, v.grid_w, W, H, mapped_u8 ? mapped_u8 : dev_u8, st);
     ST_CUDA(cudaEventRecord(ctx->ev[3], st));
     if (!o->device_outputs) {
-        if (host_float && !o->skip_float_copy)
+        if (host_float && !o->skip_float_copy && !mapped_float)
             ST_CUDA(cudaMemcpyAsync(host_float, dev_float, sizeof(FloatPixel) * grid, cudaMemcpyDeviceToHost, st));
-        if (host_u8 && dev_u8)
+        if (host_u8 && dev_u8 && !mapped_u8)
             ST_CUDA(cudaMemcpyAsync(host_u8, dev_u8, sizeof(uint32_t) * (size_t)W * H, cudaMemcpyDeviceToHost, st));
         if (o->out_prim_id)
             ST_CUDA(cudaMemcpyAsync(o->out_prim_id, dev_ids, sizeof(u32t) * grid, cudaMemcpyDeviceToHost, st));

@@ -45,8 +45,10 @@ int batch_blocks_per_sm(int tile_shape);
 // Row-segment starts of the view's ray directions: (grid_h x ceil(grid_w / kSegment)) float3.
 void launch_ray_rows(const ViewDev &v, float *dirs, cudaStream_t st);
 inline size_t ray_rows_floats(const ViewDev &v) { return (size_t)v.grid_h * ((v.grid_w + kSegment - 1) / kSegment) * 3; }
+// out_host (optional): a device-accessible page-locked host copy of `out`, written by the kernel too
 void launch_trace(const SceneDev &S, const ViewDev &v, const int4 *ssb, const float *dirs, FloatPixel *out,
-                  u32t *prim_ids, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st);
+                  u32t *prim_ids, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st,
+                  FloatPixel *out_host = nullptr);
 void launch_resolve(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out, cudaStream_t st);
 
 // ---- BVH builds (st_bvh.cu) ----

@@ -513,7 +513,8 @@ __device__ __forceinline__ v3 grid_direction(const ViewDev &v, const float *seg,
 // (black, 0, +inf).
 template <bool CNT>
 __device__ __forceinline__ void trace_point(TState<CNT> &t, const SceneDev &S, const ViewDev &v, const int4 *ssb,
-                                            const float *dirs, u32t x, u32t y, FloatPixel *out, u32t *prim_ids) {
+                                            const float *dirs, u32t x, u32t y, FloatPixel *out, u32t *prim_ids,
+                                            FloatPixel *out_host = nullptr) {
     const size_t idx = (size_t)y * v.grid_w + x;
     v3 current = grid_direction(v, dirs, x, y);
     RayD ray;
@@ -660,6 +661,12 @@ __device__ __forceinline__ void trace_point(TState<CNT> &t, const SceneDev &S, c
     o[0] = make_float2(c01.x, c01.y);
     o[1] = make_float2(c01.z, c01.w);
     reinterpret_cast<double *>(o)[2] = depth;
+    if (out_host) {        // the caller's page-locked host buffer, written over the bus as the frame is traced
+        float2 *h = reinterpret_cast<float2 *>(out_host + idx);
+        h[0] = make_float2(c01.x, c01.y);
+        h[1] = make_float2(c01.z, c01.w);
+        reinterpret_cast<double *>(h)[2] = depth;
+    }
 }
 
 template <bool CNT>
@@ -685,7 +692,7 @@ __device__ __forceinline__ void flush_counters(TState<CNT> &t, unsigned *status,
 template <bool CNT>
 __global__ void ST_TRACE_BOUNDS trace_kernel(SceneDev S, ViewDev v, const int4 *ssb, const float *dirs,
                                                     FloatPixel *out, u32t *prim_ids, unsigned *status,
-                                                    unsigned long long *counters) {
+                                                    unsigned long long *counters, FloatPixel *out_host) {
     const u32t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // a block covers 16x8 grid points; each warp an 8x4 tile
     const u32t x = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
@@ -693,7 +700,7 @@ __global__ void ST_TRACE_BOUNDS trace_kernel(SceneDev S, ViewDev v, const int4 *
     TState<CNT> t;
     t.status = 0;
     if (CNT) for (int k = 0; k < C_COUNT; k++) t.cnt[k] = 0;
-    if (x < v.grid_w && y < v.grid_h) trace_point(t, S, v, ssb, dirs, x, y, out, prim_ids);
+    if (x < v.grid_w && y < v.grid_h) trace_point(t, S, v, ssb, dirs, x, y, out, prim_ids, out_host);
     flush_counters(t, status, counters);
 }
 
@@ -761,10 +768,11 @@ void launch_ray_rows(const ViewDev &v, float *dirs, cudaStream_t st) {
     row_segments_kernel<<<(v.grid_h + 63) / 64, 64, 0, st>>>(v, dirs);
 }
 void launch_trace(const SceneDev &S, const ViewDev &v, const int4 *ssb, const float *dirs, FloatPixel *out,
-                  u32t *prim_ids, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st) {
+                  u32t *prim_ids, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st,
+                  FloatPixel *out_host) {
     dim3 grid((v.grid_w + 15) / 16, (v.grid_h + 7) / 8);
-    if (count) trace_kernel<true><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters);
-    else trace_kernel<false><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters);
+    if (count) trace_kernel<true><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, out_host);
+    else trace_kernel<false><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, out_host);
 }
 int launch_batch(const BatchView *views, u32t n_views, u32t total_tiles, int tile_shape, u32t chunk, u32t grid_blocks,
                  u32t *tile_counter, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st) {

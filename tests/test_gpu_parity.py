@@ -266,3 +266,22 @@ def test_batch_equals_per_frame_renders(renderer):
                 assert np.array_equal(a.float_pixels.view(np.uint8), b.float_pixels.view(np.uint8)), (tile, graph)
                 assert np.array_equal(a.pixels.view(np.uint8), b.pixels.view(np.uint8))
             assert opt.rays == sum(fr.rays for fr in frames)
+
+
+def test_pinned_host_outputs_written_by_the_kernels(renderer):
+    """Page-locked host buffers are written by the trace and resolve kernels directly (no copy after
+    the trace); the frame equals the one rendered into pageable buffers."""
+    import torch
+    c1, cam1 = H.small_config1(subdivisions=3, texture_size=64, blas="orc")
+    H.tlas_sah(c1)
+    renderer.upload(14, c1, tlas="host")
+    pageable = scenes.Frame(320, 180, cam1, depth=4)
+    renderer.render(14, c1, pageable)
+    pinned = scenes.Frame(320, 180, cam1, depth=4, with_pixels=False, with_float=False)
+    pf = torch.zeros(pinned.rays * 24, dtype=torch.uint8, pin_memory=True)
+    pu = torch.zeros(320 * 180 * 4, dtype=torch.uint8, pin_memory=True)
+    pinned.grid.float_pixels, pinned.grid.pixels = pf.data_ptr(), pu.data_ptr()
+    sc, keep = c1.to_ctypes()
+    assert api.lib().st_render_scene(renderer.ctx, 14, C.byref(sc), C.byref(pinned.viewport)) == 0
+    assert np.array_equal(pf.numpy(), pageable.float_pixels.view(np.uint8))
+    assert np.array_equal(pu.numpy(), pageable.pixels.view(np.uint8))
