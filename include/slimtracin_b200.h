@@ -198,6 +198,23 @@ ST_API int st_render_batch(st_ctx *ctx, const st_view *views, int view_count, st
 ST_API int st_build_lbvh_noalloc(st_ctx *ctx, const float *aabbs, uint32_t n, uint32_t max_leaf, uint32_t *codes,
                                  uint32_t *order, BVHNode *nodes, uint32_t info[2], void *stream);
 
+/* The object a click at pixel (x, y) of `viewport` selects, as manipulateSelection computes it
+ * (viewport/manipulation.h:55-123): the picking ray of setRayFromCoords (shaders/common.h:170),
+ * hitPrimitives over the resident primitives with the screen-space visibility cull at (x, y), then
+ * the glow sphere of every light.  viewport->projection_plane must be current (beginDrawing or
+ * setViewportProjectionPlane).  The host-side selection bookkeeping (pointers, offsets) stays with
+ * the caller. */
+typedef struct st_pick_result {
+    int found;                  /* 1 when a primitive or a light was hit */
+    int object_type;            /* PrimitiveType_* of the hit; PrimitiveType_Light for a light */
+    uint32_t object_id;         /* primitive index, or light index */
+    float position[3];          /* world-space hit position */
+    float distance;             /* along the picking ray */
+    float object_distance;      /* camera-space z of the hit (selection->object_distance) */
+} st_pick_result;
+ST_API int st_pick(st_ctx *ctx, int slot, const Scene *scene, const Viewport *viewport, int x, int y,
+                   st_pick_result *result);
+
 /* ---- serving: continuous batching of render requests ---------------------------------------------
  * A worker thread inside the library takes submitted requests in order, admits them while the
  * device-memory budget for in-flight frame/ray buffers allows, applies their transform updates,

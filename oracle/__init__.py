@@ -46,6 +46,8 @@ def reference():
     lib.ref_render_rows.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32]
     lib.ref_begin_drawing.argtypes = [C.c_void_p]
     lib.ref_update_scene_ssb.argtypes = [C.c_void_p, C.c_void_p]
+    lib.ref_pick.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+    lib.ref_pick.restype = C.c_int
     lib.ref_resolve.argtypes = [C.c_void_p]
     lib.ref_update_scene_bvh.argtypes = [C.c_void_p]
     lib.ref_update_mesh_bvh.argtypes = [C.c_void_p]
@@ -69,4 +71,6 @@ def restatement():
     lib.orc_primitive_aabbs.argtypes = [C.c_void_p, C.c_void_p]
     lib.orc_binned_sah.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.orc_binned_sah.restype = C.c_int
+    lib.orc_pick.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+    lib.orc_pick.restype = C.c_int
     return lib

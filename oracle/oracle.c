@@ -1780,3 +1780,49 @@ int orc_binned_sah(const float *aabbs, uint32_t n, uint32_t max_leaf, uint32_t *
     free(cent); free(ids); free(tmp); free(cur); free(next);
     return 0;
 }
+
+/* ---- picking: manipulateSelection viewport/manipulation.h:55-123 ------------------------------- */
+/* setRayFromCoords (shaders/common.h:170): start + right*x + down*y, normalised; then hitPrimitives
+ * over the TLAS leaf list with the visibility cull at (x, y) and every light's glow sphere
+ * (radius intensity/128, hitSphereSimple sphere.h:44).  Primitive screen bounds as the scene
+ * holds them (call orc_update_scene_ssb for the viewport first). */
+int orc_pick(const Scene *sc, const Viewport *vp, int x, int y, OrcPick *out) {
+    OTrace *tr = (OTrace*)calloc(1, sizeof(OTrace));
+    if (!tr) return -1;
+    if (sc->settings.meshes) tr->closest_mesh_hit.object_type = PrimitiveType_Mesh;
+    Ray ray;
+    memset(&ray, 0, sizeof(ray));
+    ray.origin = vp->camera->transform.position;
+    ray.direction = vsfma(vp->projection_plane.right, (f32)x, vp->projection_plane.start);
+    ray.direction = vsfma(vp->projection_plane.down, (f32)y, ray.direction);
+    ray.direction = vnorm(ray.direction);
+    ray.direction_reciprocal = vrcp(ray.direction);
+    RayHit *hit = &tr->closest_hit;
+    hit->distance = hit->distance_squared = INFINITY;
+    bool found = hit_primitives(tr, &ray, sc, sc->bvh.leaf_ids, sc->settings.primitives, false, true, (u16)x, (u16)y);
+    if (sc->lights) {
+        for (u32 i = 0; i < sc->settings.lights; i++) {
+            const Light *light = sc->lights + i;
+            f32 radius = light->intensity * (1.0f / (8.0f * 16.0f));
+            tr->sphere_hit.furthest = hit->distance / radius;
+            if (hit_sphere_simple(ray.origin, ray.direction, light->position_or_direction, 1.0f / radius, &tr->sphere_hit)) {
+                hit->distance = tr->sphere_hit.t_near * radius;
+                hit->position = vsfma(ray.direction, hit->distance, ray.origin);
+                hit->object_type = PrimitiveType_Light;
+                hit->object_id = i;
+                found = true;
+            }
+        }
+    }
+    memset(out, 0, sizeof(*out));
+    out->found = found;
+    if (found) {
+        out->object_type = hit->object_type;
+        out->object_id = hit->object_id;
+        out->position = hit->position;
+        out->distance = hit->distance;
+        out->object_distance = vmat3(vsub(hit->position, ray.origin), vp->camera->transform.rotation_matrix_inverted).z;
+    }
+    free(tr);
+    return 0;
+}

@@ -49,6 +49,17 @@ int orc_lbvh30(const float *aabbs, uint32_t n, uint32_t max_leaf, uint32_t *code
 int orc_binned_sah(const float *aabbs, uint32_t n, uint32_t max_leaf, uint32_t *order, BVHNode *nodes,
                    uint32_t *info);
 
+/* The object a click at pixel (x, y) selects (manipulateSelection, viewport/manipulation.h:55):
+ * found, PrimitiveType (PrimitiveType_Light for a light's glow sphere), index, world position,
+ * distance along the picking ray and camera-space z. */
+typedef struct OrcPick {
+    int found, object_type;
+    uint32_t object_id;
+    vec3 position;
+    float distance, object_distance;
+} OrcPick;
+int orc_pick(const Scene *scene, const Viewport *viewport, int x, int y, OrcPick *out);
+
 #ifdef __cplusplus
 }
 #endif

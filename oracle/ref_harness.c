@@ -298,3 +298,58 @@ void ref_free_texture(Texture *texture) {
 }
 
 void ref_free(void *p) { free(p); }
+
+/* The picking ray of manipulateSelection (viewport/manipulation.h:55-123), run with the reference's
+ * own functions: setViewportProjectionPlane, setRayFromCoords (shaders/common.h:170), hitPrimitives
+ * over scene->bvh.leaf_ids with the visibility cull at (x, y), then every light's glow sphere
+ * (hitSphereSimple, sphere.h:44).  Outputs the hit the selection would take: found, object type and
+ * id, world position, distance and the camera-space z the selection keeps (object_distance). */
+typedef struct { int found, object_type; u32 object_id; vec3 position; f32 distance, object_distance; } RefPick;
+int ref_pick(Scene *scene, Viewport *viewport, int x, int y, RefPick *out) {
+    Trace trace;
+    memset(&trace, 0, sizeof(trace));
+    trace.scene_stack = (u32*)calloc(scene->settings.primitives * 2 + 64, sizeof(u32));
+    trace.mesh_stack = (u32*)calloc(256, sizeof(u32));
+    trace.mesh_stack_size = 255;
+    trace.scene_stack_size = 255;
+    if (scene->settings.meshes) trace.closest_mesh_hit.object_type = PrimitiveType_Mesh;
+    setViewportProjectionPlane(viewport);
+    vec2i coords;
+    coords.x = x;
+    coords.y = y;
+    Ray ray;
+    setRayFromCoords(&ray, coords, viewport);
+    ray.direction_reciprocal = oneOverVec3(ray.direction);
+    RayHit *hit = &trace.closest_hit;
+    hit->distance = hit->distance_squared = MAX_DISTANCE;
+    bool found = hitPrimitives(&ray, &trace, scene, scene->bvh.leaf_ids, scene->settings.primitives, false, true,
+                               (u16)x, (u16)y);
+    Light *light = scene->lights;
+    if (light) {
+        for (u32 i = 0; i < scene->settings.lights; i++, light++) {
+            f32 light_radius = light->intensity * (1.0f / (8.0f * 16.0f));
+            trace.sphere_hit.furthest = hit->distance / light_radius;
+            if (hitSphereSimple(ray.origin, ray.direction, light->position_or_direction, 1.0f / light_radius,
+                                &trace.sphere_hit)) {
+                hit->distance = trace.sphere_hit.t_near * light_radius;
+                hit->position = scaleAddVec3(ray.direction, hit->distance, ray.origin);
+                hit->object_type = PrimitiveType_Light;
+                hit->object_id = i;
+                found = true;
+            }
+        }
+    }
+    memset(out, 0, sizeof(*out));
+    out->found = found;
+    if (found) {
+        out->object_type = hit->object_type;
+        out->object_id = hit->object_id;
+        out->position = hit->position;
+        out->distance = hit->distance;
+        out->object_distance = mulVec3Mat3(subVec3(hit->position, ray.origin),
+                                           viewport->camera->transform.rotation_matrix_inverted).z;
+    }
+    free(trace.scene_stack);
+    free(trace.mesh_stack);
+    return 0;
+}

@@ -62,6 +62,11 @@ class st_result(C.Structure):
 ST_ERR_NOT_READY, ST_ERR_TIMEOUT = 11, 7
 
 
+class st_pick_result(C.Structure):
+    _fields_ = [("found", C.c_int), ("object_type", C.c_int), ("object_id", C.c_uint32),
+                ("position", C.c_float * 3), ("distance", C.c_float), ("object_distance", C.c_float)]
+
+
 class STError(RuntimeError):
     def __init__(self, status, what, detail=""):
         self.status = status
@@ -103,6 +108,7 @@ def lib():
             "st_build_lbvh_noalloc": (i, [vp, vp, u32, u32, vp, vp, vp, vp, vp]),
             "st_render_ex": (i, [vp, i, vp, vp, C.POINTER(st_render_options)]),
             "st_render_batch": (i, [vp, vp, i, C.POINTER(st_batch_options)]),
+            "st_pick": (i, [vp, i, vp, vp, i, i, C.POINTER(st_pick_result)]),
             "st_serve_start": (i, [vp, C.POINTER(st_serve_config)]),
             "st_submit": (i, [vp, C.POINTER(st_request), C.POINTER(u64)]),
             "st_poll": (i, [vp, u64, C.POINTER(st_result)]),
@@ -203,6 +209,13 @@ class Renderer:
         self._check(self.L.st_build_bvh(self.ctx, mode, boxes.ctypes.data, n, max_leaf, codes.ctypes.data,
                                         order.ctypes.data, nodes.ctypes.data, info.ctypes.data), "st_build_bvh")
         return codes, order, nodes[:info[0]], int(info[0]), int(info[1])
+
+    def pick(self, slot, sd, frame, x, y):
+        """st_pick: what a click at pixel (x, y) of the frame's viewport selects."""
+        sc, keep = sd.to_ctypes()
+        res = st_pick_result()
+        self._check(self.L.st_pick(self.ctx, slot, C.byref(sc), C.byref(frame.viewport), x, y, C.byref(res)), "st_pick")
+        return res
 
     def free(self, slot):
         self._check(self.L.st_free_scene(self.ctx, slot), "st_free_scene")

@@ -1182,6 +1182,31 @@ int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *
     return ST_OK;
 }
 
+int st_pick(st_ctx *ctx, int slot, const Scene *scene, const Viewport *viewport, int x, int y, st_pick_result *result) {
+    static_assert(sizeof(PickDev) == sizeof(st_pick_result), "st_pick_result mirrors PickDev");
+    SceneSlot *S = slot_of(ctx, slot);
+    if (!S || !viewport || !result || x < 0 || y < 0) return ST_ERR_INVALID_ARG;
+    if (!S->allocated || !S->tlas_valid || !S->n_prims) return ST_ERR_NOT_RESIDENT;
+    for (const Primitive &p : S->prims_host)
+        if (p.type == PrimitiveType_Mesh && !S->meshes_valid) return ST_ERR_NOT_RESIDENT;
+    cudaSetDevice(ctx->device);
+    ViewDev v;
+    ST_TRY(make_view(viewport, v));
+    ST_TRY(reserve(ctx, ctx->ssb, sizeof(int4) * std::max(S->n_prims, 1u)));
+    ST_TRY(reserve(ctx, ctx->counters, sizeof(unsigned long long) * 16));
+    SceneDev sd = scene_view(*S, scene);
+    cudaStream_t st = ctx->stream;
+    launch_ssb(sd, v, P<int4>(ctx->ssb), st);
+    PickDev *d = reinterpret_cast<PickDev *>(ctx->counters.ptr);     // 128 bytes of scratch
+    launch_pick(sd, v, P<int4>(ctx->ssb), x, y, d, st);
+    ST_CUDA(cudaGetLastError());
+    PickDev h;
+    ST_CUDA(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, st));
+    ST_CUDA(cudaStreamSynchronize(st));
+    memcpy(result, &h, sizeof(h));
+    return ST_OK;
+}
+
 int st_render_scene(st_ctx *ctx, int slot, const Scene *scene, Viewport *viewport) {
     if (!viewport || !viewport->frame_buffer) return ST_ERR_INVALID_ARG;
     st_render_options o;

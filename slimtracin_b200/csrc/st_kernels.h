@@ -49,6 +49,14 @@ inline size_t ray_rows_floats(const ViewDev &v) { return (size_t)v.grid_h * ((v.
 void launch_trace(const SceneDev &S, const ViewDev &v, const int4 *ssb, const float *dirs, FloatPixel *out,
                   u32t *prim_ids, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st,
                   FloatPixel *out_host = nullptr);
+// The result of a pick (layout of st_pick_result)
+struct PickDev {
+    int found, object_type;
+    u32t object_id;
+    float position[3];
+    float distance, object_distance;
+};
+void launch_pick(const SceneDev &S, const ViewDev &v, const int4 *ssb, int x, int y, PickDev *out, cudaStream_t st);
 void launch_resolve(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out, cudaStream_t st);
 
 // ---- BVH builds (st_bvh.cu) ----

@@ -704,6 +704,50 @@ __global__ void ST_TRACE_BOUNDS trace_kernel(SceneDev S, ViewDev v, const int4 *
     flush_counters(t, status, counters);
 }
 
+// ---- picking: manipulateSelection viewport/manipulation.h:55-123 ---------------------------------
+// One thread: the ray of setRayFromCoords (shaders/common.h:170) through pixel (x, y), hitPrimitives
+// over the TLAS leaf list with the visibility cull at (x, y), then every light's glow sphere
+// (radius intensity/128, hitSphereSimple sphere.h:44); out: found, type, id, position, distance,
+// camera-space z.
+__global__ void pick_kernel(SceneDev S, ViewDev v, const int4 *ssb, int x, int y, PickDev *out) {
+    if (threadIdx.x || blockIdx.x) return;
+    TState<false> t;
+    t.status = 0;
+    t.closest.distance = t.closest.distance_squared = INFINITY;       // MAX_DISTANCE base.h:164
+    t.closest.cone_width = 0;
+    t.mesh_closest.object_type = PrimitiveType_Mesh;
+    t.current.cone_width = 0;
+    RayD ray;
+    ray.origin = v.cam_pos;
+    ray.direction = norm(vsfma(v.pp_down, (float)y, vsfma(v.pp_right, (float)x, v.pp_start)));
+    ray.rcp = rcp(ray.direction);
+    bool found = hit_primitives(t, S, ray, S.tlas_leaf_ids, 0, S.n_prims, false, ssb, (int)(uint16_t)x,
+                                (int)(uint16_t)y, 0.0f);
+    Hit &hit = t.closest;
+    for (u32t i = 0; S.lights && i < S.n_lights; i++) {
+        const Light &L = S.lights[i];
+        const float radius = L.intensity * (1.0f / (8.0f * 16.0f));
+        t.sphere.furthest = hit.distance / radius;
+        if (hit_sphere_simple(ray.origin, ray.direction, from(L.position_or_direction), 1.0f / radius, t.sphere)) {
+            hit.distance = t.sphere.t_near * radius;
+            hit.position = vsfma(ray.direction, hit.distance, ray.origin);
+            hit.object_type = PrimitiveType_Light;
+            hit.object_id = i;
+            found = true;
+        }
+    }
+    PickDev r;
+    r.found = found;
+    r.object_type = found ? hit.object_type : 0;
+    r.object_id = found ? hit.object_id : 0;
+    r.position[0] = found ? hit.position.x : 0;
+    r.position[1] = found ? hit.position.y : 0;
+    r.position[2] = found ? hit.position.z : 0;
+    r.distance = found ? hit.distance : 0;
+    r.object_distance = found ? vmat3(hit.position - ray.origin, v.cam_rot_matrix_inv).z : 0;
+    *out = r;
+}
+
 // ---- batched views: one persistent launch over the tiles of many views ------------------------
 // Every view is cut into tiles of tile_w x tile_h grid points (one warp per tile when the tile has
 // 32 points); warps take tiles from one global counter, `chunk` tiles at a time, so views of
@@ -804,6 +848,9 @@ void tile_dims(int tile_shape, u32t &tw, u32t &th) {
         case TILE_4x8: tw = 4; th = 8; return;
         default: tw = 8; th = 4; return;
     }
+}
+void launch_pick(const SceneDev &S, const ViewDev &v, const int4 *ssb, int x, int y, PickDev *out, cudaStream_t st) {
+    pick_kernel<<<1, 32, 0, st>>>(S, v, ssb, x, y, out);
 }
 void launch_resolve(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out, cudaStream_t st) {
     dim3 grid((width + 127) / 128, height);

@@ -114,3 +114,33 @@ def small_config1(subdivisions=3, texture_size=64, blas="orc"):
     if blas in ("orc", "ref"):
         blas_sah(sd.meshes[0], blas)
     return sd, cam
+
+
+def picks(sd, cam, w, h, coords, which="orc"):
+    """The selection a click at each (x, y) makes, by the oracle ("orc") or by the reference's own
+    picking sequence ("ref"), after the SSB update of the view.  Returns st_pick_result records."""
+    from slimtracin_b200 import api
+    lib = oracle.restatement() if which == "orc" else oracle.reference()
+    d = sd.copy()
+    sc, keep = d.to_ctypes()
+    fr = scenes.Frame(w, h, cam, with_pixels=False, with_float=False)
+    (lib.orc_update_scene_ssb if which == "orc" else lib.ref_update_scene_ssb)(C.byref(sc), C.byref(fr.viewport))
+    fn = lib.orc_pick if which == "orc" else lib.ref_pick
+    out = []
+    for x, y in coords:
+        r = api.st_pick_result()
+        fn(C.byref(sc), C.byref(fr.viewport), int(x), int(y), C.byref(r))
+        out.append(r)
+    return out
+
+
+def pick_key(r):
+    """Every field of a pick result as exact bits."""
+    import struct
+    return (r.found, r.object_type, r.object_id, struct.pack("5f", *r.position, r.distance, r.object_distance))
+
+
+def light_coords(sd, cam, w, h, step=2):
+    """Pixels whose picking ray hits a light's glow sphere (scanned with the oracle)."""
+    coords = [(x, y) for y in range(0, h, step) for x in range(0, w, step)]
+    return [c for c, r in zip(coords, picks(sd, cam, w, h, coords)) if r.found and r.object_type == 6]

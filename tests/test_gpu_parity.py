@@ -285,3 +285,24 @@ def test_pinned_host_outputs_written_by_the_kernels(renderer):
     assert api.lib().st_render_scene(renderer.ctx, 14, C.byref(sc), C.byref(pinned.viewport)) == 0
     assert np.array_equal(pf.numpy(), pageable.float_pixels.view(np.uint8))
     assert np.array_equal(pu.numpy(), pageable.pixels.view(np.uint8))
+
+
+@pytest.mark.parametrize("which", ["config0", "config1"])
+def test_pick_equals_oracle(renderer, which):
+    """st_pick (manipulateSelection's picking ray on the device) equals the oracle's pick bit for bit
+    on scattered pixels and on pixels whose ray hits a light's glow sphere."""
+    if which == "config0":
+        sd, cam = scenes.config0()
+    else:
+        sd, cam = H.small_config1(subdivisions=3, texture_size=64, blas="orc")
+    H.tlas_sah(sd)
+    renderer.upload(15, sd, tlas="host")
+    w, h = 160, 120
+    rng = np.random.default_rng(5)
+    coords = [tuple(c) for c in rng.integers(0, [w, h], (80, 2))]
+    coords += H.light_coords(sd, cam, w, h)[:10] if len(sd.lights) else []
+    fr = scenes.Frame(w, h, cam, with_pixels=False, with_float=False)
+    dev = [H.pick_key(renderer.pick(15, sd, fr, int(x), int(y))) for x, y in coords]
+    orc = [H.pick_key(r) for r in H.picks(sd, cam, w, h, coords)]
+    assert dev == orc
+    assert any(k[0] for k in dev)

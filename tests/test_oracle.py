@@ -216,3 +216,30 @@ def test_bvh_oracle_structure(n, max_leaf, builder):
     walk(0, 0)
     assert np.all(covered == 1)
     assert height == max(depth_max, 1)
+
+
+@pytest.mark.parametrize("which", ["config0", "area", "config1"])
+def test_pick_matches_reference(which):
+    """manipulateSelection's picking ray (viewport/manipulation.h:55-123): the oracle's pick equals
+    the reference's own hitPrimitives + glow-sphere sequence bit for bit, on scattered pixels and on
+    pixels that hit a light."""
+    if not oracle.reference_available():
+        pytest.skip("reference harness not built")
+    if which == "config0":
+        sd, cam = scenes.config0()
+    elif which == "area":
+        sd, cam = scenes.example_area_lights()
+    else:
+        sd, cam = H.small_config1(subdivisions=3, texture_size=64, blas="ref")
+    H.tlas_sah(sd, "ref")
+    w, h = 160, 120
+    rng = np.random.default_rng(11)
+    coords = [tuple(c) for c in rng.integers(0, [w, h], (60, 2))]
+    lights = H.light_coords(sd, cam, w, h) if len(sd.lights) else []
+    coords += lights[:10]
+    a = [H.pick_key(r) for r in H.picks(sd, cam, w, h, coords, "orc")]
+    b = [H.pick_key(r) for r in H.picks(sd, cam, w, h, coords, "ref")]
+    assert a == b
+    assert any(k[0] for k in a)
+    if which == "config0":
+        assert any(k[1] == 6 for k in a), "no pixel hit a light"
