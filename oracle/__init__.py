@@ -34,6 +34,21 @@ def _load(name, path):
     return _libs[name]
 
 
+def dropin():
+    """oracle/_ref/libdropin.so: a host built from the reference's headers whose GPU seams call
+    libslimtracin_b200 (dropin.c)."""
+    lib = _load("dropin", os.path.join(HERE, "_ref", "libdropin.so"))
+    lib.dropin_frame.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int]
+    lib.dropin_frame.restype = C.c_int
+    lib.dropin_shutdown.argtypes = []
+    lib.dropin_shutdown.restype = None
+    return lib
+
+
+def dropin_available():
+    return os.path.exists(os.path.join(HERE, "_ref", "libdropin.so"))
+
+
 def reference_available():
     return os.path.exists(os.path.join(HERE, "_ref", "libslimref.so"))
 
