@@ -18,6 +18,8 @@ roofline   the trace kernel: algorithmic bytes per frame (device event counters 
 cpu_baseline / --impl reference
            the reference's own renderer (oracle/_ref, compiled from the reference sources) on the
            same scene bytes, all host threads, over a bounded sample of rows
+config0    config 0: 16 implicit primitives, 3 point lights, 640x480, depth 2: the device frame beside
+           the reference's CPU renderer (all host threads, and one thread)
 dynamic    config 2: 4096 moving primitives, TLAS rebuilt (LBVH30, binned SAH) or refit every frame,
            1280x720 depth 2, 300 frames: build ms (API wall time) and trace ms (device events)
 batched    64 views (resolutions from 256x256 to 1920x1080, 1-6 bounces) over 8 resident scenes:
@@ -116,22 +118,22 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
-def reference_frame_setup(sd, cam):
+def reference_frame_setup(sd, cam, width=WIDTH, height=HEIGHT, depth=DEPTH):
     """The reference's per-frame set-up on a private copy of the scene: updateSceneSSB, beginDrawing."""
     import oracle
     ref = oracle.reference()
     d = sd.copy()
     sc, keep = d.to_ctypes()
-    fr = scenes.Frame(WIDTH, HEIGHT, cam, depth=DEPTH)
+    fr = scenes.Frame(width, height, cam, depth=depth)
     ref.ref_update_scene_ssb(C.byref(sc), C.byref(fr.viewport))
     ref.ref_begin_drawing(C.byref(fr.viewport))
     return ref, sc, fr, (d, keep)
 
 
-def cpu_reference_sample(sd, cam, threads, budget_s):
+def cpu_reference_sample(sd, cam, threads, budget_s, width=WIDTH, height=HEIGHT, depth=DEPTH):
     """The reference's renderer (oracle/_ref) on whole frames of the same scene bytes, repeated until
     about budget_s seconds have passed.  Returns (rays, seconds, frames)."""
-    ref, sc, fr, keep = reference_frame_setup(sd, cam)
+    ref, sc, fr, keep = reference_frame_setup(sd, cam, width, height, depth)
     rays, total, frames = 0, 0.0, 0
     while total < budget_s or frames == 0:
         t = time.perf_counter()
@@ -309,6 +311,41 @@ def dynamic_tlas(r, frames, cpu_reference):
     return out
 
 
+def config0_section(r, cpu_reference):
+    """Config 0 (16 implicit primitives, 3 point lights, 640x480, depth 2): the device frame (device
+    outputs, trace kernel by CUDA events) beside the reference's CPU renderer on the same scene."""
+    import torch
+    from slimtracin_b200 import api
+    sd, cam = scenes.config0()
+    slot = 13
+    r.upload(slot, sd, tlas=None)
+    r.build_tlas(slot, sd, api.ST_BVH_BINNED_SAH)
+    fr = scenes.Frame(640, 480, cam, depth=2, with_pixels=False, with_float=False)
+    dev_f = torch.empty(fr.rays * 24, dtype=torch.uint8, device="cuda")
+    dev_u = torch.empty(640 * 480 * 4, dtype=torch.uint8, device="cuda")
+    for _ in range(5):
+        r.render_device(slot, sd, fr, dev_f.data_ptr(), dev_u.data_ptr())
+    trace = [r.render_device(slot, sd, fr, dev_f.data_ptr(), dev_u.data_ptr()).trace_ms for _ in range(50)]
+    out = {"width": 640, "height": 480, "depth": 2, "rays_per_frame": fr.rays,
+           "gpu_trace_ms_p50": float(np.median(trace)), "gpu_mrays_s": fr.rays / float(np.median(trace)) / 1e3}
+    r.free(slot)
+    if cpu_reference:
+        try:
+            import oracle
+            if oracle.reference_available():
+                import tests.helpers as H
+                ref_sd = sd.copy()
+                H.tlas_sah(ref_sd, "ref")
+                threads = os.cpu_count() or 1
+                rays, dt, frames = cpu_reference_sample(ref_sd, cam, threads, 3.0, 640, 480, 2)
+                rays1, dt1, frames1 = cpu_reference_sample(ref_sd, cam, 1, 0.0, 640, 480, 2)
+                out.update({"cpu_mrays_s": rays / dt / 1e6, "cpu_threads": threads,
+                            "cpu_1thread_frame_ms": dt1 / frames1 * 1e3})
+        except Exception as ex:  # reported, never required
+            out["cpu_mrays_s"] = f"failed: {ex}"
+    return out
+
+
 def measure_l2_gbs():
     """Read bandwidth of a 48 MB float32 array that stays in the 126 MB L2 (torch.sum, CUDA events):
     the denominator of the trace kernel's L2 fraction."""
@@ -460,6 +497,7 @@ def main():
     dynamic = dynamic_tlas(r, args.dynamic_frames, rank == 0 and world == 1 and not args.no_cpu_baseline) \
         if args.dynamic_frames > 0 else None
     l2_gbs = measure_l2_gbs()
+    cfg0 = config0_section(r, rank == 0 and world == 1 and not args.no_cpu_baseline)
 
     # ---- roofline of the trace kernel -----------------------------------------------------------
     trace_avg_ms = sum(trace_ms) / len(trace_ms)
@@ -514,6 +552,7 @@ def main():
                          "l2_peak": l2_gbs, "l2_frac": achieved / l2_gbs,
                          "l2_peak_source": "48 MB L2-resident read (torch.sum), measured in this run"},
             "counters": counters,
+            "config0": cfg0,
             "dynamic_tlas": dynamic,
             "batched": mixed["batched"] if mixed else None,
             "served": mixed["served"] if mixed else None,
