@@ -95,6 +95,8 @@ struct ServeReq {
     int batch_size = 0;
     size_t dev_float = 0, dev_ssb = 0, dev_seg = 0, dev_u8 = 0;   // byte offsets in the batch's device arena
     size_t host_float = 0, host_u8 = 0;                           // byte offsets in the flight's pinned staging
+    uint32_t *mapped_u8 = nullptr;     // the device view of a page-locked out_u8 (written by the resolve kernel)
+    bool pinned_float = false;         // out_float is page-locked (one direct device-to-host copy)
 };
 
 struct InFlight {
@@ -1240,8 +1242,9 @@ void finish_flight(st_ctx *ctx, InFlight &F) {
     const double now = st_clock();
     for (auto &r : F.reqs) {
         const size_t grid = (size_t)r->view.grid_w * r->view.grid_h;
-        if (r->out_float) memcpy(r->out_float, F.pinned + r->host_float, sizeof(FloatPixel) * grid);
-        if (r->out_u8) memcpy(r->out_u8, F.pinned + r->host_u8, sizeof(uint32_t) * (size_t)(r->view.grid_w - 1) * (r->view.grid_h - 1));
+        if (r->out_float && !r->pinned_float) memcpy(r->out_float, F.pinned + r->host_float, sizeof(FloatPixel) * grid);
+        if (r->out_u8 && !r->mapped_u8)
+            memcpy(r->out_u8, F.pinned + r->host_u8, sizeof(uint32_t) * (size_t)(r->view.grid_w - 1) * (r->view.grid_h - 1));
     }
     std::lock_guard<std::mutex> lk(V.m);
     for (auto &r : F.reqs) {
@@ -1334,14 +1337,17 @@ int enqueue_flight(st_ctx *ctx, InFlight &F, BatchPlan &p, std::vector<std::shar
         const ServeReq &r = *reqs[i];
         const BatchView &b = p.table[i];
         const size_t grid = (size_t)b.view.grid_w * b.view.grid_h;
-        if (r.out_u8) {
+        if (r.out_u8 && r.mapped_u8) {            // page-locked: the resolve kernel writes the host frame
+            launch_resolve(b.out, b.view.grid_w, b.view.grid_w - 1, b.view.grid_h - 1, r.mapped_u8, st);
+        } else if (r.out_u8) {
             uint32_t *u8 = reinterpret_cast<uint32_t *>(arena + r.dev_u8);
             launch_resolve(b.out, b.view.grid_w, b.view.grid_w - 1, b.view.grid_h - 1, u8, st);
             ST_CUDA(cudaMemcpyAsync(F.pinned + r.host_u8, u8, (size_t)(b.view.grid_w - 1) * (b.view.grid_h - 1) * 4,
                                     cudaMemcpyDeviceToHost, st));
         }
         if (r.out_float)
-            ST_CUDA(cudaMemcpyAsync(F.pinned + r.host_float, b.out, sizeof(FloatPixel) * grid, cudaMemcpyDeviceToHost, st));
+            ST_CUDA(cudaMemcpyAsync(r.pinned_float ? reinterpret_cast<char *>(r.out_float) : F.pinned + r.host_float, b.out,
+                                    sizeof(FloatPixel) * grid, cudaMemcpyDeviceToHost, st));
     }
     ST_CUDA(cudaMemcpyAsync(F.pinned, F.status.ptr, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     ST_CUDA(cudaEventRecord(F.done_ev, st));
@@ -1422,8 +1428,11 @@ int launch_flight(st_ctx *ctx, int f, std::vector<std::shared_ptr<ServeReq>> &re
     // host staging: the status word, then each request's float grid and u8 frame
     for (auto &r : reqs) {
         const size_t grid = (size_t)r->view.grid_w * r->view.grid_h;
-        if (r->out_float) { r->host_float = host; host += align256(sizeof(FloatPixel) * grid); }
-        if (r->out_u8) { r->host_u8 = host; host += align256((size_t)(r->view.grid_w - 1) * (r->view.grid_h - 1) * 4); }
+        if (r->out_float && !r->pinned_float) { r->host_float = host; host += align256(sizeof(FloatPixel) * grid); }
+        if (r->out_u8 && !r->mapped_u8) {
+            r->host_u8 = host;
+            host += align256((size_t)(r->view.grid_w - 1) * (r->view.grid_h - 1) * 4);
+        }
     }
     if (F.pinned_cap < host) {                  // grows geometrically: cudaFreeHost waits for the device
         const size_t cap = std::max(host, 2 * F.pinned_cap);
@@ -1600,6 +1609,9 @@ int st_submit(st_ctx *ctx, const st_request *req, st_ticket *ticket) {
     }
     r->out_float = req->view.out_float;
     r->out_u8 = req->view.out_u8;
+    // page-locked outputs need no staging and no copy on the worker thread
+    if (r->out_u8) r->mapped_u8 = static_cast<uint32_t *>(device_view_of_host(r->out_u8));
+    if (r->out_float) r->pinned_float = device_view_of_host(r->out_float) != nullptr;
     if (req->moved_count) {
         if (!req->moved || !req->moved_ids) return ST_ERR_INVALID_ARG;
         for (uint32_t k = 0; k < req->moved_count; k++)

@@ -162,7 +162,10 @@ class Stream:
         self.residents, self.slots, self.rate = residents, slots, rate
         self.refit_fraction = refit_fraction
         self.arrivals = poisson_arrivals(rng, rate, count)
-        self.out = {r: np.zeros(r[0] * r[1], dtype=S.PIXEL_DT) for r in RESOLUTIONS}
+        # one page-locked frame per resolution, shared by the requests (the kernels write it directly)
+        import torch
+        self.pinned = {r: torch.zeros(r[0] * r[1] * 4, dtype=torch.uint8, pin_memory=True) for r in RESOLUTIONS}
+        self.out = {r: t.data_ptr() for r, t in self.pinned.items()}
         self.requests = []
         for k in range(count):
             si, w, h, d = random_view(rng, len(residents))
@@ -172,7 +175,7 @@ class Stream:
             req.view.slot = slots[si]
             req.view.scene = C.addressof(residents[si].sc)
             req.view.viewport = C.addressof(fr.viewport)
-            req.view.out_u8 = self.out[(w, h)].ctypes.data
+            req.view.out_u8 = self.out[(w, h)]
             if upd is not None:
                 req.moved, req.moved_ids, req.moved_count = upd.ctypes.data, ids.ctypes.data, len(ids)
             self.requests.append((si, w, h, fr, upd, ids, req))
@@ -228,7 +231,7 @@ class Stream:
                 if mode != api.ST_BVH_REFIT:
                     moved_since[si] = 0
                 renderer._check(L.st_update_scene_bvh(ctx, slot, None, mode), "st_update_scene_bvh")
-            opt.out_u8 = self.out[(w, h)].ctypes.data
+            opt.out_u8 = self.out[(w, h)]
             renderer._check(L.st_render_ex(ctx, slot, C.byref(self.residents[si].sc), C.byref(fr.viewport),
                                            C.byref(opt)), "st_render_ex")
             res.append((arrival, L.st_clock(), fr.rays, 0, w, h, 1))

@@ -111,3 +111,36 @@ def test_request_over_frame_budget_is_refused():
         assert res.status == 5   # ST_ERR_BUDGET: a 320x240 grid never fits in 4 KiB
     finally:
         r.close()
+
+
+def test_served_views_into_page_locked_buffers():
+    """Requests whose output frames are page-locked are resolved straight into them (no staging);
+    each equals the same view rendered alone."""
+    import torch
+    sd, cam = scenes.config0()
+    H.tlas_sah(sd)
+    r = api.Renderer(device=0)
+    try:
+        r.upload(0, sd, tlas="host")
+        sizes = [(64, 48), (96, 64), (33, 17), (128, 96)]
+        frames, bufs = [], []
+        for w, h in sizes:
+            fr = scenes.Frame(w, h, cam, depth=2, with_pixels=False)
+            buf = torch.zeros(w * h * 4, dtype=torch.uint8, pin_memory=True)
+            fr.grid.pixels = buf.data_ptr()
+            frames.append(fr)
+            bufs.append(buf)
+        srv = api.Server(r, max_in_flight=2, max_views_per_batch=4)
+        try:
+            tickets = [srv.submit(0, sd, fr) for fr in frames]
+            results = [srv.wait(t, timeout=60) for t in tickets]
+        finally:
+            srv.stop()
+        assert all(res.status == api.ST_OK for res in results)
+        for (w, h), fr, buf in zip(sizes, frames, bufs):
+            alone = scenes.Frame(w, h, cam, depth=2)
+            r.render(0, sd, alone)
+            assert np.array_equal(buf.numpy(), alone.pixels.view(np.uint8))
+            assert np.array_equal(fr.float_pixels.view(np.uint8), alone.float_pixels.view(np.uint8))
+    finally:
+        r.close()
