@@ -75,7 +75,21 @@ typedef struct st_render_options {
     uint64_t counters[16];      /* out: see enum st_counter */
     float trace_ms;             /* out: CUDA-event time of the trace kernel on the launch stream */
     float total_ms;             /* out: CUDA-event time of the whole render on the launch stream */
+    int overlays;               /* ST_OVERLAY_* bits: debug overlays drawn over the traced grid, before
+                                   the resolve */
 } st_render_options;
+
+/* The debug overlays of render/raytracer.h:46 (drawBVH: TLAS node boxes, leaf primitives' boxes,
+ * mesh instances' BLAS nodes of depth <= 5) and render/SSB.h:175 (drawSSB: each visible primitive's
+ * screen-space bounds), drawn on the device in the reference's order with its anti-aliased line
+ * rasteriser (shapes/line.h:46) and blending (setPixel, core/types.h:422), using
+ * viewport->projection_matrix (set by beginDrawing) and the clipping distances of
+ * viewport->settings.  drawBVH walks every TLAS node (the reference's u8 node counter never
+ * terminates at 256 nodes or more). */
+enum st_overlay {
+    ST_OVERLAY_BVH = 1,
+    ST_OVERLAY_SSB = 2
+};
 
 enum st_counter {
     ST_CNT_PRIMARY_RAYS = 0,
@@ -152,7 +166,9 @@ ST_API int st_build_bvh(st_ctx *ctx, int mode, const float *aabbs, uint32_t n, u
  * values the reference passes by value to its kernel (counts, ambient light); the arrays come from
  * the device copy.  viewport->trace.depth is the bounce count.  Page-locked host buffers (pinned
  * or registered) are written by the kernels while the frame is traced; pageable ones receive a
- * copy once it is done. */
+ * copy once it is done.  viewport->settings.show_BVH / show_SSB draw the drawBVH / drawSSB overlays
+ * into the frame before the resolve (a host that binds renderScene here drops its own drawBVH and
+ * drawSSB calls). */
 ST_API int st_render_scene(st_ctx *ctx, int slot, const Scene *scene, Viewport *viewport);
 /* st_render_scene with explicit outputs, stream, counters and timings. */
 ST_API int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *viewport,

@@ -71,6 +71,8 @@ def reference():
     lib.ref_load_texture.argtypes = [C.c_void_p, C.c_uint16, C.c_uint16, C.c_int, C.c_int, C.c_void_p, C.c_int]
     lib.ref_free_texture.argtypes = [C.c_void_p]
     lib.ref_free.argtypes = [C.c_void_p]
+    lib.ref_draw_overlays.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    lib.ref_draw_overlays.restype = C.c_int
     return lib
 
 
@@ -88,4 +90,6 @@ def restatement():
     lib.orc_binned_sah.restype = C.c_int
     lib.orc_pick.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
     lib.orc_pick.restype = C.c_int
+    lib.orc_draw_overlays.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    lib.orc_draw_overlays.restype = None
     return lib

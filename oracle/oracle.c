@@ -1826,3 +1826,324 @@ int orc_pick(const Scene *sc, const Viewport *vp, int x, int y, OrcPick *out) {
     free(tr);
     return 0;
 }
+
+/* ---- debug overlays: drawBVH (render/raytracer.h:46) and drawSSB (render/SSB.h:175) ----------- */
+/* The unit box initBox (core/init.h:279) leaves in viewport->default_box, corners in BoxCorners
+ * order (core/types.h:86), and the 12 edges of setBoxEdgesFromVertices (core/init.h:250) in
+ * BoxEdgeSides order (core/types.h:102): the order in which drawBox draws them. */
+static const f32 kBoxCorner[8][3] = {{-1, 1, 1}, {1, 1, 1}, {-1, -1, 1}, {1, -1, 1},
+                                     {-1, 1, -1}, {1, 1, -1}, {-1, -1, -1}, {1, -1, -1}};
+static const u8 kBoxEdge[12][2] = {{0, 1}, {2, 3}, {2, 0}, {3, 1}, {4, 5}, {6, 7},
+                                   {6, 4}, {7, 5}, {2, 6}, {0, 4}, {3, 7}, {1, 5}};
+
+/* A float -> i32 conversion as x86's truncating convert performs it: out-of-range values and NaN
+ * give INT32_MIN (the "integer indefinite" value), which is what the reference's (i32) casts
+ * produce on the machines it runs on. */
+static inline i32 trunc_i32(f32 v) { return (v >= -2147483648.0f && v < 2147483648.0f) ? (i32)v : INT32_MIN; }
+static inline f32 frac_of(f32 v) { return v - floorf(v); }              /* fractionOf line.h:39 */
+static inline f32 one_minus_frac_of(f32 v) { return 1 - frac_of(v); }  /* oneMinusFractionOf line.h:43 */
+static inline int in_range(i32 v, i32 end, i32 start) { return v >= start && v < end; }   /* base.h:381 */
+
+typedef struct {
+    FloatPixel *px;
+    u16 stride;
+    i32 x_left, y_top, w, h;   /* viewport position and frame extent + position */
+} OCanvas;
+
+static inline void plot(const OCanvas *c, i32 x, i32 y, f64 z, vec3 color, f32 opacity) {
+    set_pixel(c->px + (c->stride * y) + x, color, opacity, z);   /* setPixelByCoords types.h:453 */
+}
+
+/* drawLine shapes/line.h:46 (an anti-aliased line of 1 + line_width + 1 pixels across) */
+static void draw_line(const OCanvas *c, f32 x1, f32 y1, f64 z1, f32 x2, f32 y2, f64 z2, vec3 color, f32 opacity,
+                      u8 line_width) {
+    if (x1 < 0 && y1 < 0 && x2 < 0 && y2 < 0) return;
+    const i32 x_left = c->x_left, y_top = c->y_top, w = c->w, h = c->h;
+    x1 += (f32)x_left; x2 += (f32)x_left;
+    y1 += (f32)y_top;  y2 += (f32)y_top;
+    color = vmul(color, color);
+    f64 tmp, z_range, range_remap, z = 0, z_curr = 0, z_step = 0;
+    f32 dx = x2 - x1, dy = y2 - y1, gap, grad, first_offset, last_offset;
+    vec3 first, last;
+    i32 x, y, sx, sy, ex, ey;
+    const int has_depth = z1 || z2;
+    if (fabsf(dx) > fabsf(dy)) {   /* shallow: one column per x */
+        if (x2 < x1) { tmp = x2; x2 = x1; x1 = (f32)tmp; tmp = y2; y2 = y1; y1 = (f32)tmp; tmp = z2; z2 = z1; z1 = tmp; }
+        grad = dy / dx;
+        first.x = roundf(x1); last.x = roundf(x2);
+        first_offset = first.x - x1; last_offset = last.x - x2;
+        first.y = y1 + grad * first_offset; last.y = y2 + grad * last_offset;
+        sx = trunc_i32(first.x); sy = trunc_i32(first.y); ex = trunc_i32(last.x); ey = trunc_i32(last.y);
+        x = sx; y = sy;
+        gap = one_minus_frac_of(x1 + 0.5f);
+        if (in_range(x, w, x_left)) {
+            if (in_range(y, h, y_top)) plot(c, x, y, z1, color, one_minus_frac_of(first.y) * gap * opacity);
+            for (u8 i = 0; i < line_width; i++) { y++; if (in_range(y, h, y_top)) plot(c, x, y, z1, color, opacity); }
+            y++;
+            if (in_range(y, h, y_top)) plot(c, x, y, z1, color, frac_of(first.y) * gap * opacity);
+        }
+        x = ex; y = ey;
+        gap = frac_of(x2 + 0.5f);
+        if (in_range(x, w, x_left)) {
+            if (in_range(y, h, y_top)) plot(c, x, y, z2, color, one_minus_frac_of(last.y) * gap * opacity);
+            for (u8 i = 0; i < line_width; i++) { y++; if (in_range(y, h, y_top)) plot(c, x, y, z2, color, opacity); }
+            y++;
+            if (in_range(y, h, y_top)) plot(c, x, y, z2, color, frac_of(last.y) * gap * opacity);
+        }
+        if (has_depth) {   /* 1/z interpolated across the interior columns */
+            z1 = 1.0 / z1; z2 = 1.0 / z2;
+            z_range = z2 - z1;
+            range_remap = z_range / (f64)(x2 - x1);
+            z1 += range_remap * (f64)(first_offset + 1);
+            z2 += range_remap * (f64)(last_offset - 1);
+            z_range = z2 - z1;
+            z_step = z_range / (f64)(last.x - first.x - 1);
+            z_curr = z1;
+        } else z = 0;
+        gap = first.y + grad;
+        for (x = sx + 1; x < ex; x++) {
+            if (in_range(x, w, x_left)) {
+                if (has_depth) z = 1.0 / z_curr;
+                y = trunc_i32(gap);
+                if (in_range(y, h, y_top)) plot(c, x, y, z, color, one_minus_frac_of(gap) * opacity);
+                for (u8 i = 0; i < line_width; i++) { y++; if (in_range(y, h, y_top)) plot(c, x, y, z, color, opacity); }
+                y++;
+                if (in_range(y, h, y_top)) plot(c, x, y, z, color, frac_of(gap) * opacity);
+            }
+            gap += grad;
+            if (has_depth) z_curr += z_step;
+        }
+    } else {   /* steep: one row per y */
+        if (y2 < y1) { tmp = x2; x2 = x1; x1 = (f32)tmp; tmp = y2; y2 = y1; y1 = (f32)tmp; tmp = z2; z2 = z1; z1 = tmp; }
+        grad = dx / dy;
+        first.y = roundf(y1); last.y = roundf(y2);
+        first_offset = y1 - first.y; last_offset = last.y - y2;
+        first.x = x1 + grad * first_offset; last.x = x2 + grad * last_offset;
+        sy = trunc_i32(first.y); sx = trunc_i32(first.x); ey = trunc_i32(last.y); ex = trunc_i32(last.x);
+        x = sx; y = sy;
+        gap = one_minus_frac_of(y1 + 0.5f);
+        if (in_range(y, h, y_top)) {
+            if (in_range(x, w, x_left)) plot(c, x, y, z1, color, one_minus_frac_of(first.x) * gap * opacity);
+            for (u8 i = 0; i < line_width; i++) { x++; if (in_range(x, w, x_left)) plot(c, x, y, z1, color, opacity); }
+            x++;
+            if (in_range(x, w, x_left)) plot(c, x, y, z1, color, frac_of(first.x) * gap * opacity);
+        }
+        x = ex; y = ey;
+        gap = frac_of(y2 + 0.5f);
+        if (in_range(y, h, y_top)) {
+            if (in_range(x, w, x_left)) plot(c, x, y, z2, color, one_minus_frac_of(last.x) * gap * opacity);
+            for (u8 i = 0; i < line_width; i++) { x++; if (in_range(x, w, x_left)) plot(c, x, y, z2, color, opacity); }
+            x++;
+            if (in_range(x, w, x_left)) plot(c, x, y, z2, color, frac_of(last.x) * gap * opacity);
+        }
+        if (has_depth) {
+            z1 = 1.0 / z1; z2 = 1.0 / z2;
+            z_range = z2 - z1;
+            range_remap = z_range / (f64)(y2 - y1);
+            z1 += range_remap * (f64)(first_offset + 1);
+            z2 += range_remap * (f64)(last_offset - 1);
+            z_range = z2 - z1;
+            z_step = z_range / (f64)(last.y - first.y - 1);
+            z_curr = z1;
+        } else z = 0;
+        gap = first.x + grad;
+        for (y = sy + 1; y < ey; y++) {
+            if (in_range(y, h, y_top)) {
+                if (has_depth) z = 1.0 / z_curr;
+                x = trunc_i32(gap);
+                if (in_range(x, w, x_left)) plot(c, x, y, z, color, one_minus_frac_of(gap) * opacity);
+                for (u8 i = 0; i < line_width; i++) { x++; if (in_range(x, w, x_left)) plot(c, x, y, z, color, opacity); }
+                x++;
+                if (in_range(x, w, x_left)) plot(c, x, y, z, color, frac_of(gap) * opacity);
+            }
+            gap += grad;
+            if (has_depth) z_curr += z_step;
+        }
+    }
+}
+
+/* lerpVec3 vec3.h:265 */
+static inline vec3 vlerp(vec3 from, vec3 to, f32 by) { return vsfma(vsub(to, from), by, from); }
+
+/* cullAndClipEdge shapes/edge.h:8: near, far, then the left/right/bottom/top frustum planes */
+static int clip_edge(vec3 *pa, vec3 *pb, const Viewport *vp) {
+    vec3 A = *pa, B = *pb, N;
+    f32 d = vp->settings.near_clipping_plane_distance, na, nb;
+    u8 out = (A.z < d) | ((B.z < d) << 1);
+    if (out) {
+        if (out == 3) return 0;
+        if (out & 1) A = vlerp(A, B, (d - A.z) / (B.z - A.z));
+        else         B = vlerp(B, A, (d - B.z) / (A.z - B.z));
+    }
+    d = vp->settings.far_clipping_plane_distance;
+    out = (A.z > d) | ((B.z > d) << 1);
+    if (out) {
+        if (out == 3) return 0;
+        if (out & 1) A = vlerp(A, B, (A.z - d) / (A.z - B.z));
+        else         B = vlerp(B, A, (B.z - d) / (B.z - A.z));
+    }
+    for (int plane = 0; plane < 4; plane++) {
+        if (plane == 0) N = V3(vp->camera->focal_length, 0, vp->frame_buffer->dimensions.width_over_height);
+        else if (plane == 1) N.x = -N.x;
+        else if (plane == 2) N = V3(0, vp->camera->focal_length, 1);
+        else N.y = -N.y;
+        na = vdot(N, A);
+        nb = vdot(N, B);
+        out = (na < 0) | ((nb < 0) << 1);
+        if (out) {
+            if (out == 3) return 0;
+            if (out & 1) A = vlerp(A, B, na / (na - nb));
+            else         B = vlerp(B, A, nb / (nb - na));
+        }
+    }
+    *pa = A;
+    *pb = B;
+    return 1;
+}
+
+/* mulVec4Mat4 vec4.h:96 with w = 1, then the perspective divide */
+static inline vec3 project_point(vec3 p, const mat4 *m) {
+    vec4 o;
+    o.x = p.x * m->X.x + p.y * m->Y.x + p.z * m->Z.x + 1.0f * m->W.x;
+    o.y = p.x * m->X.y + p.y * m->Y.y + p.z * m->Z.y + 1.0f * m->W.y;
+    o.z = p.x * m->X.z + p.y * m->Y.z + p.z * m->Z.z + 1.0f * m->W.z;
+    o.w = p.x * m->X.w + p.y * m->Y.w + p.z * m->Z.w + 1.0f * m->W.w;
+    return vscale(V3(o.x, o.y, o.z), 1.0f / o.w);
+}
+
+/* drawEdge shapes/edge.h:112 = projectEdge (:83) + drawLine */
+static void draw_edge(const OCanvas *c, const Viewport *vp, vec3 A, vec3 B, vec3 color, f32 opacity, u8 line_width) {
+    if (!clip_edge(&A, &B, vp)) return;
+    const f32 az = A.z, bz = B.z;
+    const Dimensions *dim = &vp->frame_buffer->dimensions;
+    vec3 a = project_point(A, &vp->projection_matrix), b = project_point(B, &vp->projection_matrix);
+    a.x += 1; a.x *= dim->h_width;
+    b.x += 1; b.x *= dim->h_width;
+    a.y += 1; a.y *= dim->h_height;
+    b.y += 1; b.y *= dim->h_height;
+    a.y = dim->f_height - a.y;
+    b.y = dim->f_height - b.y;
+    draw_line(c, a.x, a.y, az, b.x, b.y, bz, color, opacity, line_width);
+}
+
+/* drawBox scene/box.h:20 with BOX__ALL_SIDES: corners to world (convertPositionToWorldSpace) and to
+ * view space (camera position, inverted camera rotation), then the 12 edges */
+static void draw_box(const OCanvas *c, const Viewport *vp, const Primitive *p, vec3 color, f32 opacity, u8 line_width) {
+    vec3 v[8];
+    const xform3 *xf = &vp->camera->transform;
+    for (int i = 0; i < 8; i++) {
+        vec3 q = pos_to_world(V3(kBoxCorner[i][0], kBoxCorner[i][1], kBoxCorner[i][2]), p);
+        v[i] = qrot(vsub(q, xf->position), xf->rotation_inverted);
+    }
+    for (int e = 0; e < 12; e++) draw_edge(c, vp, v[kBoxEdge[e][0]], v[kBoxEdge[e][1]], color, opacity, line_width);
+}
+
+/* setBoxPrimitiveFromAABB raytracer.h:18 */
+static void box_from_aabb(Primitive *box, const AABB *a) {
+    box->rotation.axis = splat(0);
+    box->rotation.amount = 1;
+    box->position = vscale(vadd(a->min, a->max), 0.5f);
+    box->scale = vscale(vsub(a->max, a->min), 0.5f);
+    box->flags = IS_TRANSLATED | IS_SCALED | IS_SCALED_NON_UNIFORMLY;
+}
+
+/* The reference's Color() (core/base.h:577) values of the colours the overlays use */
+static vec3 overlay_color(int id) {
+    const f32 M = 255.0f;
+    switch (id) {
+        case 1: return V3(M, M, M);                     /* White */
+        case 2: return V3(M / 2.0f, M / 2.0f, M / 2.0f); /* Grey */
+        case 3: return V3(M, 0, 0);                     /* Red */
+        case 4: return V3(0, M, 0);                     /* Green */
+        case 5: return V3(0, 0, M);                     /* Blue */
+        case 6: return V3(0, M, M);                     /* Cyan */
+        case 7: return V3(M, 0, M);                     /* Magenta */
+        case 8: return V3(M, M, 0);                     /* Yellow */
+        default: return splat(0);
+    }
+}
+
+void orc_draw_overlays(const Scene *sc, const Viewport *vp, int what) {
+    const Dimensions *dim = &vp->frame_buffer->dimensions;
+    OCanvas c;
+    c.px = vp->frame_buffer->float_pixels;
+    c.stride = dim->width;
+    c.x_left = vp->position.x;
+    c.y_top = vp->position.y;
+    c.w = dim->width + c.x_left;
+    c.h = dim->height + c.y_top;
+    if (what & ORC_OVERLAY_BVH) {   /* drawBVH raytracer.h:46 */
+        Primitive box;
+        memset(&box, 0, sizeof(box));
+        for (u32 node_id = 0; node_id < sc->bvh.node_count; node_id++) {
+            const BVHNode *node = sc->bvh.nodes + node_id;
+            int color;
+            if (node->child_count) {
+                for (u32 i = 0; i < node->child_count; i++) {
+                    const Primitive *p = sc->primitives + sc->bvh.leaf_ids[node->first_child_id + i];
+                    switch (p->type) {
+                        case PrimitiveType_Box: color = 6; break;
+                        case PrimitiveType_Quad: color = 1; break;
+                        case PrimitiveType_Sphere: color = 8; break;
+                        case PrimitiveType_Tetrahedron: color = 7; break;
+                        case PrimitiveType_Mesh: {   /* drawMeshAccelerationStructure raytracer.h:33 */
+                            const BVH *bvh = &sc->meshes[p->id].bvh;
+                            for (u32 m = 0; m < bvh->node_count; m++) {
+                                const BVHNode *mn = bvh->nodes + m;
+                                if (mn->depth > 5) continue;
+                                box_from_aabb(&box, &mn->aabb);   /* setBoxPrimitiveFromPrimitiveAndAABB :25 */
+                                box.scale = vmul(box.scale, p->scale);
+                                box.rotation = p->rotation;
+                                box.flags |= IS_ROTATED;
+                                box.position = pos_to_world(box.position, p);
+                                draw_box(&c, vp, &box, overlay_color(mn->child_count ? 7 : (m ? 4 : 5)), 0.125f, 0);
+                            }
+                        } continue;
+                        default: continue;
+                    }
+                    draw_box(&c, vp, p, overlay_color(color), 1, 1);
+                }
+                color = 1;
+            } else color = node_id ? 2 : 5;
+            box_from_aabb(&box, &node->aabb);
+            draw_box(&c, vp, &box, overlay_color(color), 1, 1);
+        }
+    }
+    if (what & ORC_OVERLAY_SSB) {   /* drawSSB SSB.h:175 with drawHLine/drawVLine line.h:5,22 */
+        for (u32 i = 0; i < sc->settings.primitives; i++) {
+            const Primitive *p = sc->primitives + i;
+            if (!(p->flags & IS_VISIBLE)) continue;
+            int color;
+            switch (p->type) {
+                case PrimitiveType_Box: color = 6; break;
+                case PrimitiveType_Quad: color = 1; break;
+                case PrimitiveType_Sphere: color = 8; break;
+                case PrimitiveType_Tetrahedron: color = 7; break;
+                case PrimitiveType_Mesh: color = 3; break;
+                default: continue;
+            }
+            vec3 col = overlay_color(color);
+            col = vmul(col, col);
+            const vec2i mn = p->screen_bounds.min, mx = p->screen_bounds.max;
+            /* two horizontal lines (rows min.y, max.y), then two vertical ones (columns min.x, max.x) */
+            for (int k = 0; k < 4; k++) {
+                const int horizontal = k < 2;
+                i32 from = horizontal ? mn.x : mn.y, to = horizontal ? mx.x : mx.y;
+                i32 at = k == 0 ? mn.y : k == 1 ? mx.y : k == 2 ? mn.x : mx.x;
+                const i32 along0 = horizontal ? c.x_left : c.y_top, across0 = horizontal ? c.y_top : c.x_left;
+                const i32 along_end = (horizontal ? dim->width : dim->height) + along0;
+                const i32 across_end = (horizontal ? dim->height : dim->width) + across0;
+                from += along0; to += along0; at += across0;
+                if (!in_range(at, across_end, across0)) continue;
+                i32 first = from, last = to;   /* subRange base.h:373 */
+                if (to < from) { first = to; last = from; }
+                first = first > along0 ? first : along0;
+                last = (last < along_end ? last : along_end) - 1;
+                for (i32 s = first; s <= last; s++) {
+                    if (horizontal) plot(&c, s, at, 0, col, 1);
+                    else plot(&c, at, s, 0, col, 1);
+                }
+            }
+        }
+    }
+}

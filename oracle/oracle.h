@@ -60,6 +60,14 @@ typedef struct OrcPick {
 } OrcPick;
 int orc_pick(const Scene *scene, const Viewport *viewport, int x, int y, OrcPick *out);
 
+/* The debug overlays drawBVH (render/raytracer.h:46) and drawSSB (render/SSB.h:175), drawn into
+ * viewport->frame_buffer->float_pixels with viewport->projection_matrix (set by beginDrawing) and
+ * the unit box of initBox.  drawSSB reads the primitives' screen_bounds and IS_VISIBLE (call
+ * orc_update_scene_ssb first).  drawBVH walks all scene->bvh.node_count nodes (the reference's u8
+ * node counter only terminates below 256 nodes). */
+enum { ORC_OVERLAY_BVH = 1, ORC_OVERLAY_SSB = 2 };
+void orc_draw_overlays(const Scene *scene, const Viewport *viewport, int what);
+
 #ifdef __cplusplus
 }
 #endif

@@ -353,3 +353,15 @@ int ref_pick(Scene *scene, Viewport *viewport, int x, int y, RefPick *out) {
     free(trace.mesh_stack);
     return 0;
 }
+
+/* The debug overlays with the reference's own drawBVH (render/raytracer.h:46) and drawSSB
+ * (render/SSB.h:175), after initBox on the viewport's default box as initViewport does
+ * (core/init.h:443).  what: 1 = BVH, 2 = SSB.  drawBVH counts nodes with a u8, so a BVH of 256 or
+ * more nodes would never finish: refused with -1. */
+int ref_draw_overlays(Scene *scene, Viewport *viewport, int what) {
+    if ((what & 1) && scene->bvh.node_count > 255) return -1;
+    initBox(&viewport->default_box);
+    if (what & 1) drawBVH(scene, viewport);
+    if (what & 2) drawSSB(scene, viewport);
+    return 0;
+}

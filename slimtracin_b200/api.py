@@ -30,7 +30,10 @@ class st_render_options(C.Structure):
     _fields_ = [("stream", C.c_void_p), ("device_outputs", C.c_int), ("out_float", C.c_void_p),
                 ("out_u8", C.c_void_p), ("out_prim_id", C.c_void_p), ("skip_float_copy", C.c_int),
                 ("count_work", C.c_int), ("counters", C.c_uint64 * 16), ("trace_ms", C.c_float),
-                ("total_ms", C.c_float)]
+                ("total_ms", C.c_float), ("overlays", C.c_int)]
+
+
+OVERLAY_BVH, OVERLAY_SSB = 1, 2     # enum st_overlay
 
 
 class st_view(C.Structure):
@@ -222,15 +225,16 @@ class Renderer:
         self._keep.pop(slot, None)
 
     # -- render --------------------------------------------------------------------------------------
-    def render(self, slot, sd, frame, prim_ids=None, count_work=False, skip_float_copy=False):
+    def render(self, slot, sd, frame, prim_ids=None, count_work=False, skip_float_copy=False, overlays=0):
         """st_render_ex into the frame's host buffers; returns the options struct (timings,
-        counters)."""
+        counters).  overlays: OVERLAY_BVH | OVERLAY_SSB draws drawBVH / drawSSB over the frame."""
         sc, keep = sd.to_ctypes()
         opt = st_render_options()
         if prim_ids is not None:
             opt.out_prim_id = prim_ids.ctypes.data
         opt.count_work = int(count_work)
         opt.skip_float_copy = int(skip_float_copy)
+        opt.overlays = int(overlays)
         self._check(self.L.st_render_ex(self.ctx, slot, C.byref(sc), C.byref(frame.viewport), C.byref(opt)),
                     "st_render_ex")
         return opt

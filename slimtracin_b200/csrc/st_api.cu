@@ -48,6 +48,8 @@ struct SceneSlot {
     BVHNode tlas_root{};
     DevBuf meshes, mesh_pairs, tri_hot, tri_full;
     std::vector<MeshDev> mesh_host;
+    DevBuf outlines, outline_ranges;       // BLAS nodes drawBVH outlines (depth <= 5), per mesh ranges
+    std::vector<uint2> outline_host;       // per mesh: (first outline, count)
     bool meshes_valid = false;
     DevBuf textures, mips, quads;
     DevBuf emissive, occluders;
@@ -148,6 +150,7 @@ struct st_ctx {
     DevBuf ssb, dirs, out_float, out_u8, prim_ids, status, counters;
     DevBuf upd_host_dev;                 // st_update_primitives: records and ids on the device
     DevBuf sah_scratch;                  // binned-SAH builds (kept between builds)
+    DevBuf overlay_scratch, overlay_frags;   // debug overlays: boxes/edges, and the plotted pixels
     char *upd_pinned = nullptr;          // ... and their pinned staging
     size_t upd_pinned_cap = 0;
     LbvhScratch lbvh;
@@ -365,7 +368,7 @@ void st_shutdown(st_ctx *ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (int i = 0; i < (int)ctx->slots.size(); i++) st_free_scene(ctx, i);
     for (DevBuf *b : {&ctx->ssb, &ctx->dirs, &ctx->out_float, &ctx->out_u8, &ctx->prim_ids, &ctx->status, &ctx->counters,
-                      &ctx->upd_host_dev, &ctx->sah_scratch})
+                      &ctx->upd_host_dev, &ctx->sah_scratch, &ctx->overlay_scratch, &ctx->overlay_frags})
         release(ctx, *b);
     if (ctx->upd_pinned) cudaFreeHost(ctx->upd_pinned);
     lbvh_release(ctx->lbvh);
@@ -389,7 +392,8 @@ int st_free_scene(st_ctx *ctx, int slot) {
     if (!S) return ST_ERR_INVALID_ARG;
     for (DevBuf *b : {&S->prims_raw, &S->prims, &S->materials, &S->lights, &S->tlas_nodes, &S->tlas_leaf_ids,
                       &S->tlas_pairs, &S->tlas_aabbs, &S->tlas_scratch, &S->meshes, &S->mesh_pairs, &S->tri_hot,
-                      &S->tri_full, &S->textures, &S->mips, &S->quads, &S->emissive, &S->occluders})
+                      &S->tri_full, &S->textures, &S->mips, &S->quads, &S->emissive, &S->occluders, &S->outlines,
+                      &S->outline_ranges})
         release(ctx, *b);
     for (MotionBufs &m : S->spare)
         for (int k = 0; k < 7; k++) {
@@ -563,6 +567,8 @@ int st_upload_mesh_bvhs(st_ctx *ctx, int slot, const Scene *scene) {
     cudaSetDevice(ctx->device);
     ST_TRY(ensure(ctx, *S, scene));
     S->mesh_host.clear();
+    S->outline_host.clear();
+    std::vector<OutlineBox> outlines;
     u32t tri_off = 0, pair_off = 0;
     for (u32t m = 0; m < scene->settings.meshes; m++) {
         const Mesh &M = scene->meshes[m];
@@ -592,9 +598,30 @@ int st_upload_mesh_bvhs(st_ctx *ctx, int slot, const Scene *scene) {
             launch_make_pairs(tmp, M.bvh.node_count, P<NodePair>(S->mesh_pairs) + pair_off, ctx->stream);
             ST_CUDA(cudaFreeAsync(tmp, ctx->stream));
         }
+        // the nodes drawMeshAccelerationStructure (raytracer.h:33) outlines: depth <= 5, coloured
+        // Magenta (leaf), Green (inner) or Blue (root)
+        const u32t first_outline = (u32t)outlines.size();
+        for (u32t k = 0; k < M.bvh.node_count; k++) {
+            const BVHNode &nd = M.bvh.nodes[k];
+            if (nd.depth > 5) continue;
+            OutlineBox o;
+            memcpy(o.aabb, &nd.aabb, sizeof(o.aabb));
+            o.color = nd.child_count ? 7u : (k ? 4u : 5u);
+            o.pad = 0;
+            outlines.push_back(o);
+        }
+        S->outline_host.push_back(make_uint2(first_outline, (u32t)outlines.size() - first_outline));
         tri_off += M.triangle_count;
         pair_off += M.bvh.node_count > 1 ? (M.bvh.node_count - 1) / 2 : 0;
     }
+    ST_TRY(reserve(ctx, S->outlines, sizeof(OutlineBox) * std::max<size_t>(outlines.size(), 1)));
+    ST_TRY(reserve(ctx, S->outline_ranges, sizeof(uint2) * std::max<size_t>(S->outline_host.size(), 1)));
+    if (!outlines.empty())
+        ST_CUDA(cudaMemcpyAsync(S->outlines.ptr, outlines.data(), sizeof(OutlineBox) * outlines.size(),
+                                cudaMemcpyHostToDevice, ctx->stream));
+    if (!S->outline_host.empty())
+        ST_CUDA(cudaMemcpyAsync(S->outline_ranges.ptr, S->outline_host.data(), sizeof(uint2) * S->outline_host.size(),
+                                cudaMemcpyHostToDevice, ctx->stream));
     S->n_meshes = (u32t)S->mesh_host.size();
     if (S->n_meshes)
         ST_CUDA(cudaMemcpyAsync(S->meshes.ptr, S->mesh_host.data(), sizeof(MeshDev) * S->n_meshes, cudaMemcpyHostToDevice, ctx->stream));
@@ -871,6 +898,61 @@ static SceneDev scene_view(SceneSlot &S, const Scene *scene) {
     return d;
 }
 
+// drawBVH (raytracer.h:46) and drawSSB (SSB.h:175) over the traced grid: the scene's device TLAS,
+// primitives and outlined BLAS nodes, the SSB of this render (ctx->ssb), the viewport's projection
+// matrix and clipping planes.
+static int draw_overlays(st_ctx *ctx, SceneSlot &S, const Viewport *vp, const ViewDev &v, int what, FloatPixel *grid,
+                         FloatPixel *grid_host, cudaStream_t st) {
+    OverlayParams op;
+    memset(&op, 0, sizeof(op));
+    const bool bvh = (what & ST_OVERLAY_BVH) != 0;
+    op.nodes = P<BVHNode>(S.tlas_nodes);
+    op.node_count = bvh ? S.tlas_node_count : 0;
+    op.leaf_ids = P<u32t>(S.tlas_leaf_ids);
+    op.prims = P<Primitive>(S.prims_raw);
+    op.n_prims = (what & ST_OVERLAY_SSB) ? S.n_prims : 0;
+    op.outlines = P<OutlineBox>(S.outlines);
+    op.outline_range = P<uint2>(S.outline_ranges);
+    op.n_meshes = (u32t)S.outline_host.size();
+    op.cam_pos = v.cam_pos;
+    op.cam_rot_inv = v.cam_rot_inv;
+    memcpy(op.proj, &vp->projection_matrix, sizeof(op.proj));
+    op.near_plane = vp->settings.near_clipping_plane_distance;
+    op.far_plane = vp->settings.far_clipping_plane_distance;
+    op.focal_length = v.focal_length;
+    const Dimensions &d = vp->frame_buffer->dimensions;
+    op.width_over_height = d.width_over_height;
+    op.h_width = d.h_width;
+    op.h_height = d.h_height;
+    op.f_height = d.f_height;
+    op.width = d.width;
+    op.height = d.height;
+    op.stride = d.width;
+    op.pos_x = vp->position.x;
+    op.pos_y = vp->position.y;
+    op.grid_pixels = v.grid_w * v.grid_h;
+    // boxes drawBVH draws: one per node, one per implicit primitive, the outlines of each mesh
+    // instance (every primitive sits in exactly one leaf of a valid TLAS)
+    u32t n_boxes = 0;
+    if (bvh) {
+        n_boxes = S.tlas_node_count;
+        for (const Primitive &p : S.prims_host) {
+            if (p.type == PrimitiveType_Mesh) n_boxes += p.id < S.outline_host.size() ? S.outline_host[p.id].y : 0;
+            else if (p.type == PrimitiveType_Box || p.type == PrimitiveType_Quad || p.type == PrimitiveType_Sphere ||
+                     p.type == PrimitiveType_Tetrahedron)
+                n_boxes += 1;
+        }
+    }
+    ST_TRY(reserve(ctx, ctx->overlay_scratch, overlay_scratch_bytes(op, n_boxes)));
+    u32t n_frags = 0;
+    ST_CUDA(overlay_count(op, P<int4>(ctx->ssb), n_boxes, ctx->overlay_scratch.ptr, &n_frags, st));
+    if (!n_frags) return ST_OK;
+    ST_TRY(reserve(ctx, ctx->overlay_frags, overlay_fragment_bytes(n_frags)));
+    ST_CUDA(overlay_draw(op, P<int4>(ctx->ssb), n_boxes, ctx->overlay_scratch.ptr, n_frags, ctx->overlay_frags.ptr, grid,
+                         grid_host, st));
+    return ST_OK;
+}
+
 int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *viewport, st_render_options *o) {
     SceneSlot *S = slot_of(ctx, slot);
     if (!S || !viewport) return ST_ERR_INVALID_ARG;
@@ -934,6 +1016,8 @@ int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *view
                  P<unsigned long long>(ctx->counters), o->count_work != 0, st, mapped_float);
     ST_CUDA(cudaGetLastError());
     ST_CUDA(cudaEventRecord(ctx->ev[2], st));
+    if (o->overlays & (ST_OVERLAY_BVH | ST_OVERLAY_SSB))
+        ST_TRY(draw_overlays(ctx, *S, viewport, v, o->overlays, dev_float, mapped_float, st));
     if (dev_u8) launch_resolve(dev_float, v.grid_w, W, H, mapped_u8 ? mapped_u8 : dev_u8, st);
     ST_CUDA(cudaEventRecord(ctx->ev[3], st));
     if (!o->device_outputs) {
@@ -1213,6 +1297,7 @@ int st_render_scene(st_ctx *ctx, int slot, const Scene *scene, Viewport *viewpor
     if (!viewport || !viewport->frame_buffer) return ST_ERR_INVALID_ARG;
     st_render_options o;
     memset(&o, 0, sizeof(o));
+    o.overlays = (viewport->settings.show_BVH ? ST_OVERLAY_BVH : 0) | (viewport->settings.show_SSB ? ST_OVERLAY_SSB : 0);
     return st_render_ex(ctx, slot, scene, viewport, &o);
 }
 

@@ -251,6 +251,25 @@ __global__ void rs_scatter_kernel(const u32t *kin, const u32t *vin, u32t *kout, 
     }
 }
 
+size_t radix_sort_scratch_bytes(u32t n) {
+    const size_t nblocks = (n + RS_TILE - 1) / RS_TILE;
+    const size_t hist = 256 * nblocks;
+    return sizeof(u32t) * (hist + (hist + SCAN_BLOCK - 1) / SCAN_BLOCK + 64);
+}
+int radix_sort_pairs(u32t *k0, u32t *v0, u32t *k1, u32t *v1, u32t n, int passes, void *scratch, cudaStream_t st) {
+    const u32t nblocks = (n + RS_TILE - 1) / RS_TILE;
+    u32t *hist = static_cast<u32t *>(scratch), *sums = hist + (size_t)256 * nblocks;
+    u32t *kin = k0, *vin = v0, *kout = k1, *vout = v1;
+    for (int pass = 0; pass < passes; pass++) {
+        rs_hist_kernel<<<nblocks, RS_THREADS, 0, st>>>(kin, n, 8 * pass, hist, nblocks);
+        scan_exclusive_u32(hist, hist, 256 * nblocks, sums, nullptr, st);
+        rs_scatter_kernel<<<nblocks, RS_THREADS, 0, st>>>(kin, vin, kout, vout, n, 8 * pass, hist, nblocks);
+        u32t *tk = kin; kin = kout; kout = tk;
+        u32t *tv = vin; vin = vout; vout = tv;
+    }
+    return passes & 1;
+}
+
 // ---- Karras topology ------------------------------------------------------------------------------
 __device__ __forceinline__ int delta(const u32t *codes, const u32t *order, u32t n, int i, int j) {
     if (j < 0 || j >= (int)n) return -1;

@@ -120,4 +120,50 @@ void launch_make_primdev(const Primitive *prims, u32t n, PrimDev *out, cudaStrea
 void launch_scatter_prims(const Primitive *recs, const u32t *ids, u32t count, Primitive *raw, PrimDev *dev,
                           cudaStream_t st);
 
+// ---- shared primitives (st_bvh.cu) ----
+// Exclusive scan of n u32 values (in place allowed); sums: (n/1024 + 1) words of scratch; total
+// (optional, device) receives the sum.
+void scan_exclusive_u32(const u32t *in, u32t *out, u32t n, u32t *sums, u32t *total, cudaStream_t st);
+// Stable LSD radix sort of n (key, value) pairs on the low 8*passes bits of the keys, ping-ponging
+// between (k0, v0) and (k1, v1); returns 1 when the result is in (k1, v1), 0 when in (k0, v0).
+// scratch: radix_sort_scratch_bytes(n) bytes.
+size_t radix_sort_scratch_bytes(u32t n);
+int radix_sort_pairs(u32t *k0, u32t *v0, u32t *k1, u32t *v1, u32t n, int passes, void *scratch, cudaStream_t st);
+
+// ---- debug overlays (st_overlay.cu): drawBVH raytracer.h:46, drawSSB SSB.h:175 ----
+// One BLAS node drawMeshAccelerationStructure outlines (depth <= 5): its box and colour id
+// (Magenta leaf, Green inner, Blue root).
+struct OutlineBox {
+    float aabb[6];
+    u32t color, pad;
+};
+struct OverlayParams {
+    const BVHNode *nodes;          // the TLAS (reference layout), node_count nodes; null: no BVH overlay
+    u32t node_count;
+    const u32t *leaf_ids;
+    const Primitive *prims;
+    u32t n_prims;
+    const OutlineBox *outlines;    // every mesh's outlined nodes, in node order
+    const uint2 *outline_range;    // per mesh: (first outline, count)
+    u32t n_meshes;
+    v3 cam_pos;
+    q4 cam_rot_inv;                // camera->transform.rotation_inverted
+    float proj[16];                // viewport->projection_matrix, rows X Y Z W
+    float near_plane, far_plane, focal_length;
+    float width_over_height, h_width, h_height, f_height;   // frame buffer Dimensions
+    u32t width, height, stride;    // frame buffer width/height (the QCAA grid); stride = width
+    int pos_x, pos_y;              // viewport->position
+    u32t grid_pixels;              // pixels in the float grid
+};
+// Device scratch for one overlay pass with n_boxes boxes (0: drawSSB only).
+size_t overlay_scratch_bytes(const OverlayParams &P, u32t n_boxes);
+size_t overlay_fragment_bytes(u32t n_frags);
+// Pass 1: boxes, edges and the number of pixels the overlays plot (synchronises `st`).
+cudaError_t overlay_count(const OverlayParams &P, const int4 *ssb, u32t n_boxes, void *scratch, u32t *n_frags,
+                          cudaStream_t st);
+// Pass 2: plot, sort by pixel and blend into grid (and grid_host, a device view of a page-locked
+// host copy, when non-null).  frag_buf: overlay_fragment_bytes(n_frags) bytes.
+cudaError_t overlay_draw(const OverlayParams &P, const int4 *ssb, u32t n_boxes, void *scratch, u32t n_frags,
+                         void *frag_buf, FloatPixel *grid, FloatPixel *grid_host, cudaStream_t st);
+
 }  // namespace st

@@ -176,6 +176,25 @@ def set_projection_plane(vp: S.Viewport, cam: S.Camera, grid_w: int, grid_h: int
     pp.down.x, pp.down.y, pp.down.z = [F32(v) for v in down]
 
 
+def set_projection_matrix(vp: S.Viewport, cam: S.Camera, dim: S.Dimensions):
+    """setProjectionMatrix (viewport/viewport.h:95) in float32: the matrix beginDrawing leaves in
+    viewport->projection_matrix, which the debug overlays project their edges with."""
+    n = F32(vp.settings.near_clipping_plane_distance)
+    f = F32(vp.settings.far_clipping_plane_distance)
+    fl = F32(cam.focal_length)
+    ar = F32(dim.height_over_width)
+    gl = bool(vp.settings.use_cube_NDC)
+    M = vp.projection_matrix
+    for row in (M.X, M.Y, M.Z, M.W):
+        row.x = row.y = row.z = row.w = 0.0
+    M.Z.w = 1.0
+    M.X.x = F32(fl * ar)
+    M.Y.y = fl
+    zz = F32(F32(1.0) / F32(f - n))
+    M.Z.z = F32(zz * (F32(f + n) if gl else f))
+    M.W.z = F32(zz * (F32(F32(F32(-2) * f) * n) if gl else F32(F32(-n) * f)))
+
+
 def update_dimensions(dim: S.Dimensions, width, height, qcaa=True):
     """updateDimensions (core/base.h:344)."""
     if qcaa:
@@ -220,6 +239,7 @@ class Frame:
         s.use_GPU = 1
         vp.trace.depth = depth
         set_projection_plane(vp, self.camera, self.grid_w, self.grid_h)
+        set_projection_matrix(vp, self.camera, self.grid.dimensions)
         vp.projection_plane.cone_angle = F32(cone_angle)
 
     @property

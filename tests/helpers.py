@@ -61,10 +61,10 @@ def reference_frame(sd, cam, w, h, depth=2, mode=S.RM_BEAUTY, cone_angle=0.0, th
     return fr
 
 
-def gpu_frame(renderer, slot, sd, cam, w, h, depth=2, mode=S.RM_BEAUTY, cone_angle=0.0, counters=False):
+def gpu_frame(renderer, slot, sd, cam, w, h, depth=2, mode=S.RM_BEAUTY, cone_angle=0.0, counters=False, overlays=0):
     fr = scenes.Frame(w, h, cam, depth=depth, mode=mode, cone_angle=cone_angle)
     ids = np.zeros(fr.rays, dtype=np.uint32)
-    opt = renderer.render(slot, sd, fr, prim_ids=ids, count_work=counters)
+    opt = renderer.render(slot, sd, fr, prim_ids=ids, count_work=counters, overlays=overlays)
     fr.prim_ids = ids
     fr.options = opt
     fr.counters = np.array([opt.counters[k] for k in range(16)], dtype=np.uint64)
@@ -144,3 +144,39 @@ def light_coords(sd, cam, w, h, step=2):
     """Pixels whose picking ray hits a light's glow sphere (scanned with the oracle)."""
     coords = [(x, y) for y in range(0, h, step) for x in range(0, w, step)]
     return [c for c, r in zip(coords, picks(sd, cam, w, h, coords)) if r.found and r.object_type == 6]
+
+
+def overlay_frame(sd, cam, w, h, what, which="orc", depth=1, mode=S.RM_BEAUTY):
+    """The oracle's render of the view with the debug overlays (what: 1 = drawBVH, 2 = drawSSB)
+    drawn over it by the oracle ("orc") or by the reference's own drawBVH/drawSSB ("ref").
+    Returns the Frame; its float grid holds the overlaid pixels and `base` the render under them."""
+    fr = oracle_frame(sd, cam, w, h, depth=depth, mode=mode)
+    fr.base = fr.float_pixels.copy()
+    lib = oracle.restatement() if which == "orc" else oracle.reference()
+    d = sd.copy()
+    sc, keep = d.to_ctypes()
+    (lib.orc_update_scene_ssb if which == "orc" else lib.ref_update_scene_ssb)(C.byref(sc), C.byref(fr.viewport))
+    if which == "orc":
+        lib.orc_draw_overlays(C.byref(sc), C.byref(fr.viewport), what)
+    else:
+        assert lib.ref_draw_overlays(C.byref(sc), C.byref(fr.viewport), what) == 0
+    return fr
+
+
+def overlay_scene(which):
+    """Scenes of the overlay tests: config0, the area-light example, config1 at test scale (reference
+    BLAS), cameras inside them (edges cut by the near and side planes), and 384 primitives (a TLAS
+    past the reference's 255-node drawBVH limit)."""
+    if which in ("config0", "inside"):
+        sd, cam = scenes.config0()
+    elif which == "area":
+        sd, cam = scenes.example_area_lights()
+    elif which == "config2":
+        sd, cam = scenes.config2(count=384, spread=6.0)
+    else:
+        sd, cam = small_config1(subdivisions=3, texture_size=64, blas="ref" if oracle.reference_available() else "orc")
+    if which == "inside":
+        cam = scenes.CameraSpec((0.5, 0.3, -1.0), 0.4, 0.2, 2.0)
+    elif which == "inside_mesh":
+        cam = scenes.look_at((1.0, 1.5, -3.0), (0.0, 1.0, 4.0))
+    return sd, cam

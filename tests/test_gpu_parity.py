@@ -306,3 +306,54 @@ def test_pick_equals_oracle(renderer, which):
     orc = [H.pick_key(r) for r in H.picks(sd, cam, w, h, coords)]
     assert dev == orc
     assert any(k[0] for k in dev)
+
+
+@pytest.mark.parametrize("which", ["config0", "area", "config1", "inside", "inside_mesh", "config2"])
+@pytest.mark.parametrize("what", [1, 2, 3])
+def test_overlays_equal_oracle(renderer, which, what):
+    """drawBVH / drawSSB (render/raytracer.h:46, render/SSB.h:175) drawn by the device over a
+    byte-exact render (normals mode): the float grid equals the oracle's overlaid grid byte for
+    byte.  config2 has 384 primitives, a TLAS past the reference's 255-node drawBVH limit."""
+    sd, cam = H.overlay_scene(which)
+    H.tlas_sah(sd)
+    renderer.upload(4, sd, tlas="host")
+    g = H.gpu_frame(renderer, 4, sd, cam, 320, 240, depth=1, mode=S.RM_NORMALS, overlays=what)
+    o = H.overlay_frame(sd, cam, 320, 240, what, "orc", depth=1, mode=S.RM_NORMALS)
+    touched = np.count_nonzero(o.float_pixels.view(np.uint8).reshape(o.rays, -1)
+                               != o.base.view(np.uint8).reshape(o.rays, -1), axis=1)
+    print(which, what, "pixels drawn", np.count_nonzero(touched))
+    assert np.count_nonzero(touched) > 100
+    assert g.float_pixels.tobytes() == o.float_pixels.tobytes()
+
+
+def test_overlays_over_beauty_add_no_difference(renderer):
+    """Over a beauty render (within tolerance of the oracle, not byte-exact), the overlays add no
+    difference of their own: every pixel where the overlaid grids differ already differs without
+    the overlays."""
+    sd, cam = H.overlay_scene("config1")
+    H.tlas_sah(sd)
+    renderer.upload(4, sd, tlas="host")
+    g0 = H.gpu_frame(renderer, 4, sd, cam, 320, 180, depth=4)
+    g = H.gpu_frame(renderer, 4, sd, cam, 320, 180, depth=4, overlays=3)
+    o = H.overlay_frame(sd, cam, 320, 180, 3, "orc", depth=4)
+    diff = lambda a, b: np.any(a.view(np.uint8).reshape(len(a), -1) != b.view(np.uint8).reshape(len(b), -1), axis=1)
+    before = diff(g0.float_pixels, o.base)
+    after = diff(g.float_pixels, o.float_pixels)
+    assert not np.any(after & ~before)
+    assert np.count_nonzero(diff(g.float_pixels, g0.float_pixels)) > 100
+
+
+def test_render_scene_draws_overlays_from_viewport_settings(renderer):
+    """st_render_scene draws drawBVH / drawSSB when viewport->settings.show_BVH / show_SSB are set,
+    as st_render_ex does with the overlay bits."""
+    sd, cam = H.overlay_scene("config0")
+    H.tlas_sah(sd)
+    renderer.upload(4, sd, tlas="host")
+    a = H.gpu_frame(renderer, 4, sd, cam, 200, 150, depth=1, mode=S.RM_NORMALS, overlays=3)
+    fr = scenes.Frame(200, 150, cam, depth=1, mode=S.RM_NORMALS)
+    fr.viewport.settings.show_BVH = 1
+    fr.viewport.settings.show_SSB = 1
+    sc, keep = sd.to_ctypes()
+    assert renderer.L.st_render_scene(renderer.ctx, 4, C.byref(sc), C.byref(fr.viewport)) == 0
+    assert fr.float_pixels.tobytes() == a.float_pixels.tobytes()
+    assert np.array_equal(fr.pixels, a.pixels)

@@ -243,3 +243,37 @@ def test_pick_matches_reference(which):
     assert any(k[0] for k in a)
     if which == "config0":
         assert any(k[1] == 6 for k in a), "no pixel hit a light"
+
+
+def test_projection_matrix_matches_begin_drawing():
+    """scenes.set_projection_matrix equals the matrix the reference's beginDrawing leaves
+    (setProjectionMatrix, viewport/viewport.h:95), bit for bit, with and without cube NDC."""
+    if not oracle.reference_available():
+        pytest.skip("reference harness not built")
+    ref = oracle.reference()
+    sd, cam = scenes.config0()
+    for cube in (0, 1):
+        fr = scenes.Frame(200, 150, cam, with_pixels=False)
+        fr.viewport.settings.use_cube_NDC = cube
+        scenes.set_projection_matrix(fr.viewport, fr.camera, fr.grid.dimensions)
+        mine = bytes(fr.viewport.projection_matrix)
+        ref.ref_begin_drawing(C.byref(fr.viewport))
+        assert bytes(fr.viewport.projection_matrix) == mine
+
+
+@pytest.mark.parametrize("which", ["config0", "area", "config1", "inside", "inside_mesh"])
+def test_overlays_match_reference(which):
+    """drawBVH and drawSSB (render/raytracer.h:46, render/SSB.h:175): the oracle's overlays leave
+    the float grid byte-identical to the reference's own drawing over the same render, for the
+    BVH alone, the SSB alone and both."""
+    if not oracle.reference_available():
+        pytest.skip("reference harness not built")
+    sd, cam = H.overlay_scene(which)
+    H.tlas_sah(sd, "ref")
+    for what in (1, 2, 3):
+        a = H.overlay_frame(sd, cam, 160, 120, what, "orc")
+        b = H.overlay_frame(sd, cam, 160, 120, what, "ref")
+        assert a.float_pixels.tobytes() == b.float_pixels.tobytes()
+        changed = np.count_nonzero(a.float_pixels.view(np.uint8).reshape(len(a.float_pixels), -1)
+                                   != a.base.view(np.uint8).reshape(len(a.base), -1), axis=1)
+        assert np.count_nonzero(changed) > 100, "the overlay drew almost nothing"
