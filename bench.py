@@ -346,6 +346,44 @@ def config0_section(r, cpu_reference):
     return out
 
 
+def ingest_section(r, cpu_reference):
+    """Texture ingestion: loadTexture (bmp2texture.c:324) of the 1024x1024 RGB texture config 1 uses,
+    on the device through st_bake_texture (API wall time: image upload, bake, quads download into
+    host memory) beside the reference's CPU baker on one thread."""
+    import ctypes as C
+    L = r.L
+    rgb = scenes.perlin_textures(1024, 0x5EED0001)[0]
+    comps = np.ascontiguousarray(rgb[..., :3])
+    need = L.st_texture_bytes(1024, 1024, 1)
+    mem = np.zeros(need, dtype=np.uint8)
+    tex = S.Texture()
+    ts = []
+    for k in range(8):
+        t0 = time.perf_counter()
+        st = L.st_bake_texture(r.ctx, comps.ctypes.data, 1024, 1024, 24, 1, 1, C.byref(tex), mem.ctypes.data, need)
+        ts.append((time.perf_counter() - t0) * 1e3)
+        if st != 0:
+            return {"texture_bake": f"failed: status {st}"}
+    out = {"texture": "1024x1024 RGB, wrap, 9 mips", "bytes_out": int(need),
+           "device_bake_ms_p50": float(np.median(ts[3:]))}
+    if cpu_reference:
+        try:
+            import oracle
+            if oracle.reference_available():
+                ref = oracle.reference()
+                rts = []
+                for _ in range(3):
+                    rt = S.Texture()
+                    t0 = time.perf_counter()
+                    ref.ref_load_texture(C.byref(rt), 1024, 1024, 1, 1, comps.ctypes.data, 24)
+                    rts.append((time.perf_counter() - t0) * 1e3)
+                    ref.ref_free_texture(C.byref(rt))
+                out["reference_cpu_bake_ms_p50"] = float(np.median(rts))
+        except Exception as ex:  # reported, never required
+            out["reference_cpu_bake_ms_p50"] = f"failed: {ex}"
+    return out
+
+
 def measure_l2_gbs():
     """Read bandwidth of a 48 MB float32 array that stays in the 126 MB L2 (torch.sum, CUDA events):
     the denominator of the trace kernel's L2 fraction."""
@@ -498,6 +536,7 @@ def main():
         if args.dynamic_frames > 0 else None
     l2_gbs = measure_l2_gbs()
     cfg0 = config0_section(r, rank == 0 and world == 1 and not args.no_cpu_baseline)
+    ingest = ingest_section(r, rank == 0 and world == 1 and not args.no_cpu_baseline)
 
     # ---- roofline of the trace kernel -----------------------------------------------------------
     trace_avg_ms = sum(trace_ms) / len(trace_ms)
@@ -554,6 +593,7 @@ def main():
             "counters": counters,
             "config0": cfg0,
             "dynamic_tlas": dynamic,
+            "ingest": ingest,
             "batched": mixed["batched"] if mixed else None,
             "served": mixed["served"] if mixed else None,
             "clocks": clocks.summary(),

@@ -44,7 +44,8 @@ enum st_status {
     ST_ERR_BAD_SCENE = 9,       /* the scene data is inconsistent (e.g. a leaf id out of range) */
     ST_ERR_QUEUE_FULL = 10,     /* the serving queue has no free slot */
     ST_ERR_NOT_READY = 11,      /* st_poll: the request is still running */
-    ST_ERR_CANCELLED = 12       /* st_poll: the request was cancelled before it ran */
+    ST_ERR_CANCELLED = 12,      /* st_poll: the request was cancelled before it ran */
+    ST_ERR_IO = 13              /* a file could not be opened, or was shorter than its header says */
 };
 
 /* TLAS/BLAS build modes for st_update_scene_bvh / st_update_mesh_bvh. */
@@ -280,6 +281,36 @@ ST_API int st_wait(st_ctx *ctx, st_ticket ticket, st_result *result, double time
 ST_API int st_serve_stop(st_ctx *ctx);
 /* The library's steady clock, in seconds. */
 ST_API double st_clock(void);
+
+/* ---- ingestion: textures and the reference's file formats ----------------------------------- */
+/* loadTexture (bmp2texture.c:324) on the device: an 8-bit image (`components`, row-major RGB, or
+ * RGBX when bit_count == 32) -> the reference's texture: wrap/mipmap flags, the mip chain (halving
+ * while both sides exceed 4 when mipmap is set), each mip a (w+1)x(h+1) TexelQuad grid with the
+ * reference's edge replication, byte-identical to the reference's baker.  `memory` (host,
+ * st_texture_bytes bytes) receives the TextureMip table and the quads; texture->mips points into it.
+ * width and height must be at least 2. */
+ST_API uint64_t st_texture_bytes(uint16_t width, uint16_t height, int mipmap);
+ST_API int st_bake_texture(st_ctx *ctx, const uint8_t *components, uint16_t width, uint16_t height, int bit_count,
+                           int wrap, int mipmap, Texture *texture, void *memory, uint64_t memory_bytes);
+
+/* .mesh files (scene/io.h:62-175): st_mesh_file_bytes = the host memory st_read_mesh_file needs
+ * (getMeshMemorySize), or -1 when the header cannot be read; st_read_mesh_file = loadMeshFromFile
+ * into `memory` (mesh's arrays point into it; bvh.nodes has room for 2 * triangle_count nodes);
+ * st_write_mesh_file = saveMeshToFile. */
+ST_API int64_t st_mesh_file_bytes(const char *path);
+ST_API int st_read_mesh_file(const char *path, Mesh *mesh, void *memory, uint64_t memory_bytes);
+ST_API int st_write_mesh_file(const char *path, const Mesh *mesh);
+/* .texture files (scene/io.h:6-59; written by bmp2texture.c:367-385): sizes from the file's own mip
+ * table, so a file whose mip count differs from getTextureMemorySize's estimate still fits. */
+ST_API int64_t st_texture_file_bytes(const char *path);
+ST_API int st_read_texture_file(const char *path, Texture *texture, void *memory, uint64_t memory_bytes);
+ST_API int st_write_texture_file(const char *path, const Texture *texture);
+/* .scene files (scene/io.h:178-213): SceneSettings, cameras, primitives.  Reading takes the counts
+ * from the file, refuses (ST_ERR_BUDGET) more cameras or primitives than the capacities of
+ * scene->cameras / scene->primitives, keeps the caller's file-name strings (the file holds the
+ * writer's pointers) and re-points each camera's direction pointers at its own matrix. */
+ST_API int st_read_scene_file(const char *path, Scene *scene, uint32_t camera_capacity, uint32_t primitive_capacity);
+ST_API int st_write_scene_file(const char *path, const Scene *scene);
 
 #ifdef __cplusplus
 }

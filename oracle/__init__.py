@@ -73,6 +73,13 @@ def reference():
     lib.ref_free.argtypes = [C.c_void_p]
     lib.ref_draw_overlays.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
     lib.ref_draw_overlays.restype = C.c_int
+    lib.ref_save_mesh.argtypes = [C.c_void_p, C.c_char_p]
+    lib.ref_save_scene.argtypes = [C.c_void_p, C.c_char_p]
+    lib.ref_load_scene.argtypes = [C.c_void_p, C.c_char_p]
+    lib.ref_load_texture_file.argtypes = [C.c_void_p, C.c_char_p, C.c_uint64]
+    lib.ref_load_texture_file.restype = C.c_void_p
+    lib.bmp2texture.argtypes = [C.c_char_p, C.c_char_p, C.c_bool, C.c_bool]   # bmp2texture.c:364
+    lib.bmp2texture.restype = C.c_int
     return lib
 
 

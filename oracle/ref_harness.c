@@ -365,3 +365,45 @@ int ref_draw_overlays(Scene *scene, Viewport *viewport, int what) {
     if (what & 2) drawSSB(scene, viewport);
     return 0;
 }
+
+/* ---- the reference's file formats (scene/io.h) ---------------------------------------------- */
+static void *stOpenW(const char *path) { return fopen(path, "wb"); }
+static bool stWrite(void *in, unsigned size, void *handle) { return fwrite(in, 1, size, (FILE*)handle) == size; }
+static void fileCallbacks(Platform *platform) {
+    memset(platform, 0, sizeof(*platform));
+    platform->openFileForReading = (CallbackForFileOpen)stOpen;
+    platform->openFileForWriting = (CallbackForFileOpen)stOpenW;
+    platform->readFromFile = stRead;
+    platform->writeToFile = (CallbackForFileRW)stWrite;
+    platform->closeFile = stClose;
+}
+
+/* saveMeshToFile (scene/io.h:145) */
+void ref_save_mesh(Mesh *mesh, const char *path) {
+    Platform platform;
+    fileCallbacks(&platform);
+    saveMeshToFile(mesh, (char*)path, &platform);
+}
+
+/* saveSceneToFile (scene/io.h:199) and loadSceneFromFile (:178) */
+void ref_save_scene(Scene *scene, const char *path) {
+    Platform platform;
+    fileCallbacks(&platform);
+    saveSceneToFile(scene, (char*)path, &platform);
+}
+void ref_load_scene(Scene *scene, const char *path) {
+    Platform platform;
+    fileCallbacks(&platform);
+    loadSceneFromFile(scene, (char*)path, &platform);
+}
+
+/* loadTextureFromFile (scene/io.h:34) into an arena the harness allocates (free with ref_free) */
+void *ref_load_texture_file(Texture *texture, const char *path, u64 bytes) {
+    Platform platform;
+    fileCallbacks(&platform);
+    void *mem = calloc(1, bytes);
+    Memory memory;
+    initMemory(&memory, (u8*)mem, bytes);
+    loadTextureFromFile(texture, (char*)path, &platform, &memory);
+    return mem;
+}

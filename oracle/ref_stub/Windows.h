@@ -1,6 +1,6 @@
 /* Minimal stand-in for <Windows.h> so that the reference's bmp2texture.c compiles on Linux for the
- * oracle harness.  Only the bitmap header types that file names are declared; the harness never
- * calls its BMP reader, only its texture baker (bmp2texture.c:324 loadTexture). */
+ * oracle harness.  Only the bitmap header types that file names are declared, with the Win32
+ * packing (the 14-byte file header), so that its BMP reader parses real files. */
 #ifndef ST_REF_STUB_WINDOWS_H
 #define ST_REF_STUB_WINDOWS_H
 #include <stdint.h>

@@ -16,6 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libslimtracin_b200.so")
 
 ST_OK = 0
+ST_ERR_INVALID_ARG, ST_ERR_BUDGET, ST_ERR_BAD_SCENE, ST_ERR_IO = 1, 5, 9, 13
 ST_BVH_LBVH30, ST_BVH_BINNED_SAH, ST_BVH_REFIT = 1, 2, 3
 COUNTER_NAMES = ["primary_rays", "shadow_rays", "bounce_rays", "aabb_tests", "triangle_tests",
                  "primitive_tests", "leaf_id_reads", "shaded_hits", "texel_fetches", "mesh_entries"]
@@ -118,6 +119,16 @@ def lib():
             "st_wait": (i, [vp, u64, C.POINTER(st_result), C.c_double]),
             "st_serve_stop": (i, [vp]),
             "st_clock": (C.c_double, []),
+            "st_texture_bytes": (u64, [C.c_uint16, C.c_uint16, i]),
+            "st_bake_texture": (i, [vp, vp, C.c_uint16, C.c_uint16, i, i, i, vp, vp, u64]),
+            "st_mesh_file_bytes": (C.c_int64, [C.c_char_p]),
+            "st_read_mesh_file": (i, [C.c_char_p, vp, vp, u64]),
+            "st_write_mesh_file": (i, [C.c_char_p, vp]),
+            "st_texture_file_bytes": (C.c_int64, [C.c_char_p]),
+            "st_read_texture_file": (i, [C.c_char_p, vp, vp, u64]),
+            "st_write_texture_file": (i, [C.c_char_p, vp]),
+            "st_read_scene_file": (i, [C.c_char_p, vp, u32, u32]),
+            "st_write_scene_file": (i, [C.c_char_p, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

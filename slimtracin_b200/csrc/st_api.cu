@@ -310,6 +310,7 @@ const char *st_strerror(int s) {
         case ST_ERR_QUEUE_FULL: return "request queue full";
         case ST_ERR_NOT_READY: return "request not finished";
         case ST_ERR_CANCELLED: return "request cancelled";
+        case ST_ERR_IO: return "file missing or truncated";
         default: return "unknown status";
     }
 }
@@ -1299,6 +1300,57 @@ int st_render_scene(st_ctx *ctx, int slot, const Scene *scene, Viewport *viewpor
     memset(&o, 0, sizeof(o));
     o.overlays = (viewport->settings.show_BVH ? ST_OVERLAY_BVH : 0) | (viewport->settings.show_SSB ? ST_OVERLAY_SSB : 0);
     return st_render_ex(ctx, slot, scene, viewport, &o);
+}
+
+// ---- texture baking ----------------------------------------------------------------------------
+uint64_t st_texture_bytes(uint16_t width, uint16_t height, int mipmap) {
+    const int mips = texture_mip_count(width, height, mipmap != 0);
+    return ((sizeof(TextureMip) * mips + 15) & ~(size_t)15) + sizeof(TexelQuad) * texture_quad_count(width, height, mipmap != 0);
+}
+
+int st_bake_texture(st_ctx *ctx, const uint8_t *components, uint16_t width, uint16_t height, int bit_count, int wrap,
+                    int mipmap, Texture *texture, void *memory, uint64_t memory_bytes) {
+    if (!ctx || !components || !texture || !memory || width < 2 || height < 2 || (bit_count != 24 && bit_count != 32))
+        return ST_ERR_INVALID_ARG;
+    if (memory_bytes < st_texture_bytes(width, height, mipmap)) return ST_ERR_BUDGET;
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    const int mips = texture_mip_count(width, height, mipmap != 0);
+    const size_t quads = texture_quad_count(width, height, mipmap != 0);
+    const size_t image = (size_t)width * height * (bit_count / 8);
+    const size_t table = (sizeof(TextureMip) * mips + 15) & ~(size_t)15;
+    const size_t bytes = ((image + 255) & ~(size_t)255) + texture_scratch_bytes(width, height) + sizeof(TexelQuad) * quads + 512;
+    if (ctx->in_use + bytes > ctx->budget) return ST_ERR_BUDGET;
+    char *base = nullptr;
+    ST_CUDA(cudaMallocAsync((void **)&base, bytes, st));
+    uint8_t *dev_image = reinterpret_cast<uint8_t *>(base);
+    char *scratch = base + ((image + 255) & ~(size_t)255);
+    TexelQuad *dev_quads = reinterpret_cast<TexelQuad *>(scratch + ((texture_scratch_bytes(width, height) + 255) & ~(size_t)255));
+    cudaError_t e = cudaMemcpyAsync(dev_image, components, image, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = bake_texture(dev_image, width, height, bit_count, wrap != 0, mipmap != 0, scratch, dev_quads, st);
+    char *host = static_cast<char *>(memory);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(host + table, dev_quads, sizeof(TexelQuad) * quads, cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(base, st);
+    const cudaError_t e2 = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) return fail_cuda(ctx, e);
+    TextureMip *mip = reinterpret_cast<TextureMip *>(host);
+    TexelQuad *q = reinterpret_cast<TexelQuad *>(host + table);
+    u32t w = width, h = height;
+    for (int m = 0; m < mips; m++, w /= 2, h /= 2) {
+        mip[m].width = (u16)w;
+        mip[m].height = (u16)h;
+        mip[m].texel_quads = q;
+        q += (size_t)(w + 1) * (h + 1);
+    }
+    texture->width = width;
+    texture->height = height;
+    texture->wrap = wrap != 0;
+    texture->mipmap = mipmap != 0;
+    texture->mip_count = (u8)mips;
+    texture->mips = mip;
+    return ST_OK;
 }
 
 // ---- serving ---------------------------------------------------------------------------------

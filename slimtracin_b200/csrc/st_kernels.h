@@ -120,6 +120,15 @@ void launch_make_primdev(const Primitive *prims, u32t n, PrimDev *out, cudaStrea
 void launch_scatter_prims(const Primitive *recs, const u32t *ids, u32t count, Primitive *raw, PrimDev *dev,
                           cudaStream_t st);
 
+// ---- texture baking (st_texture.cu): loadTexture bmp2texture.c:324 ----
+int texture_mip_count(u32t width, u32t height, bool mipmap);
+size_t texture_quad_count(u32t width, u32t height, bool mipmap);
+size_t texture_scratch_bytes(u32t width, u32t height);
+// dev_components: width*height texels of 3 (bit_count 24) or 4 (32) bytes; scratch:
+// texture_scratch_bytes; dev_quads: texture_quad_count quads, mip after mip.
+cudaError_t bake_texture(const uint8_t *dev_components, u32t width, u32t height, int bit_count, bool wrap, bool mipmap,
+                         void *scratch, TexelQuad *dev_quads, cudaStream_t st);
+
 // ---- shared primitives (st_bvh.cu) ----
 // Exclusive scan of n u32 values (in place allowed); sums: (n/1024 + 1) words of scratch; total
 // (optional, device) receives the sum.
