@@ -311,6 +311,18 @@ ST_API int st_write_texture_file(const char *path, const Texture *texture);
  * writer's pointers) and re-points each camera's direction pointers at its own matrix. */
 ST_API int st_read_scene_file(const char *path, Scene *scene, uint32_t camera_capacity, uint32_t primitive_capacity);
 ST_API int st_write_scene_file(const char *path, const Scene *scene);
+/* obj2mesh (obj2mesh.c:25): a Wavefront OBJ with faces "f v/t/n v/t/n v/t/n" -> a Mesh ready for
+ * st_write_mesh_file or upload: positions, uvs, normals and their 1-based face indices read as the
+ * reference reads them (the same sscanf formats, lines of at most 1023 characters), winding
+ * optionally inverted, the AABB over the vertices and the origin with the vertices centred on its
+ * middle, the unique edges in first-appearance order (found on the device), and the BLAS with the
+ * Triangle records built on the device by `mode` (ST_BVH_LBVH30 or ST_BVH_BINNED_SAH; the reference
+ * uses its full-sweep SAH).  Arrays are carved from `memory` (st_obj_mesh_bytes bytes, -1 when the
+ * file cannot be read).  Other face layouts give ST_ERR_BAD_SCENE (the reference's updateMeshBVH
+ * reads vertex normals for every triangle). */
+ST_API int64_t st_obj_mesh_bytes(const char *obj_path);
+ST_API int st_obj_to_mesh(st_ctx *ctx, const char *obj_path, int invert_winding_order, int mode, Mesh *mesh,
+                          void *memory, uint64_t memory_bytes);
 
 #ifdef __cplusplus
 }

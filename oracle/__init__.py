@@ -80,6 +80,8 @@ def reference():
     lib.ref_load_texture_file.restype = C.c_void_p
     lib.bmp2texture.argtypes = [C.c_char_p, C.c_char_p, C.c_bool, C.c_bool]   # bmp2texture.c:364
     lib.bmp2texture.restype = C.c_int
+    lib.obj2mesh.argtypes = [C.c_char_p, C.c_char_p, C.c_bool]              # obj2mesh.c:25
+    lib.obj2mesh.restype = C.c_int
     return lib
 
 

@@ -1,10 +1,10 @@
 /*
  * ref_harness.c — TEST INFRASTRUCTURE, not part of the product.
  *
- * Compiles the reference's own tracing path (render/raytracer.h, the top-down SAH builder and the
- * bmp2texture texture baker) in place from the reference sources and exposes it to the tests and to
- * bench.py's reference arm as a shared library, oracle/_ref/libslimref.so.  Nothing in the product
- * links or loads this file.
+ * Compiles the reference's own tracing path (render/raytracer.h, the top-down SAH builder, the
+ * bmp2texture texture baker and the obj2mesh converter) in place from the reference sources and
+ * exposes it to the tests and to bench.py's reference arm as a shared library,
+ * oracle/_ref/libslimref.so.  Nothing in the product links or loads this file.
  *
  * The reference is written for Win32, where `unsigned long` is 32 bits.  To get that layout on
  * Linux without copying or patching any reference source, the reference headers are compiled with
@@ -30,6 +30,11 @@
 #include "render/raytracer.h"
 #define main st_ref_bmp2texture_main
 #include "bmp2texture.c"
+#undef main
+#define main st_ref_obj2mesh_main
+#define EndsWith st_ref_obj2mesh_EndsWith
+#include "obj2mesh.c"
+#undef EndsWith
 #undef main
 #undef long
 #undef u64

@@ -129,6 +129,8 @@ def lib():
             "st_write_texture_file": (i, [C.c_char_p, vp]),
             "st_read_scene_file": (i, [C.c_char_p, vp, u32, u32]),
             "st_write_scene_file": (i, [C.c_char_p, vp]),
+            "st_obj_mesh_bytes": (C.c_int64, [C.c_char_p]),
+            "st_obj_to_mesh": (i, [vp, C.c_char_p, i, i, vp, vp, u64]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libslimtracin_b200.so")
-SOURCES = ["st_api.cu", "st_render.cu", "st_bvh.cu", "st_sah.cu", "st_overlay.cu", "st_texture.cu", "st_io.cu"]
+SOURCES = ["st_api.cu", "st_render.cu", "st_bvh.cu", "st_sah.cu", "st_overlay.cu", "st_texture.cu", "st_io.cu", "st_obj.cu"]
 HEADERS = ["st_device.cuh", "st_trace.cuh", "st_kernels.h"]
 INCLUDES = [os.path.join(ROOT, "include"), CSRC]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",

@@ -1353,6 +1353,128 @@ int st_bake_texture(st_ctx *ctx, const uint8_t *components, uint16_t width, uint
     return ST_OK;
 }
 
+// ---- OBJ ingestion: obj2mesh.c:25 ---------------------------------------------------------------
+namespace {
+struct ObjCarve {
+    size_t nodes, leaf_ids, positions, position_ids, edges, triangles, uvs, uv_ids, normals, normal_ids, total;
+};
+ObjCarve obj_carve(const ObjCounts &c) {
+    ObjCarve k;
+    size_t at = 0;
+    auto take = [&](size_t b) { size_t o = at; at += (b + 15) & ~(size_t)15; return o; };
+    const size_t t = c.triangles;
+    k.nodes = take(sizeof(BVHNode) * 2 * t);
+    k.leaf_ids = take(sizeof(u32t) * t);
+    k.positions = take(sizeof(vec3) * (size_t)c.vertices);
+    k.position_ids = take(sizeof(TriangleVertexIndices) * t);
+    k.edges = take(sizeof(EdgeVertexIndices) * 3 * t);
+    k.triangles = take(sizeof(Triangle) * t);
+    k.uvs = take(sizeof(vec2) * (size_t)c.uvs);
+    k.uv_ids = take(sizeof(TriangleVertexIndices) * t);
+    k.normals = take(sizeof(vec3) * (size_t)c.normals);
+    k.normal_ids = take(sizeof(TriangleVertexIndices) * t);
+    k.total = at;
+    return k;
+}
+}  // namespace
+
+int64_t st_obj_mesh_bytes(const char *obj_path) {
+    ObjCounts c;
+    if (!obj_path || obj_count(obj_path, c) != 0) return -1;
+    return (int64_t)obj_carve(c).total;
+}
+
+int st_obj_to_mesh(st_ctx *ctx, const char *obj_path, int invert_winding_order, int mode, Mesh *mesh, void *memory,
+                   uint64_t memory_bytes) {
+    if (!ctx || !obj_path || !mesh || !memory || (mode != ST_BVH_LBVH30 && mode != ST_BVH_BINNED_SAH))
+        return ST_ERR_INVALID_ARG;
+    ObjCounts c;
+    if (obj_count(obj_path, c) != 0) return ST_ERR_IO;
+    // updateMeshBVH reads vertex normals and obj2mesh reads uvs for every face, so only the
+    // positions/uvs/normals face layout converts
+    if (c.layout != 3 || !c.triangles || !c.vertices || !c.uvs || !c.normals) return ST_ERR_BAD_SCENE;
+    const ObjCarve k = obj_carve(c);
+    if (k.total > memory_bytes) return ST_ERR_BUDGET;
+    char *base = static_cast<char *>(memory);
+    Mesh m;
+    memset(&m, 0, sizeof(m));
+    m.vertex_count = c.vertices;
+    m.triangle_count = c.triangles;
+    m.uvs_count = c.uvs;
+    m.normals_count = c.normals;
+    m.bvh.nodes = reinterpret_cast<BVHNode *>(base + k.nodes);
+    m.bvh.leaf_ids = reinterpret_cast<u32t *>(base + k.leaf_ids);
+    m.vertex_positions = reinterpret_cast<vec3 *>(base + k.positions);
+    m.vertex_position_indices = reinterpret_cast<TriangleVertexIndices *>(base + k.position_ids);
+    m.edge_vertex_indices = reinterpret_cast<EdgeVertexIndices *>(base + k.edges);
+    m.triangles = reinterpret_cast<Triangle *>(base + k.triangles);
+    m.vertex_uvs = reinterpret_cast<vec2 *>(base + k.uvs);
+    m.vertex_uvs_indices = reinterpret_cast<TriangleVertexIndices *>(base + k.uv_ids);
+    m.vertex_normals = reinterpret_cast<vec3 *>(base + k.normals);
+    m.vertex_normal_indices = reinterpret_cast<TriangleVertexIndices *>(base + k.normal_ids);
+    const int parsed = obj_parse(obj_path, invert_winding_order != 0, c, m.vertex_positions, m.vertex_normals, m.vertex_uvs,
+                                 reinterpret_cast<uint32_t *>(m.vertex_position_indices),
+                                 reinterpret_cast<uint32_t *>(m.vertex_uvs_indices),
+                                 reinterpret_cast<uint32_t *>(m.vertex_normal_indices));
+    if (parsed == -1) return ST_ERR_IO;
+    if (parsed != 0) return ST_ERR_BAD_SCENE;
+    // the AABB over the vertices and the origin (obj2mesh.c:185-193), then centred on its middle
+    // when that is not the origin (:195-202)
+    AABB box;
+    memset(&box, 0, sizeof(box));
+    for (u32t i = 0; i < m.vertex_count; i++) {
+        const vec3 &v = m.vertex_positions[i];
+        box.min.x = box.min.x < v.x ? box.min.x : v.x;
+        box.min.y = box.min.y < v.y ? box.min.y : v.y;
+        box.min.z = box.min.z < v.z ? box.min.z : v.z;
+        box.max.x = box.max.x > v.x ? box.max.x : v.x;
+        box.max.y = box.max.y > v.y ? box.max.y : v.y;
+        box.max.z = box.max.z > v.z ? box.max.z : v.z;
+    }
+    vec3 centre;
+    centre.x = (box.min.x + box.max.x) * 0.5f;
+    centre.y = (box.min.y + box.max.y) * 0.5f;
+    centre.z = (box.min.z + box.max.z) * 0.5f;
+    if (centre.x != 0 || centre.y != 0 || centre.z != 0) {
+        box.min.x -= centre.x; box.min.y -= centre.y; box.min.z -= centre.z;
+        box.max.x -= centre.x; box.max.y -= centre.y; box.max.z -= centre.z;
+        for (u32t i = 0; i < m.vertex_count; i++) {
+            vec3 &v = m.vertex_positions[i];
+            v.x -= centre.x;
+            v.y -= centre.y;
+            v.z -= centre.z;
+        }
+    }
+    m.aabb = box;
+    // unique edges on the device
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    const size_t ids_bytes = sizeof(uint32_t) * 3 * (size_t)m.triangle_count;
+    const size_t edges_bytes = sizeof(EdgeVertexIndices) * 3 * (size_t)m.triangle_count;
+    const size_t bytes = ((ids_bytes + 255) & ~(size_t)255) + ((edges_bytes + 255) & ~(size_t)255) +
+                         unique_edges_scratch_bytes(m.triangle_count);
+    if (ctx->in_use + bytes > ctx->budget) return ST_ERR_BUDGET;
+    char *dev = nullptr;
+    ST_CUDA(cudaMallocAsync((void **)&dev, bytes, st));
+    uint32_t *dev_ids = reinterpret_cast<uint32_t *>(dev);
+    EdgeVertexIndices *dev_edges = reinterpret_cast<EdgeVertexIndices *>(dev + ((ids_bytes + 255) & ~(size_t)255));
+    void *scratch = dev + ((ids_bytes + 255) & ~(size_t)255) + ((edges_bytes + 255) & ~(size_t)255);
+    u32t n_edges = 0;
+    cudaError_t e = cudaMemcpyAsync(dev_ids, m.vertex_position_indices, ids_bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = unique_edges(dev_ids, m.triangle_count, m.vertex_count, scratch, dev_edges, &n_edges, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(m.edge_vertex_indices, dev_edges, sizeof(EdgeVertexIndices) * n_edges, cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(dev, st);
+    const cudaError_t e2 = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) return fail_cuda(ctx, e);
+    m.edge_count = n_edges;
+    // updateMeshBVH on the device: BLAS and the leaf-ordered Triangle records
+    ST_TRY(st_update_mesh_bvh(ctx, &m, mode));
+    *mesh = m;
+    return ST_OK;
+}
+
 // ---- serving ---------------------------------------------------------------------------------
 double st_clock(void) {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();

@@ -129,6 +129,23 @@ size_t texture_scratch_bytes(u32t width, u32t height);
 cudaError_t bake_texture(const uint8_t *dev_components, u32t width, u32t height, int bit_count, bool wrap, bool mipmap,
                          void *scratch, TexelQuad *dev_quads, cudaStream_t st);
 
+// ---- OBJ ingestion (st_obj.cu): obj2mesh.c:25 ----
+struct ObjCounts {
+    uint32_t vertices = 0, normals = 0, uvs = 0, triangles = 0;
+    int layout = 0;    // face layout of obj2mesh: 0 unknown, 1 positions, 2 positions/uvs, 3 positions/uvs/normals
+};
+// Count pass: -1 when the file cannot be read.
+int obj_count(const char *path, ObjCounts &c);
+// Parse pass into caller arrays sized by `expect` (the count pass): -1 unreadable or changed file,
+// -2 a line that does not parse with the face layout or an index out of range.
+int obj_parse(const char *path, bool invert_winding, const ObjCounts &expect, vec3 *positions, vec3 *normals, vec2 *uvs,
+              uint32_t *position_ids, uint32_t *uv_ids, uint32_t *normal_ids);
+// The unique undirected triangle sides in first-appearance order (obj2mesh.c:209-234); dev_edges
+// holds up to 3 * n_triangles.  Synchronises `st`.
+size_t unique_edges_scratch_bytes(u32t n_triangles);
+cudaError_t unique_edges(const uint32_t *dev_ids, u32t n_triangles, u32t n_vertices, void *scratch,
+                         EdgeVertexIndices *dev_edges, u32t *n_edges, cudaStream_t st);
+
 // ---- shared primitives (st_bvh.cu) ----
 // Exclusive scan of n u32 values (in place allowed); sums: (n/1024 + 1) words of scratch; total
 // (optional, device) receives the sum.
