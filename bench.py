@@ -366,6 +366,45 @@ def ingest_section(r, cpu_reference):
             return {"texture_bake": f"failed: status {st}"}
     out = {"texture": "1024x1024 RGB, wrap, 9 mips", "bytes_out": int(need),
            "device_bake_ms_p50": float(np.median(ts[3:]))}
+    # obj2mesh: a displaced icosphere written as OBJ text (positions, uvs, normals), converted on
+    # the device (parse on the host's threads, device edges and binned-SAH BLAS) and by the
+    # reference's converter (full-sweep SAH, quadratic edge search) at the size it finishes in
+    import tempfile
+    tmp = tempfile.mkdtemp()
+
+    def write_obj(path, md):
+        with open(path, "w") as f:
+            f.write("\n".join("v %.9g %.9g %.9g" % tuple(p) for p in md.positions) + "\n")
+            f.write("\n".join("vt %.9g %.9g" % tuple(t) for t in md.uvs) + "\n")
+            f.write("\n".join("vn %.9g %.9g %.9g" % tuple(n) for n in md.normals) + "\n")
+            f.write("\n".join("f %d/%d/%d %d/%d/%d %d/%d/%d" % (a, a, a, b, b, b, c, c, c)
+                               for a, b, c in md.indices + 1) + "\n")
+
+    objs = {}
+    for sub in (5, 7):
+        md = scenes.displaced_icosphere(sub, 0x5EED0001)
+        path = os.path.join(tmp, f"ico{sub}.obj")
+        write_obj(path, md)
+        need = L.st_obj_mesh_bytes(path.encode())
+        omem = np.zeros(need, dtype=np.uint8)
+        m = S.Mesh()
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            st = L.st_obj_to_mesh(r.ctx, path.encode(), 0, 2, C.byref(m), omem.ctypes.data, need)
+            ts.append((time.perf_counter() - t0) * 1e3)
+        objs[sub] = path
+        out[f"obj_{len(md.indices)}_triangles_device_ms_p50"] = float(np.median(ts)) if st == 0 else f"failed: status {st}"
+    if cpu_reference:
+        try:
+            import oracle
+            if oracle.reference_available():
+                ref = oracle.reference()
+                t0 = time.perf_counter()
+                ref.obj2mesh(objs[5].encode(), os.path.join(tmp, "ref.mesh").encode(), False)
+                out["obj_20480_triangles_reference_cpu_ms"] = (time.perf_counter() - t0) * 1e3
+        except Exception as ex:  # reported, never required
+            out["obj_20480_triangles_reference_cpu_ms"] = f"failed: {ex}"
     if cpu_reference:
         try:
             import oracle
