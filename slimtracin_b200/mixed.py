@@ -42,21 +42,21 @@ def resident_scenes(mesh_subdivisions=(6, 7, 8), texture_size=1024, big=None):
             sd = big
         else:
             sd, _ = scenes.config1(seed_offset=200 + sub, subdivisions=sub, texture_size=texture_size)
-        out.append(Resident(f"mesh{sd.meshes[0].triangle_count}", sd, (0.0, 1.5, 0.0), 15.0, 8.0, "lbvh"))
+        out.append(Resident(f"mesh{sd.meshes[0].triangle_count}", sd, (0.0, 1.5, 0.0), 15.0, 8.0, "sah"))
     sd, _ = scenes.config2(seed_offset=300)
-    out.append(Resident("implicit4096", sd, (0.0, 0.0, 0.0), 20.0, 3.0, "lbvh"))
+    out.append(Resident("implicit4096", sd, (0.0, 0.0, 0.0), 20.0, 3.0, "sah"))
     return out
 
 
 def upload(renderer, residents, first_slot=0):
-    """Upload every scene into consecutive slots; mesh BLASes (LBVH30) and TLASes (binned SAH for
-    the small implicit scenes, LBVH30 otherwise) are built on the device."""
+    """Upload every scene into consecutive slots; mesh BLASes and TLASes are built on the device
+    with the binned SAH (the serving loop rebuilds moved scenes' TLASes with LBVH30)."""
     slots = []
     for k, res in enumerate(residents):
         slot = first_slot + k
         for md in res.sd.meshes:
             if md.triangle_count and not getattr(md, "device_built", False):
-                renderer.build_blas(md, api.ST_BVH_LBVH30)
+                renderer.build_blas(md, api.ST_BVH_BINNED_SAH)
                 md.device_built = True
         renderer.upload(slot, res.sd, tlas=None)
         renderer.build_tlas(slot, res.sd, api.ST_BVH_BINNED_SAH if res.tlas == "sah" else api.ST_BVH_LBVH30)
