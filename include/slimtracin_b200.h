@@ -193,6 +193,9 @@ typedef struct st_batch_options {
     float batch_ms;             /* out: CUDA-event time of the batch on the launch stream */
     uint64_t rays;              /* out: primary rays traced */
     int tile_shape_used, chunk_used, graph_replayed;   /* out */
+    int stack_placement;        /* -1: autotuned; 0: traversal stacks in local memory; 1: their first 16
+                                   entries in shared memory (the traversal is the same either way) */
+    int stack_placement_used;   /* out */
 } st_batch_options;
 
 /* Render `view_count` views (different sizes, scenes, render modes and bounce counts) with one

@@ -45,7 +45,8 @@ class st_view(C.Structure):
 class st_batch_options(C.Structure):
     _fields_ = [("stream", C.c_void_p), ("device_outputs", C.c_int), ("tile_shape", C.c_int), ("chunk", C.c_int),
                 ("use_graph", C.c_int), ("batch_ms", C.c_float), ("rays", C.c_uint64),
-                ("tile_shape_used", C.c_int), ("chunk_used", C.c_int), ("graph_replayed", C.c_int)]
+                ("tile_shape_used", C.c_int), ("chunk_used", C.c_int), ("graph_replayed", C.c_int),
+                ("stack_placement", C.c_int), ("stack_placement_used", C.c_int)]
 
 
 class st_serve_config(C.Structure):
@@ -265,7 +266,7 @@ class Renderer:
         return opt
 
 
-def render_batch(renderer, items, tile_shape=-1, chunk=0, use_graph=False, device_outputs=False):
+def render_batch(renderer, items, tile_shape=-1, chunk=0, use_graph=False, device_outputs=False, stack_placement=-1):
     """st_render_batch over items = [(slot, SceneData, Frame)]; outputs go to each Frame's buffers
     (host) unless device_outputs, in which case Frame.grid pointers are used as device pointers."""
     keep = []
@@ -280,6 +281,7 @@ def render_batch(renderer, items, tile_shape=-1, chunk=0, use_graph=False, devic
         views[k].out_u8 = fr.grid.pixels
     opt = st_batch_options()
     opt.tile_shape, opt.chunk, opt.use_graph, opt.device_outputs = tile_shape, chunk, int(use_graph), int(device_outputs)
+    opt.stack_placement = stack_placement
     renderer._check(renderer.L.st_render_batch(renderer.ctx, views, len(items), C.byref(opt)), "st_render_batch")
     return opt
 

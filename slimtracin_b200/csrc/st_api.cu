@@ -77,7 +77,7 @@ struct BatchState {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     std::string graph_key;
-    std::map<std::string, std::pair<int, int>> tuned;   // scene-class key -> (tile shape, chunk)
+    std::map<std::string, std::pair<int, int>> tuned;   // scene-class key -> (kernel variant, chunk)
 };
 
 struct ServeReq {
@@ -142,7 +142,7 @@ struct st_ctx {
     int device = 0;
     Server server;
     int sm_count = 148;
-    int blocks_per_sm[TILE_SHAPES] = {1, 1, 1, 1};
+    int blocks_per_sm[BATCH_VARIANTS] = {1, 1, 1, 1, 1, 1, 1, 1};
     BatchState batch;
     cudaStream_t stream = nullptr;
     uint64_t budget = 0, in_use = 0;
@@ -345,7 +345,7 @@ int st_init(st_ctx **out, const st_config *cfg) {
         return ST_ERR_CUDA;
     }
     cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
-    for (int t = 0; t < TILE_SHAPES; t++) ctx->blocks_per_sm[t] = batch_blocks_per_sm(t);
+    for (int t = 0; t < BATCH_VARIANTS; t++) ctx->blocks_per_sm[t] = batch_blocks_per_sm(t);
     if (const char *path = getenv("ST_AUTOTUNE_CACHE")) {
         std::ifstream f(path);
         std::string key;
@@ -1164,47 +1164,58 @@ int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *
     st_batch_options dflt;
     memset(&dflt, 0, sizeof(dflt));
     dflt.tile_shape = -1;
+    dflt.stack_placement = -1;
     st_batch_options &o = opt ? *opt : dflt;
     cudaStream_t st = o.stream ? (cudaStream_t)o.stream : ctx->stream;
     BatchState &B = ctx->batch;
-    // the tile shape and queue chunk: given, cached for this scene class, or tuned now
+    // the kernel variant (tile shape, stack placement) and queue chunk: given, cached for this scene
+    // class, or tuned now
+    if (o.tile_shape >= TILE_SHAPES || o.stack_placement >= STACK_PLACEMENTS) return ST_ERR_INVALID_ARG;
     BatchPlan p;
-    int tile = o.tile_shape;
+    int tile = (o.tile_shape >= 0 && o.stack_placement >= 0) ? o.tile_shape + TILE_SHAPES * o.stack_placement : -1;
     u32t chunk = o.chunk > 0 ? (u32t)o.chunk : 0;
-    ST_TRY(plan_batch(ctx, views, n, tile >= 0 ? tile : 0, o, p));
+    ST_TRY(plan_batch(ctx, views, n, o.tile_shape >= 0 ? o.tile_shape : 0, o, p));
     if (tile < 0 || chunk == 0) {
         auto it = B.tuned.find(p.class_key);
-        if (it != B.tuned.end()) {
+        const bool fits = it != B.tuned.end() && (o.tile_shape < 0 || variant_tile(it->second.first) == o.tile_shape) &&
+                          (o.stack_placement < 0 || variant_stack(it->second.first) == o.stack_placement);
+        if (fits) {
             if (tile < 0) tile = it->second.first;
             if (!chunk) chunk = (u32t)it->second.second;
         } else {
             const int shapes[4] = {TILE_8x4, TILE_16x2, TILE_4x8, TILE_32x1};
             const u32t chunks[2] = {1, 4};
             float best = INFINITY;
-            int best_tile = TILE_8x4;
+            int best_variant = TILE_8x4;
             u32t best_chunk = 1;
-            for (int si = 0; si < 4; si++) {
-                if (tile >= 0 && shapes[si] != tile) continue;
-                for (u32t c : chunks) {
-                    if (chunk && c != chunk) continue;
-                    BatchPlan q;
-                    ST_TRY(plan_batch(ctx, views, n, shapes[si], o, q));
-                    ST_TRY(batch_reserve(ctx, B, q, n));
-                    ST_CUDA(cudaEventRecord(ctx->ev[0], st));
-                    ST_TRY(enqueue_batch(ctx, B, P<unsigned>(ctx->status), views, n, q, shapes[si], c, st, o));
-                    ST_CUDA(cudaEventRecord(ctx->ev[1], st));
-                    ST_CUDA(cudaStreamSynchronize(st));
-                    float ms = 0;
-                    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
-                    if (ms < best) { best = ms; best_tile = shapes[si]; best_chunk = c; }
+            for (int stack = 0; stack < STACK_PLACEMENTS; stack++) {
+                if (o.stack_placement >= 0 && stack != o.stack_placement) continue;
+                for (int si = 0; si < 4; si++) {
+                    if (o.tile_shape >= 0 && shapes[si] != o.tile_shape) continue;
+                    const int variant = shapes[si] + TILE_SHAPES * stack;
+                    for (u32t c : chunks) {
+                        if (chunk && c != chunk) continue;
+                        BatchPlan q;
+                        ST_TRY(plan_batch(ctx, views, n, variant, o, q));
+                        ST_TRY(batch_reserve(ctx, B, q, n));
+                        ST_CUDA(cudaEventRecord(ctx->ev[0], st));
+                        ST_TRY(enqueue_batch(ctx, B, P<unsigned>(ctx->status), views, n, q, variant, c, st, o));
+                        ST_CUDA(cudaEventRecord(ctx->ev[1], st));
+                        ST_CUDA(cudaStreamSynchronize(st));
+                        float ms = 0;
+                        cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+                        if (ms < best) { best = ms; best_variant = variant; best_chunk = c; }
+                    }
                 }
             }
-            B.tuned[p.class_key] = {best_tile, (int)best_chunk};
-            if (const char *path = getenv("ST_AUTOTUNE_CACHE")) {
-                std::ofstream f(path, std::ios::app);
-                f << p.class_key << " " << best_tile << " " << best_chunk << "\n";
+            if (o.tile_shape < 0 && o.stack_placement < 0 && !o.chunk) {
+                B.tuned[p.class_key] = {best_variant, (int)best_chunk};
+                if (const char *path = getenv("ST_AUTOTUNE_CACHE")) {
+                    std::ofstream f(path, std::ios::app);
+                    f << p.class_key << " " << best_variant << " " << best_chunk << "\n";
+                }
             }
-            if (tile < 0) tile = best_tile;
+            if (tile < 0) tile = best_variant;
             if (!chunk) chunk = best_chunk;
         }
         ST_TRY(plan_batch(ctx, views, n, tile, o, p));
@@ -1263,7 +1274,8 @@ int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *
     ST_CUDA(cudaStreamSynchronize(st));
     cudaEventElapsedTime(&o.batch_ms, ctx->ev[0], ctx->ev[1]);
     o.rays = p.rays;
-    o.tile_shape_used = tile;
+    o.tile_shape_used = variant_tile(tile);
+    o.stack_placement_used = variant_stack(tile);
     o.chunk_used = (int)chunk;
     if (status[0] & S_STACK_OVERFLOW) return ST_ERR_STACK_OVERFLOW;
     return ST_OK;

@@ -36,12 +36,19 @@ struct BatchView {
     u32t tile_begin, tiles_x;
 };
 enum TileShape { TILE_8x4 = 0, TILE_16x2 = 1, TILE_32x1 = 2, TILE_4x8 = 3, TILE_SHAPES = 4 };
+// A batch kernel variant: tile shape + TILE_SHAPES * stack placement (0: traversal stacks in local
+// memory; 1: their first kSharedStackEntries entries in shared memory).
+constexpr int kSharedStackEntries = 16;
+constexpr int STACK_PLACEMENTS = 2;
+constexpr int BATCH_VARIANTS = TILE_SHAPES * STACK_PLACEMENTS;
+inline int variant_tile(int variant) { return variant % TILE_SHAPES; }
+inline int variant_stack(int variant) { return variant / TILE_SHAPES; }
 
 void launch_ssb(const SceneDev &S, const ViewDev &v, int4 *ssb, cudaStream_t st);
-int launch_batch(const BatchView *views, u32t n_views, u32t total_tiles, int tile_shape, u32t chunk, u32t grid_blocks,
+int launch_batch(const BatchView *views, u32t n_views, u32t total_tiles, int variant, u32t chunk, u32t grid_blocks,
                  u32t *tile_counter, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st);
-void tile_dims(int tile_shape, u32t &tw, u32t &th);
-int batch_blocks_per_sm(int tile_shape);
+void tile_dims(int variant, u32t &tw, u32t &th);
+int batch_blocks_per_sm(int variant);
 // Row-segment starts of the view's ray directions: (grid_h x ceil(grid_w / kSegment)) float3.
 void launch_ray_rows(const ViewDev &v, float *dirs, cudaStream_t st);
 inline size_t ray_rows_floats(const ViewDev &v) { return (size_t)v.grid_h * ((v.grid_w + kSegment - 1) / kSegment) * 3; }

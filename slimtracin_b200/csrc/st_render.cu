@@ -7,8 +7,8 @@
 namespace st {
 
 // ---- triangles and the BLAS walk: intersection/mesh.h ----------------------------------------
-template <bool CNT>
-__device__ bool hit_triangles(TState<CNT> &t, const SceneDev &S, u32t base, u32t n, bool any_hit) {   // mesh.h:5
+template <bool CNT, int SHS>
+__device__ bool hit_triangles(TState<CNT, SHS> &t, const SceneDev &S, u32t base, u32t n, bool any_hit) {   // mesh.h:5
     const RayD &ray = t.local;
     Hit &hit = t.current;
     Hit &closest = t.mesh_closest;
@@ -49,8 +49,8 @@ __device__ __forceinline__ NodePair load_pair(const NodePair *p) {
     return r;
 }
 
-template <bool CNT>
-__device__ __forceinline__ bool trace_mesh(TState<CNT> &t, const SceneDev &S, const MeshDev &M, bool any_hit) {   // mesh.h:38
+template <bool CNT, int SHS>
+__device__ __forceinline__ bool trace_mesh(TState<CNT, SHS> &t, const SceneDev &S, const MeshDev &M, bool any_hit) {   // mesh.h:38
     const RayD &ray = t.local;
     Hit &closest = t.mesh_closest;
     float ld, rd;
@@ -88,13 +88,13 @@ __device__ __forceinline__ bool trace_mesh(TState<CNT> &t, const SceneDev &S, co
                         pair = kNoPair;
                         continue;
                     }
-                    t.mesh_stack[sp++] = far_pair;
+                    t.push(true, sp++, far_pair);
                 }
                 pair = near_pair;
             } else if (rgo) {
                 pair = P.d.z;
             } else {
-                pair = sp ? t.mesh_stack[--sp] : kNoPair;
+                pair = sp ? t.at(true, --sp) : kNoPair;
             }
         }
         if (!leaves) break;
@@ -113,8 +113,8 @@ __device__ __forceinline__ bool trace_mesh(TState<CNT> &t, const SceneDev &S, co
 
 // ---- hitPrimitives intersection/primitives.h:9 ----------------------------------------------------
 // ids == nullptr: the candidates are primitives first..first+count-1 in index order.
-template <bool CNT>
-__device__ __forceinline__ bool hit_primitives(TState<CNT> &t, const SceneDev &S, const RayD &ray, const u32t *ids, u32t first,
+template <bool CNT, int SHS>
+__device__ __forceinline__ bool hit_primitives(TState<CNT, SHS> &t, const SceneDev &S, const RayD &ray, const u32t *ids, u32t first,
                                u32t count, bool any_hit, const int4 *ssb, int x, int y, float cone_angle) {
     Hit &hit = t.current, &closest = t.closest;
     bool found = false;
@@ -198,8 +198,8 @@ __device__ __forceinline__ bool hit_primitives(TState<CNT> &t, const SceneDev &S
 // inlined copy of the walk carries one copy of them (the instruction footprint of the megakernel).
 // all_prims: test every primitive in leaf-id order without the root box (the primary-ray path of
 // scenes with few primitives, raytracer.h:100).
-template <bool CNT>
-__device__ __forceinline__ bool trace_scene(TState<CNT> &t, const SceneDev &S, RayD &ray, bool any_hit, const int4 *ssb,
+template <bool CNT, int SHS>
+__device__ __forceinline__ bool trace_scene(TState<CNT, SHS> &t, const SceneDev &S, RayD &ray, bool any_hit, const int4 *ssb,
                                             int x, int y, float cone_angle, bool prepped, bool all_prims) {
     if (!prepped) {
         ray.rcp = rcp(ray.direction);
@@ -237,13 +237,13 @@ __device__ __forceinline__ bool trace_scene(TState<CNT> &t, const SceneDev &S, R
                         pair = kNoPair;
                         continue;
                     }
-                    t.scene_stack[sp++] = far_pair;
+                    t.push(false, sp++, far_pair);
                 }
                 pair = near_pair;
             } else if (rgo) {
                 pair = P.d.z;
             } else {
-                pair = sp ? t.scene_stack[--sp] : kNoPair;
+                pair = sp ? t.at(false, --sp) : kNoPair;
             }
         }
         if (!leaves) break;
@@ -260,8 +260,8 @@ __device__ __forceinline__ bool trace_scene(TState<CNT> &t, const SceneDev &S, R
 }
 
 // ---- closest_hit/surface.h, lights.h ------------------------------------------------------------
-template <bool CNT>
-__device__ v3 shade_from_lights(TState<CNT> &t, const SceneDev &S, Shaded &s, RayD &ray, v3 color) {   // surface.h:9
+template <bool CNT, int SHS>
+__device__ v3 shade_from_lights(TState<CNT, SHS> &t, const SceneDev &S, Shaded &s, RayD &ray, v3 color) {   // surface.h:9
     Hit &hit = t.closest;
     for (u32t i = 0; i < S.n_lights; i++) {
         const Light &light = S.lights[i];
@@ -282,8 +282,8 @@ __device__ v3 shade_from_lights(TState<CNT> &t, const SceneDev &S, Shaded &s, Ra
     return color;
 }
 
-template <bool CNT>
-__device__ bool shade_from_emissive_quads(TState<CNT> &t, const SceneDev &S, Shaded &s, RayD &ray, v3 &color) {  // surface.h:37
+template <bool CNT, int SHS>
+__device__ bool shade_from_emissive_quads(TState<CNT, SHS> &t, const SceneDev &S, Shaded &s, RayD &ray, v3 &color) {  // surface.h:37
     Hit &hit = t.current;
     bool found = false;
     for (u32t e = 0; e < S.n_emissive; e++) {
@@ -360,8 +360,8 @@ __device__ __forceinline__ float volume_density(const SphereHitD &h) {   // ligh
     return (h.c * t1 - h.b * t1 * t1 + t1 * t1 * t1 / 3.0f - (
             h.c * t2 - h.b * t2 * t2 + t2 * t2 * t2 / 3.0f)) * (3.0f / 4.0f);
 }
-template <bool CNT>
-__device__ bool shade_lights(TState<CNT> &t, const SceneDev &S, v3 Ro, v3 Rd, float max_distance, v3 &color) {  // lights.h:17
+template <bool CNT, int SHS>
+__device__ bool shade_lights(TState<CNT, SHS> &t, const SceneDev &S, v3 Ro, v3 Rd, float max_distance, v3 &color) {  // lights.h:17
     bool hit_light = false;
     SphereHitD &sh = t.sphere;
     sh.closest_distance = INFINITY;
@@ -381,8 +381,8 @@ __device__ bool shade_lights(TState<CNT> &t, const SceneDev &S, v3 Ro, v3 Rd, fl
     return hit_light;
 }
 
-template <bool CNT>
-__device__ __forceinline__ void apply_textures(TState<CNT> &t, const SceneDev &S, Shaded &s, Hit &hit, const Material &M,
+template <bool CNT, int SHS>
+__device__ __forceinline__ void apply_textures(TState<CNT, SHS> &t, const SceneDev &S, Shaded &s, Hit &hit, const Material &M,
                                                float &du, float &dv, bool first) {
     s.u = hit.u * M.uv_repeat.x;
     s.v = hit.v * M.uv_repeat.y;
@@ -511,8 +511,8 @@ __device__ __forceinline__ v3 grid_direction(const ViewDev &v, const float *seg,
 // rayTrace render/raytracer.h:81 for one QCAA grid point, writing the FloatPixel the reference's
 // setPixel leaves after beginDrawing's clear (viewport.h:88): hit -> (color, 1, z), miss ->
 // (black, 0, +inf).
-template <bool CNT>
-__device__ __forceinline__ void trace_point(TState<CNT> &t, const SceneDev &S, const ViewDev &v, const int4 *ssb,
+template <bool CNT, int SHS>
+__device__ __forceinline__ void trace_point(TState<CNT, SHS> &t, const SceneDev &S, const ViewDev &v, const int4 *ssb,
                                             const float *dirs, u32t x, u32t y, FloatPixel *out, u32t *prim_ids,
                                             FloatPixel *out_host = nullptr) {
     const size_t idx = (size_t)y * v.grid_w + x;
@@ -669,8 +669,8 @@ __device__ __forceinline__ void trace_point(TState<CNT> &t, const SceneDev &S, c
     }
 }
 
-template <bool CNT>
-__device__ __forceinline__ void flush_counters(TState<CNT> &t, unsigned *status, unsigned long long *counters) {
+template <bool CNT, int SHS>
+__device__ __forceinline__ void flush_counters(TState<CNT, SHS> &t, unsigned *status, unsigned long long *counters) {
     if (t.status) atomicOr(status, t.status);
     if (CNT) {
         const u32t lane = threadIdx.x & 31;
@@ -697,7 +697,7 @@ __global__ void ST_TRACE_BOUNDS trace_kernel(SceneDev S, ViewDev v, const int4 *
     // a block covers 16x8 grid points; each warp an 8x4 tile
     const u32t x = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
     const u32t y = blockIdx.y * 8 + (warp >> 1) * 4 + (lane >> 3);
-    TState<CNT> t;
+    TState<CNT, 0> t;
     t.status = 0;
     if (CNT) for (int k = 0; k < C_COUNT; k++) t.cnt[k] = 0;
     if (x < v.grid_w && y < v.grid_h) trace_point(t, S, v, ssb, dirs, x, y, out, prim_ids, out_host);
@@ -752,12 +752,14 @@ __global__ void pick_kernel(SceneDev S, ViewDev v, const int4 *ssb, int x, int y
 // Every view is cut into tiles of tile_w x tile_h grid points (one warp per tile when the tile has
 // 32 points); warps take tiles from one global counter, `chunk` tiles at a time, so views of
 // different sizes, scenes and bounce counts share the launch and no warp idles while work is left.
-template <bool CNT, int TW, int TH>
+template <bool CNT, int TW, int TH, int SHS>
 __global__ void ST_TRACE_BOUNDS batch_kernel(const BatchView *views, u32t n_views, u32t total_tiles, u32t chunk,
                                                     u32t *tile_counter, unsigned *status, unsigned long long *counters) {
     static_assert(TW * TH == 32, "one warp per tile");
     const u32t lane = threadIdx.x & 31;
-    TState<CNT> t;
+    __shared__ u32t stack_columns[SHS > 0 ? 2 * SHS * kTraceBlock : 1];
+    TState<CNT, SHS> t;
+    t.sh = stack_columns + threadIdx.x;
     t.status = 0;
     if (CNT) for (int k = 0; k < C_COUNT; k++) t.cnt[k] = 0;
     for (;;) {
@@ -818,31 +820,38 @@ void launch_trace(const SceneDev &S, const ViewDev &v, const int4 *ssb, const fl
     if (count) trace_kernel<true><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, out_host);
     else trace_kernel<false><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, out_host);
 }
-int launch_batch(const BatchView *views, u32t n_views, u32t total_tiles, int tile_shape, u32t chunk, u32t grid_blocks,
+int launch_batch(const BatchView *views, u32t n_views, u32t total_tiles, int variant, u32t chunk, u32t grid_blocks,
                  u32t *tile_counter, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st) {
-#define ST_BATCH(TW, TH) (count ? (batch_kernel<true, TW, TH><<<grid_blocks, 128, 0, st>>>(views, n_views, total_tiles, chunk, tile_counter, status, counters), 0) \
-                               : (batch_kernel<false, TW, TH><<<grid_blocks, 128, 0, st>>>(views, n_views, total_tiles, chunk, tile_counter, status, counters), 0))
-    switch (tile_shape) {
-        case TILE_8x4: return ST_BATCH(8, 4);
-        case TILE_16x2: return ST_BATCH(16, 2);
-        case TILE_32x1: return ST_BATCH(32, 1);
-        case TILE_4x8: return ST_BATCH(4, 8);
+#define ST_BATCH(TW, TH, SHS) (count ? (batch_kernel<true, TW, TH, SHS><<<grid_blocks, 128, 0, st>>>(views, n_views, total_tiles, chunk, tile_counter, status, counters), 0) \
+                                     : (batch_kernel<false, TW, TH, SHS><<<grid_blocks, 128, 0, st>>>(views, n_views, total_tiles, chunk, tile_counter, status, counters), 0))
+#define ST_BATCH_STACKS(TW, TH) (variant_stack(variant) ? ST_BATCH(TW, TH, kSharedStackEntries) : ST_BATCH(TW, TH, 0))
+    if (variant < 0 || variant >= BATCH_VARIANTS) return -1;
+    switch (variant_tile(variant)) {
+        case TILE_8x4: return ST_BATCH_STACKS(8, 4);
+        case TILE_16x2: return ST_BATCH_STACKS(16, 2);
+        case TILE_32x1: return ST_BATCH_STACKS(32, 1);
+        case TILE_4x8: return ST_BATCH_STACKS(4, 8);
     }
+#undef ST_BATCH_STACKS
 #undef ST_BATCH
     return -1;
 }
-int batch_blocks_per_sm(int tile_shape) {
+int batch_blocks_per_sm(int variant) {
     int n = 0;
-    switch (tile_shape) {
-        case TILE_16x2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<false, 16, 2>, 128, 0); break;
-        case TILE_32x1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<false, 32, 1>, 128, 0); break;
-        case TILE_4x8: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<false, 4, 8>, 128, 0); break;
-        default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<false, 8, 4>, 128, 0); break;
+#define ST_OCC(TW, TH) (variant_stack(variant) \
+        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<false, TW, TH, kSharedStackEntries>, 128, 0) \
+        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<false, TW, TH, 0>, 128, 0))
+    switch (variant_tile(variant)) {
+        case TILE_16x2: ST_OCC(16, 2); break;
+        case TILE_32x1: ST_OCC(32, 1); break;
+        case TILE_4x8: ST_OCC(4, 8); break;
+        default: ST_OCC(8, 4); break;
     }
+#undef ST_OCC
     return n > 0 ? n : 1;
 }
-void tile_dims(int tile_shape, u32t &tw, u32t &th) {
-    switch (tile_shape) {
+void tile_dims(int variant, u32t &tw, u32t &th) {
+    switch (variant_tile(variant)) {
         case TILE_16x2: tw = 16; th = 2; return;
         case TILE_32x1: tw = 32; th = 1; return;
         case TILE_4x8: tw = 4; th = 8; return;

@@ -36,7 +36,13 @@ struct RayD {                                       // Ray core/types.h:180
 
 struct SphereHitD { float b, c, t_near, t_far, furthest, closest_distance; };
 
-template <bool CNT>
+// Threads per block of the kernels that trace (the stride of the shared-memory stack columns).
+constexpr u32t kTraceBlock = 128;
+
+// SHS: entries of each traversal stack kept in shared memory (the block's stack columns, one per
+// thread, entry-major so that a warp's pushes hit distinct banks); the rest live in local memory.
+// Where the entries live changes no traversal step.
+template <bool CNT, int SHS = 0>
 struct TState {
     Hit closest, mesh_closest, current;
     SphereHitD sphere;
@@ -44,9 +50,19 @@ struct TState {
     u32t depth;
     unsigned status;
     unsigned cnt[CNT ? C_COUNT : 1];
-    u32t scene_stack[kStack];   // the TLAS walk (the reference's trace->scene_stack, trace.h:22)
-    u32t mesh_stack[kStack];    // the BLAS walk nested inside it (trace->mesh_stack, mesh.h:42)
+    u32t scene_local[kStack - SHS];   // the TLAS walk (the reference's trace->scene_stack, trace.h:22)
+    u32t mesh_local[kStack - SHS];    // the BLAS walk nested inside it (trace->mesh_stack, mesh.h:42)
+    u32t *sh;                         // SHS > 0: this thread's column, 2 * SHS entries kTraceBlock apart
     __device__ __forceinline__ void count(int k, unsigned n = 1) { if (CNT) cnt[k] += n; }
+    __device__ __forceinline__ void push(bool mesh, u32t i, u32t v) {
+        if (SHS > 0 && i < (u32t)SHS) sh[((mesh ? SHS : 0) + i) * kTraceBlock] = v;
+        else if (mesh) mesh_local[i - SHS] = v;
+        else scene_local[i - SHS] = v;
+    }
+    __device__ __forceinline__ u32t at(bool mesh, u32t i) const {
+        if (SHS > 0 && i < (u32t)SHS) return sh[((mesh ? SHS : 0) + i) * kTraceBlock];
+        return mesh ? mesh_local[i - SHS] : scene_local[i - SHS];
+    }
 };
 
 // A ray that does not move along an axis (a zero direction component, or one so small that
@@ -259,8 +275,8 @@ __device__ __forceinline__ float duv_ray_cone(float NdotV, float cone_width, flo
 }
 
 // ---- scene/texture.h ---------------------------------------------------------------------------
-template <bool CNT>
-__device__ v3 sample_texture(TState<CNT> &t, const SceneDev &S, u32t tex, float U0, float V0, float du, float dv) {
+template <bool CNT, int SHS>
+__device__ v3 sample_texture(TState<CNT, SHS> &t, const SceneDev &S, u32t tex, float U0, float V0, float du, float dv) {
     TexDev T = S.textures[tex];                                      // sampleTexture :32
     unsigned level = 0;
     if (T.mipmap) {
@@ -289,8 +305,8 @@ __device__ v3 sample_texture(TState<CNT> &t, const SceneDev &S, u32t tex, float 
              ST_CH(B, 3) * br + (ST_CH(B, 2) * bl + (ST_CH(B, 1) * tr + ST_CH(B, 0) * tl)));
 #undef ST_CH
 }
-template <bool CNT>
-__device__ __forceinline__ v3 sample_normal(TState<CNT> &t, const SceneDev &S, u32t tex, float u, float v, float du, float dv) {
+template <bool CNT, int SHS>
+__device__ __forceinline__ v3 sample_normal(TState<CNT, SHS> &t, const SceneDev &S, u32t tex, float u, float v, float du, float dv) {
     v3 n = sample_texture(t, S, tex, u, v, du, dv);                 // sampleNormal surface.h:131
     float y = n.z; n.z = n.y; n.y = y;
     return norm(vsfma(n, 2.0f, splat(-1.0f)));

@@ -133,7 +133,8 @@ class PerFrame:
 class Batch:
     """The same views in one st_render_batch call (device outputs, autotuned, CUDA graph)."""
 
-    def __init__(self, renderer, items, out_float_ptrs, out_u8_ptrs, use_graph=True, tile_shape=-1, chunk=0):
+    def __init__(self, renderer, items, out_float_ptrs, out_u8_ptrs, use_graph=True, tile_shape=-1, chunk=0,
+                 stack_placement=-1):
         self.r = renderer
         self.views = (api.st_view * len(items))()
         self.keep = items
@@ -144,6 +145,7 @@ class Batch:
         self.opt = api.st_batch_options()
         self.opt.device_outputs, self.opt.use_graph = 1, int(use_graph)
         self.opt.tile_shape, self.opt.chunk = tile_shape, chunk
+        self.opt.stack_placement = stack_placement
 
     def run(self):
         s = self.r.L.st_render_batch(self.r.ctx, self.views, len(self.views), C.byref(self.opt))

@@ -258,14 +258,19 @@ def test_batch_equals_per_frame_renders(renderer):
              (11, c0, cam0, 33, 17, 3, S.RM_DEPTH)]
     singles = [H.gpu_frame(renderer, slot, sd, cam, w, h, depth=d, mode=m) for slot, sd, cam, w, h, d, m in specs]
     for tile in (0, 1, 2, 3, -1):
-        for graph in (False, True, True):
-            frames = [scenes.Frame(w, h, cam, depth=d, mode=m) for slot, sd, cam, w, h, d, m in specs]
-            opt = api.render_batch(renderer, [(sp[0], sp[1], fr) for sp, fr in zip(specs, frames)],
-                                   tile_shape=tile, use_graph=graph)
-            for a, b in zip(frames, singles):
-                assert np.array_equal(a.float_pixels.view(np.uint8), b.float_pixels.view(np.uint8)), (tile, graph)
-                assert np.array_equal(a.pixels.view(np.uint8), b.pixels.view(np.uint8))
-            assert opt.rays == sum(fr.rays for fr in frames)
+        for stack in (0, 1, -1):
+            for graph in (False, True, True):
+                frames = [scenes.Frame(w, h, cam, depth=d, mode=m) for slot, sd, cam, w, h, d, m in specs]
+                opt = api.render_batch(renderer, [(sp[0], sp[1], fr) for sp, fr in zip(specs, frames)],
+                                       tile_shape=tile, use_graph=graph, stack_placement=stack)
+                for a, b in zip(frames, singles):
+                    assert np.array_equal(a.float_pixels.view(np.uint8), b.float_pixels.view(np.uint8)), (tile, stack, graph)
+                    assert np.array_equal(a.pixels.view(np.uint8), b.pixels.view(np.uint8))
+                assert opt.rays == sum(fr.rays for fr in frames)
+                if tile >= 0:
+                    assert opt.tile_shape_used == tile
+                if stack >= 0:
+                    assert opt.stack_placement_used == stack
 
 
 def test_pinned_host_outputs_written_by_the_kernels(renderer):
