@@ -72,11 +72,11 @@ DevBuf *motion_field(SceneSlot &S, MotionBufs &m, int k, DevBuf **mine) {
 
 struct BatchState {
     DevBuf table, ssb, seg, out_float, out_u8, counter;
-    BatchView *staging = nullptr;       // pinned host copy of the view table
+    BatchView *staging = nullptr;       // pinned host copy of the device view table
     size_t staging_cap = 0;
+    BatchTable host_table;              // the view table of the launch group being issued (a kernel parameter)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    std::string graph_key;
     std::map<std::string, std::pair<int, int>> tuned;   // scene-class key -> (kernel variant, chunk)
 };
 
@@ -1057,6 +1057,16 @@ struct BatchPlan {
     std::string shape_key, class_key;
 };
 
+// A view's tiles are numbered in 2x2 groups of warp tiles, so that the four warps of a block, which
+// fetch consecutive tiles, trace one compact region as the per-frame kernel's blocks do.  Sets
+// b.tiles_x (groups per row) and returns the number of tile slots (4 per group; slots of a group
+// that fall outside the view have no grid points).
+u32t view_tiles(BatchView &b, u32t tw, u32t th) {
+    const u32t tx = (b.view.grid_w + tw - 1) / tw, ty = (b.view.grid_h + th - 1) / th;
+    b.tiles_x = (tx + 1) / 2;
+    return 4 * b.tiles_x * ((ty + 1) / 2);
+}
+
 int plan_batch(st_ctx *ctx, const st_view *views, int n, int tile, const st_batch_options &o, BatchPlan &p) {
     u32t tw, th;
     tile_dims(tile, tw, th);
@@ -1073,10 +1083,8 @@ int plan_batch(st_ctx *ctx, const st_view *views, int n, int tile, const st_batc
         ST_TRY(make_view(V.viewport, b.view));
         b.view.primary_tlas = S->n_prims > 64 ? 1 : 0;
         b.scene = scene_view(*S, V.scene);
-        b.tiles_x = (b.view.grid_w + tw - 1) / tw;
-        const u32t tiles_y = (b.view.grid_h + th - 1) / th;
         b.tile_begin = p.total_tiles;
-        p.total_tiles += b.tiles_x * tiles_y;
+        p.total_tiles += view_tiles(b, tw, th);
         const size_t grid = (size_t)b.view.grid_w * b.view.grid_h;
         p.ssb_off.push_back(p.ssb_total);
         p.ssb_total += std::max(S->n_prims, 1u);
@@ -1107,6 +1115,44 @@ int plan_batch(st_ctx *ctx, const st_view *views, int n, int tile, const st_batc
     return ST_OK;
 }
 
+// A batch's launches, kTableViews views at a time: the views' SSBs and ray-row starts, the
+// persistent trace kernel over the group's tiles, and the resolves of the views that want a frame.
+// Every launch carries the group's view table as its kernel parameter.
+int launch_groups(st_ctx *ctx, BatchState &B, const BatchPlan &p, int tile, u32t chunk, unsigned *status,
+                  cudaStream_t st) {
+    const int n = (int)p.table.size();
+    const u32t blocks = (u32t)(ctx->sm_count * ctx->blocks_per_sm[tile]);
+    // the device copy of the table, tile numbers rebased per group, for the trace kernel
+    for (int i = 0; i < n; i++) {
+        B.staging[i] = p.table[i];
+        B.staging[i].tile_begin -= p.table[i - i % kTableViews].tile_begin;
+    }
+    ST_CUDA(cudaMemcpyAsync(B.table.ptr, B.staging, sizeof(BatchView) * n, cudaMemcpyHostToDevice, st));
+    for (int g0 = 0; g0 < n; g0 += kTableViews) {
+        const int gn = std::min(kTableViews, n - g0);
+        const u32t first = p.table[g0].tile_begin;
+        const u32t end = g0 + gn < n ? p.table[g0 + gn].tile_begin : p.total_tiles;
+        u32t max_prims = 0, max_rows = 0, max_w = 0, max_h = 0;
+        for (int i = 0; i < gn; i++) {
+            const BatchView &b = B.staging[g0 + i];
+            B.host_table.v[i] = b;
+            max_prims = std::max(max_prims, b.scene.n_prims);
+            max_rows = std::max(max_rows, b.view.grid_h);
+            if (b.out_u8) {
+                max_w = std::max(max_w, b.view.grid_w - 1);
+                max_h = std::max(max_h, b.view.grid_h - 1);
+            }
+        }
+        ST_CUDA(cudaMemsetAsync(B.counter.ptr, 0, 16, st));
+        launch_batch_setup(B.host_table, (u32t)gn, max_prims, max_rows, st);
+        if (launch_batch(P<BatchView>(B.table) + g0, (u32t)gn, end - first, tile, chunk, blocks, P<u32t>(B.counter),
+                         status, P<unsigned long long>(ctx->counters), false, st) != 0)
+            return ST_ERR_INVALID_ARG;
+        if (max_w) launch_batch_resolve(B.host_table, (u32t)gn, max_w, max_h, st);
+    }
+    return ST_CUDA_LAST();
+}
+
 int enqueue_batch(st_ctx *ctx, BatchState &B, unsigned *status, const st_view *views, int n, BatchPlan &p, int tile,
                   u32t chunk, cudaStream_t st, const st_batch_options &o) {
     // per-view pointers into the arena (or the caller's device outputs)
@@ -1116,43 +1162,34 @@ int enqueue_batch(st_ctx *ctx, BatchState &B, unsigned *status, const st_view *v
         b.dirs = P<float>(B.seg) + p.seg_off[i];
         b.out = (o.device_outputs && views[i].out_float) ? views[i].out_float : P<FloatPixel>(B.out_float) + p.float_off[i];
         b.prim_ids = nullptr;
+        b.out_u8 = !p.want_u8[i] ? nullptr
+                   : o.device_outputs ? reinterpret_cast<uint32_t *>(views[i].out_u8) : P<uint32_t>(B.out_u8) + p.u8_off[i];
     }
-    memcpy(B.staging, p.table.data(), sizeof(BatchView) * n);
-    ST_CUDA(cudaMemcpyAsync(B.table.ptr, B.staging, sizeof(BatchView) * n, cudaMemcpyHostToDevice, st));
-    ST_CUDA(cudaMemsetAsync(B.counter.ptr, 0, 16, st));
     ST_CUDA(cudaMemsetAsync(status, 0, 16, st));
-    for (int i = 0; i < n; i++) {
-        BatchView &b = p.table[i];
-        launch_ssb(b.scene, b.view, const_cast<int4 *>(b.ssb), st);
-        launch_ray_rows(b.view, const_cast<float *>(b.dirs), st);
+    return launch_groups(ctx, B, p, tile, chunk, status, st);
+}
+
+// Device and pinned room for n views' table (grown geometrically: cudaFreeHost waits for the device).
+int table_reserve(st_ctx *ctx, BatchState &B, int n) {
+    ST_TRY(reserve(ctx, B.table, sizeof(BatchView) * n));
+    if (B.staging_cap < (size_t)n) {
+        const size_t cap = std::max((size_t)n, 2 * B.staging_cap);
+        if (B.staging) cudaFreeHost(B.staging);
+        B.staging = nullptr;
+        B.staging_cap = 0;
+        ST_CUDA(cudaMallocHost((void **)&B.staging, sizeof(BatchView) * cap));
+        B.staging_cap = cap;
     }
-    const u32t blocks = (u32t)(ctx->sm_count * ctx->blocks_per_sm[tile]);
-    if (launch_batch(P<BatchView>(B.table), (u32t)n, p.total_tiles, tile, chunk, blocks, P<u32t>(B.counter),
-                     status, P<unsigned long long>(ctx->counters), false, st) != 0)
-        return ST_ERR_INVALID_ARG;
-    for (int i = 0; i < n; i++) {
-        if (!p.want_u8[i]) continue;
-        const BatchView &b = p.table[i];
-        uint32_t *u8 = o.device_outputs ? reinterpret_cast<uint32_t *>(views[i].out_u8) : P<uint32_t>(B.out_u8) + p.u8_off[i];
-        launch_resolve(b.out, b.view.grid_w, b.view.grid_w - 1, b.view.grid_h - 1, u8, st);
-    }
-    return ST_CUDA_LAST();
+    return ST_OK;
 }
 
 int batch_reserve(st_ctx *ctx, BatchState &B, const BatchPlan &p, int n) {
-    ST_TRY(reserve(ctx, B.table, sizeof(BatchView) * n));
+    ST_TRY(table_reserve(ctx, B, n));
     ST_TRY(reserve(ctx, B.ssb, sizeof(int4) * p.ssb_total));
     ST_TRY(reserve(ctx, B.seg, sizeof(float) * p.seg_total));
     ST_TRY(reserve(ctx, B.out_float, sizeof(FloatPixel) * std::max(p.float_total, (size_t)1)));
     ST_TRY(reserve(ctx, B.out_u8, sizeof(uint32_t) * std::max(p.u8_total, (size_t)1)));
     ST_TRY(reserve(ctx, B.counter, 16));
-    if (B.staging_cap < (size_t)n) {
-        if (B.staging) cudaFreeHost(B.staging);
-        B.staging = nullptr;
-        B.staging_cap = 0;
-        ST_CUDA(cudaMallocHost((void **)&B.staging, sizeof(BatchView) * n));
-        B.staging_cap = n;
-    }
     return ST_OK;
 }
 
@@ -1224,34 +1261,30 @@ int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *
     o.graph_replayed = 0;
     ST_CUDA(cudaEventRecord(ctx->ev[0], st));
     if (o.use_graph) {
-        std::ostringstream key;
-        key << p.shape_key << "c" << chunk << "s" << (const void *)st;
-        if (B.exec && B.graph_key == key.str()) {
-            // same shape: refresh the view table the graph's copy node reads, then replay
-            for (int i = 0; i < n; i++) {
-                BatchView &b = p.table[i];
-                b.ssb = P<int4>(B.ssb) + p.ssb_off[i];
-                b.dirs = P<float>(B.seg) + p.seg_off[i];
-                b.out = (o.device_outputs && views[i].out_float) ? views[i].out_float : P<FloatPixel>(B.out_float) + p.float_off[i];
-                b.prim_ids = nullptr;
+        // The batch's launches are captured; an instantiated graph of the same topology (the same
+        // view groups and views wanting frames) is updated in place from the capture, so every kernel
+        // parameter - view tables, cameras, arena and output pointers - is this call's.
+        ST_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        int s = enqueue_batch(ctx, B, P<unsigned>(ctx->status), views, n, p, tile, chunk, st, o);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (s != ST_OK) { if (g) cudaGraphDestroy(g); return s; }
+        if (e != cudaSuccess) return fail_cuda(ctx, e);
+        bool updated = false;
+        if (B.exec) {
+            cudaGraphExecUpdateResultInfo info;
+            updated = cudaGraphExecUpdate(B.exec, g, &info) == cudaSuccess;
+            if (!updated) {
+                cudaGetLastError();
+                cudaGraphExecDestroy(B.exec);
+                B.exec = nullptr;
             }
-            memcpy(B.staging, p.table.data(), sizeof(BatchView) * n);
-            ST_CUDA(cudaGraphLaunch(B.exec, st));
-            o.graph_replayed = 1;
-        } else {
-            if (B.exec) { cudaGraphExecDestroy(B.exec); B.exec = nullptr; }
-            if (B.graph) { cudaGraphDestroy(B.graph); B.graph = nullptr; }
-            ST_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            int s = enqueue_batch(ctx, B, P<unsigned>(ctx->status), views, n, p, tile, chunk, st, o);
-            cudaGraph_t g = nullptr;
-            cudaError_t e = cudaStreamEndCapture(st, &g);
-            if (s != ST_OK) { if (g) cudaGraphDestroy(g); return s; }
-            if (e != cudaSuccess) return fail_cuda(ctx, e);
-            B.graph = g;
-            ST_CUDA(cudaGraphInstantiate(&B.exec, g, 0));
-            B.graph_key = key.str();
-            ST_CUDA(cudaGraphLaunch(B.exec, st));
         }
+        if (B.graph) cudaGraphDestroy(B.graph);
+        B.graph = g;
+        if (!B.exec) ST_CUDA(cudaGraphInstantiate(&B.exec, g, 0));
+        ST_CUDA(cudaGraphLaunch(B.exec, st));
+        o.graph_replayed = updated ? 1 : 0;
     } else {
         ST_TRY(enqueue_batch(ctx, B, P<unsigned>(ctx->status), views, n, p, tile, chunk, st, o));
     }
@@ -1587,35 +1620,23 @@ int enqueue_flight(st_ctx *ctx, InFlight &F, BatchPlan &p, std::vector<std::shar
     cudaStream_t st = F.stream;
     for (int i = 0; i < n; i++) {
         BatchView &b = p.table[i];
-        b.out = reinterpret_cast<FloatPixel *>(arena + reqs[i]->dev_float);
-        b.ssb = reinterpret_cast<int4 *>(arena + reqs[i]->dev_ssb);
-        b.dirs = reinterpret_cast<float *>(arena + reqs[i]->dev_seg);
+        const ServeReq &r = *reqs[i];
+        b.out = reinterpret_cast<FloatPixel *>(arena + r.dev_float);
+        b.ssb = reinterpret_cast<int4 *>(arena + r.dev_ssb);
+        b.dirs = reinterpret_cast<float *>(arena + r.dev_seg);
         b.prim_ids = nullptr;
+        // page-locked frames are written by the resolve kernel itself; others go through the arena
+        b.out_u8 = !r.out_u8 ? nullptr : r.mapped_u8 ? r.mapped_u8 : reinterpret_cast<uint32_t *>(arena + r.dev_u8);
     }
-    memcpy(F.B.staging, p.table.data(), sizeof(BatchView) * n);
-    ST_CUDA(cudaMemcpyAsync(F.B.table.ptr, F.B.staging, sizeof(BatchView) * n, cudaMemcpyHostToDevice, st));
-    ST_CUDA(cudaMemsetAsync(F.B.counter.ptr, 0, 16, st));
     ST_CUDA(cudaMemsetAsync(F.status.ptr, 0, 16, st));
-    for (int i = 0; i < n; i++) {
-        launch_ssb(p.table[i].scene, p.table[i].view, const_cast<int4 *>(p.table[i].ssb), st);
-        launch_ray_rows(p.table[i].view, const_cast<float *>(p.table[i].dirs), st);
-    }
-    const u32t blocks = (u32t)(ctx->sm_count * ctx->blocks_per_sm[tile]);
-    if (launch_batch(P<BatchView>(F.B.table), (u32t)n, p.total_tiles, tile, chunk, blocks, P<u32t>(F.B.counter),
-                     P<unsigned>(F.status), P<unsigned long long>(ctx->counters), false, st) != 0)
-        return ST_ERR_INVALID_ARG;
+    ST_TRY(launch_groups(ctx, F.B, p, tile, chunk, P<unsigned>(F.status), st));
     for (int i = 0; i < n; i++) {
         const ServeReq &r = *reqs[i];
         const BatchView &b = p.table[i];
         const size_t grid = (size_t)b.view.grid_w * b.view.grid_h;
-        if (r.out_u8 && r.mapped_u8) {            // page-locked: the resolve kernel writes the host frame
-            launch_resolve(b.out, b.view.grid_w, b.view.grid_w - 1, b.view.grid_h - 1, r.mapped_u8, st);
-        } else if (r.out_u8) {
-            uint32_t *u8 = reinterpret_cast<uint32_t *>(arena + r.dev_u8);
-            launch_resolve(b.out, b.view.grid_w, b.view.grid_w - 1, b.view.grid_h - 1, u8, st);
-            ST_CUDA(cudaMemcpyAsync(F.pinned + r.host_u8, u8, (size_t)(b.view.grid_w - 1) * (b.view.grid_h - 1) * 4,
+        if (r.out_u8 && !r.mapped_u8)
+            ST_CUDA(cudaMemcpyAsync(F.pinned + r.host_u8, b.out_u8, (size_t)(b.view.grid_w - 1) * (b.view.grid_h - 1) * 4,
                                     cudaMemcpyDeviceToHost, st));
-        }
         if (r.out_float)
             ST_CUDA(cudaMemcpyAsync(r.pinned_float ? reinterpret_cast<char *>(r.out_float) : F.pinned + r.host_float, b.out,
                                     sizeof(FloatPixel) * grid, cudaMemcpyDeviceToHost, st));
@@ -1682,9 +1703,8 @@ int launch_flight(st_ctx *ctx, int f, std::vector<std::shared_ptr<ServeReq>> &re
             b.scene.lights = r->lights_present ? P<Light>(S->lights) : nullptr;
             b.scene.n_lights = r->lights_present ? S->n_lights : 0;
         }
-        b.tiles_x = (b.view.grid_w + tw - 1) / tw;
         b.tile_begin = p.total_tiles;
-        p.total_tiles += b.tiles_x * ((b.view.grid_h + th - 1) / th);
+        p.total_tiles += view_tiles(b, tw, th);
         const size_t grid = (size_t)b.view.grid_w * b.view.grid_h;
         r->dev_float = dev; dev += align256(sizeof(FloatPixel) * grid);
         r->dev_ssb = dev; dev += align256(sizeof(int4) * std::max(S->n_prims, 1u));
@@ -1713,16 +1733,8 @@ int launch_flight(st_ctx *ctx, int f, std::vector<std::shared_ptr<ServeReq>> &re
         ST_CUDA(cudaMallocHost((void **)&F.pinned, cap));
         F.pinned_cap = cap;
     }
-    ST_TRY(reserve(ctx, F.B.table, sizeof(BatchView) * n));
     ST_TRY(reserve(ctx, F.B.counter, 16));
-    if (F.B.staging_cap < (size_t)n) {
-        const size_t cap = std::max((size_t)n, (size_t)std::max(V.cfg.max_views_per_batch, 1));
-        if (F.B.staging) cudaFreeHost(F.B.staging);
-        F.B.staging = nullptr;
-        F.B.staging_cap = 0;
-        ST_CUDA(cudaMallocHost((void **)&F.B.staging, sizeof(BatchView) * cap));
-        F.B.staging_cap = cap;
-    }
+    ST_TRY(table_reserve(ctx, F.B, std::max(n, V.cfg.max_views_per_batch)));
     cudaStream_t st = F.stream;
     char *arena = nullptr;
     ST_CUDA(cudaMallocFromPoolAsync((void **)&arena, std::max(dev, (size_t)256), V.pool, st));

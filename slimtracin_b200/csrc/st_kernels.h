@@ -33,8 +33,17 @@ struct BatchView {
     const float *dirs;             // row-segment starts (row_segments_kernel)
     FloatPixel *out;
     u32t *prim_ids;
-    u32t tile_begin, tiles_x;
+    uint32_t *out_u8;              // resolved frame (device), or null
+    u32t tile_begin, tiles_x;      // first tile slot; 2x2 groups of warp tiles per row
 };
+// A batch's views as a kernel parameter of its set-up and resolve kernels: one launch group takes at
+// most kTableViews views.  (The trace kernel reads the same views from device memory: indexed by a
+// tile's view, kernel-parameter memory measured slower there than an L1-cached table.)
+constexpr int kTableViews = 64;
+struct BatchTable {
+    BatchView v[kTableViews];
+};
+static_assert(sizeof(BatchTable) + 64 <= 32764, "kernel parameters are limited to 32764 bytes");
 enum TileShape { TILE_8x4 = 0, TILE_16x2 = 1, TILE_32x1 = 2, TILE_4x8 = 3, TILE_SHAPES = 4 };
 // A batch kernel variant: tile shape + TILE_SHAPES * stack placement (0: traversal stacks in local
 // memory; 1: their first kSharedStackEntries entries in shared memory).
@@ -65,6 +74,9 @@ struct PickDev {
 };
 void launch_pick(const SceneDev &S, const ViewDev &v, const int4 *ssb, int x, int y, PickDev *out, cudaStream_t st);
 void launch_resolve(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out, cudaStream_t st);
+// A batch's SSBs and ray-row starts (every view of the table), and its resolves (views with out_u8).
+void launch_batch_setup(const BatchTable &T, u32t n_views, u32t max_prims, u32t max_rows, cudaStream_t st);
+void launch_batch_resolve(const BatchTable &T, u32t n_views, u32t max_width, u32t max_height, cudaStream_t st);
 
 // ---- BVH builds (st_bvh.cu) ----
 // Device scratch the LBVH build needs for n items (allocated once per context and grown).

@@ -449,10 +449,8 @@ __device__ bool compute_ssb(int4 &b, v3 pos, float r, float fl, const ViewDev &v
     return false;
 }
 
-// updatePrimitiveSSB render/SSB.h:137 for every primitive of one view
-__global__ void ssb_kernel(SceneDev S, ViewDev v, int4 *ssb) {
-    u32t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= S.n_prims) return;
+// updatePrimitiveSSB render/SSB.h:137 for primitive i of one view
+__device__ __forceinline__ void ssb_one(const SceneDev &S, const ViewDev &v, int4 *ssb, u32t i) {
     const Primitive p = S.prims_raw[i];
     v3 view = vmat3(from(p.position) - v.cam_pos, v.cam_rot_matrix_inv);
     float radius;
@@ -479,15 +477,17 @@ __global__ void ssb_kernel(SceneDev S, ViewDev v, int4 *ssb) {
     bool vis = compute_ssb(b, view, radius, v.focal_length, v);
     ssb[i] = vis ? b : make_int4(1, 1, 0, 0);
 }
+__global__ void ssb_kernel(SceneDev S, ViewDev v, int4 *ssb) {
+    const u32t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < S.n_prims) ssb_one(S, v, ssb, i);
+}
 
 // The reference walks each row of the QCAA grid by repeated addition (raytracer.h:156-170):
 // row y starts at start + down added y times, pixel x at that plus right added x times.  That
 // sequence is kept exactly: one thread per row walks it and stores every kSegment-th value
 // ("segment starts", 3 MB at 1080p instead of a 25 MB direction table); the trace kernel adds
 // `right` the remaining x % kSegment times itself.
-__global__ void row_segments_kernel(ViewDev v, float *seg) {
-    const u32t row = blockIdx.x * blockDim.x + threadIdx.x;
-    if (row >= v.grid_h) return;
+__device__ __forceinline__ void row_segments_one(const ViewDev &v, float *seg, u32t row) {
     v3 cur = v.pp_start;
     for (u32t y = 0; y < row; y++) cur = cur + v.pp_down;
     const u32t nseg = (v.grid_w + kSegment - 1) / kSegment;
@@ -498,6 +498,10 @@ __global__ void row_segments_kernel(ViewDev v, float *seg) {
         out[3 * k + 2] = cur.z;
         for (int i = 0; i < kSegment; i++) cur = cur + v.pp_right;
     }
+}
+__global__ void row_segments_kernel(ViewDev v, float *seg) {
+    const u32t row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row < v.grid_h) row_segments_one(v, seg, row);
 }
 
 __device__ __forceinline__ v3 grid_direction(const ViewDev &v, const float *seg, u32t x, u32t y) {
@@ -774,7 +778,8 @@ __global__ void ST_TRACE_BOUNDS batch_kernel(const BatchView *views, u32t n_view
             while (vi + 1 < n_views && views[vi + 1].tile_begin <= tile) vi++;
             const BatchView &B = views[vi];
             const u32t local = tile - B.tile_begin;
-            const u32t tx = local % B.tiles_x, ty = local / B.tiles_x;
+            const u32t group = local >> 2, q = local & 3;    // 2x2 groups of warp tiles
+            const u32t tx = 2 * (group % B.tiles_x) + (q & 1), ty = 2 * (group / B.tiles_x) + (q >> 1);
             const u32t x = tx * TW + (lane % TW), y = ty * TH + (lane / TW);
             if (x < B.view.grid_w && y < B.view.grid_h)
                 trace_point(t, B.scene, B.view, B.ssb, B.dirs, x, y, B.out, B.prim_ids);
@@ -785,9 +790,7 @@ __global__ void ST_TRACE_BOUNDS batch_kernel(const BatchView *views, u32t n_view
 
 // drawViewportToWindowContent viewport/viewport.h:12 (QCAA branch): the 2x2 corners' colour times
 // opacity, averaged, square-rooted in double, truncated to u8; all-infinite corners -> background.
-__global__ void resolve_kernel(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out) {
-    u32t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= width || y >= height) return;
+__device__ __forceinline__ void resolve_one(const FloatPixel *in, u32t grid_w, u32t width, uint32_t *out, u32t x, u32t y) {
     const FloatPixel TL = in[(size_t)y * grid_w + x], TR = in[(size_t)y * grid_w + x + 1];
     const FloatPixel BL = in[(size_t)(y + 1) * grid_w + x], BR = in[(size_t)(y + 1) * grid_w + x + 1];
     uint32_t px;
@@ -802,6 +805,31 @@ __global__ void resolve_kernel(const FloatPixel *in, u32t grid_w, u32t width, u3
         px = B | (G << 8) | (R << 16) | 0xFF000000u;
     }
     out[(size_t)y * width + x] = px;
+}
+__global__ void resolve_kernel(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out) {
+    const u32t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x < width && y < height) resolve_one(in, grid_w, width, out, x, y);
+}
+
+// ---- a batch's per-view set-up and resolve, driven by the view table (one launch each) ----------
+__global__ void batch_ssb_kernel(const BatchTable T, u32t n_views) {
+    const u32t vi = blockIdx.y, i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (vi >= n_views) return;
+    const BatchView &B = T.v[vi];
+    if (i < B.scene.n_prims) ssb_one(B.scene, B.view, const_cast<int4 *>(B.ssb), i);
+}
+__global__ void batch_rows_kernel(const BatchTable T, u32t n_views) {
+    const u32t vi = blockIdx.y, row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (vi >= n_views) return;
+    const BatchView &B = T.v[vi];
+    if (row < B.view.grid_h) row_segments_one(B.view, const_cast<float *>(B.dirs), row);
+}
+__global__ void batch_resolve_kernel(const BatchTable T, u32t n_views) {
+    const u32t vi = blockIdx.z, x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (vi >= n_views) return;
+    const BatchView &B = T.v[vi];
+    if (B.out_u8 && x + 1 < B.view.grid_w && y + 1 < B.view.grid_h)
+        resolve_one(B.out, B.view.grid_w, B.view.grid_w - 1, B.out_u8, x, y);
 }
 
 #ifndef ST_HOST_EMU
@@ -860,6 +888,13 @@ void tile_dims(int variant, u32t &tw, u32t &th) {
 }
 void launch_pick(const SceneDev &S, const ViewDev &v, const int4 *ssb, int x, int y, PickDev *out, cudaStream_t st) {
     pick_kernel<<<1, 32, 0, st>>>(S, v, ssb, x, y, out);
+}
+void launch_batch_setup(const BatchTable &T, u32t n_views, u32t max_prims, u32t max_rows, cudaStream_t st) {
+    if (max_prims) batch_ssb_kernel<<<dim3((max_prims + 127) / 128, n_views), 128, 0, st>>>(T, n_views);
+    batch_rows_kernel<<<dim3((max_rows + 63) / 64, n_views), 64, 0, st>>>(T, n_views);
+}
+void launch_batch_resolve(const BatchTable &T, u32t n_views, u32t max_width, u32t max_height, cudaStream_t st) {
+    batch_resolve_kernel<<<dim3((max_width + 127) / 128, max_height, n_views), 128, 0, st>>>(T, n_views);
 }
 void launch_resolve(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out, cudaStream_t st) {
     dim3 grid((width + 127) / 128, height);

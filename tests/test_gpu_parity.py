@@ -362,3 +362,46 @@ def test_render_scene_draws_overlays_from_viewport_settings(renderer):
     assert renderer.L.st_render_scene(renderer.ctx, 4, C.byref(sc), C.byref(fr.viewport)) == 0
     assert fr.float_pixels.tobytes() == a.float_pixels.tobytes()
     assert np.array_equal(fr.pixels, a.pixels)
+
+
+def test_graph_replay_follows_new_views(renderer):
+    """A batch replayed through its CUDA graph with the same shapes but other cameras renders the
+    new views: every launch parameter (view tables, cameras, outputs) comes from the call."""
+    c0, cam0 = scenes.config0()
+    H.tlas_sah(c0)
+    renderer.upload(13, c0, tlas="host")
+    c1, cam1 = H.small_config1(subdivisions=3, texture_size=64, blas="orc")
+    H.tlas_sah(c1)
+    renderer.upload(14, c1, tlas="host")
+    rng = np.random.default_rng(5)
+    for step in range(3):
+        specs = [(13, c0, scenes.look_at((rng.uniform(-12, 12), rng.uniform(-2, 6), -15.0), (0, 0, 0)), 96, 64, 2),
+                 (14, c1, scenes.look_at((rng.uniform(-10, 10), rng.uniform(1, 6), -14.0), (0, 1.5, 0)), 120, 80, 4)]
+        singles = [H.gpu_frame(renderer, slot, sd, cam, w, h, depth=d) for slot, sd, cam, w, h, d in specs]
+        frames = [scenes.Frame(w, h, cam, depth=d) for slot, sd, cam, w, h, d in specs]
+        opt = api.render_batch(renderer, [(sp[0], sp[1], fr) for sp, fr in zip(specs, frames)], tile_shape=0,
+                               stack_placement=0, chunk=1, use_graph=True)
+        assert opt.graph_replayed == (1 if step else opt.graph_replayed)
+        for a, b in zip(frames, singles):
+            assert np.array_equal(a.float_pixels.view(np.uint8), b.float_pixels.view(np.uint8)), step
+            assert np.array_equal(a.pixels.view(np.uint8), b.pixels.view(np.uint8)), step
+
+
+def test_batch_larger_than_one_view_table(renderer):
+    """More views than one launch's view table holds (64): the batch runs as several launches and
+    every view equals its single render."""
+    c0, cam0 = scenes.config0()
+    H.tlas_sah(c0)
+    renderer.upload(15, c0, tlas="host")
+    rng = np.random.default_rng(9)
+    specs = []
+    for k in range(70):
+        cam = scenes.look_at((rng.uniform(-12, 12), rng.uniform(-2, 6), -15.0), (0, 0, 0))
+        specs.append((15, c0, cam, int(rng.integers(8, 40)), int(rng.integers(8, 30)), int(rng.integers(1, 4))))
+    singles = [H.gpu_frame(renderer, slot, sd, cam, w, h, depth=d) for slot, sd, cam, w, h, d in specs]
+    frames = [scenes.Frame(w, h, cam, depth=d) for slot, sd, cam, w, h, d in specs]
+    opt = api.render_batch(renderer, [(sp[0], sp[1], fr) for sp, fr in zip(specs, frames)], use_graph=False)
+    assert opt.rays == sum(fr.rays for fr in frames)
+    for a, b in zip(frames, singles):
+        assert np.array_equal(a.float_pixels.view(np.uint8), b.float_pixels.view(np.uint8))
+        assert np.array_equal(a.pixels.view(np.uint8), b.pixels.view(np.uint8))
