@@ -189,10 +189,11 @@ typedef struct st_batch_options {
     int device_outputs;         /* 1: out_* are device pointers */
     int tile_shape;             /* -1: autotuned; 0: 8x4, 1: 16x2, 2: 32x1, 3: 4x8 grid points per warp */
     int chunk;                  /* tiles a warp takes per queue fetch; 0: autotuned */
-    int use_graph;              /* 1: replay a captured CUDA graph while the batch's shape is unchanged */
+    int use_graph;              /* 1: launch through a CUDA graph: the batch's launches are captured and an
+                                   instantiated graph of the same topology is updated in place */
     float batch_ms;             /* out: CUDA-event time of the batch on the launch stream */
     uint64_t rays;              /* out: primary rays traced */
-    int tile_shape_used, chunk_used, graph_replayed;   /* out */
+    int tile_shape_used, chunk_used, graph_replayed;   /* out; graph_replayed: an existing graph was updated */
     int stack_placement;        /* -1: autotuned; 0: traversal stacks in local memory; 1: their first 16
                                    entries in shared memory (the traversal is the same either way) */
     int stack_placement_used;   /* out */
