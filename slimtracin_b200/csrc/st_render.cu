@@ -515,10 +515,13 @@ __device__ __forceinline__ v3 grid_direction(const ViewDev &v, const float *seg,
 // rayTrace render/raytracer.h:81 for one QCAA grid point, writing the FloatPixel the reference's
 // setPixel leaves after beginDrawing's clear (viewport.h:88): hit -> (color, 1, z), miss ->
 // (black, 0, +inf).
+// ret_c / ret_d (optional): the point's FloatPixel (colour and opacity, depth) is returned there
+// instead of being written to out / out_host.
 template <bool CNT, int SHS>
 __device__ __forceinline__ void trace_point(TState<CNT, SHS> &t, const SceneDev &S, const ViewDev &v, const int4 *ssb,
                                             const float *dirs, u32t x, u32t y, FloatPixel *out, u32t *prim_ids,
-                                            FloatPixel *out_host = nullptr) {
+                                            FloatPixel *out_host = nullptr, float4 *ret_c = nullptr,
+                                            double *ret_d = nullptr) {
     const size_t idx = (size_t)y * v.grid_w + x;
     v3 current = grid_direction(v, dirs, x, y);
     RayD ray;
@@ -661,6 +664,11 @@ __device__ __forceinline__ void trace_point(TState<CNT, SHS> &t, const SceneDev 
         c01 = make_float4(0, 0, 0, 0);
         depth = (double)INFINITY;
     }
+    if (ret_c) {
+        *ret_c = c01;
+        *ret_d = depth;
+        return;
+    }
     float2 *o = reinterpret_cast<float2 *>(out + idx);
     o[0] = make_float2(c01.x, c01.y);
     o[1] = make_float2(c01.z, c01.w);
@@ -704,7 +712,44 @@ __global__ void ST_TRACE_BOUNDS trace_kernel(SceneDev S, ViewDev v, const int4 *
     TState<CNT, 0> t;
     t.status = 0;
     if (CNT) for (int k = 0; k < C_COUNT; k++) t.cnt[k] = 0;
-    if (x < v.grid_w && y < v.grid_h) trace_point(t, S, v, ssb, dirs, x, y, out, prim_ids, out_host);
+    const bool active = x < v.grid_w && y < v.grid_h;
+    float4 c = make_float4(0, 0, 0, 0);
+    double d = 0;
+    if (active) trace_point(t, S, v, ssb, dirs, x, y, out, prim_ids, out_host, &c, &d);
+    if (active) {
+        const size_t idx = (size_t)y * v.grid_w + x;
+        float2 *o = reinterpret_cast<float2 *>(out + idx);
+        o[0] = make_float2(c.x, c.y);
+        o[1] = make_float2(c.z, c.w);
+        reinterpret_cast<double *>(o)[2] = d;
+    }
+    // A page-locked host copy is written over the bus as the frame is traced.  The warp's 8x4
+    // FloatPixels go out as contiguous 8-byte runs, each store instruction covering 256 bytes of
+    // whole grid rows instead of one 8-byte part of 32 pixels 24 bytes apart, so that the bus
+    // writes carry full lines.
+    if (out_host) {
+        const u32t x0 = x - (lane & 7), y0 = y - (lane >> 3);
+        if (x0 + 8 <= v.grid_w && y0 + 4 <= v.grid_h) {          // warp-uniform: the whole tile is inside
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const u32t chunk = 32 * k + lane, row = chunk / 24, j = chunk % 24, src = row * 8 + j / 3, part = j % 3;
+                const float a0 = __shfl_sync(0xFFFFFFFFu, c.x, src), a1 = __shfl_sync(0xFFFFFFFFu, c.y, src);
+                const float b0 = __shfl_sync(0xFFFFFFFFu, c.z, src), b1 = __shfl_sync(0xFFFFFFFFu, c.w, src);
+                const double dd = __shfl_sync(0xFFFFFFFFu, d, src);
+                const unsigned long long bits =
+                    part == 0 ? ((unsigned long long)__float_as_uint(a1) << 32) | __float_as_uint(a0)
+                    : part == 1 ? ((unsigned long long)__float_as_uint(b1) << 32) | __float_as_uint(b0)
+                                : (unsigned long long)__double_as_longlong(dd);
+                const size_t byte = ((size_t)(y0 + row) * v.grid_w + x0) * sizeof(FloatPixel) + 8 * j;
+                *reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(out_host) + byte) = bits;
+            }
+        } else if (active) {
+            float2 *h = reinterpret_cast<float2 *>(out_host + (size_t)y * v.grid_w + x);
+            h[0] = make_float2(c.x, c.y);
+            h[1] = make_float2(c.z, c.w);
+            reinterpret_cast<double *>(h)[2] = d;
+        }
+    }
     flush_counters(t, status, counters);
 }
 
