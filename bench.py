@@ -238,7 +238,7 @@ def mixed_workloads(r, big_sd, stream, rates):
                "per_frame_ms": pf_ms, "batch_ms": b_ms,
                "per_frame_mrays_s": rays / pf_ms / 1e3, "batch_mrays_s": rays / b_ms / 1e3,
                "speedup": pf_ms / b_ms, "tile_shape": batch.opt.tile_shape_used,
-               "stack_placement": batch.opt.stack_placement_used,
+               "stack_placement": batch.opt.stack_placement_used, "launch_mode": batch.opt.launch_mode_used,
                "chunk": batch.opt.chunk_used, "graph_replayed": batch.opt.graph_replayed}
     del fbuf, ubuf, one_f, one_u
     served = []

@@ -197,6 +197,9 @@ typedef struct st_batch_options {
     int stack_placement;        /* -1: autotuned; 0: traversal stacks in local memory; 1: their first 16
                                    entries in shared memory (the traversal is the same either way) */
     int stack_placement_used;   /* out */
+    int launch_mode;            /* -1: autotuned; 0: one persistent kernel over a shared tile queue; 1: one
+                                   trace kernel per view, the views on concurrent streams */
+    int launch_mode_used;       /* out (with launch mode 1, tile_shape_used and stack_placement_used are -1) */
 } st_batch_options;
 
 /* Render `view_count` views (different sizes, scenes, render modes and bounce counts) with one
@@ -256,6 +259,8 @@ typedef struct st_serve_config {
     int tile_shape, chunk;      /* -1 / 0: the autotuned choice for the scene class, else 8x4 and 1 */
     double refit_fraction;      /* primitives moved since the scene's last full TLAS build, as a fraction of
                                    all, below which the TLAS is refit, else rebuilt (LBVH30); 0 -> 0.25 */
+    int launch_mode;            /* 0: one trace kernel per view on concurrent streams; 1: one persistent
+                                   kernel over a shared tile queue (tile_shape and chunk apply) */
 } st_serve_config;
 
 typedef struct st_request {

@@ -46,12 +46,13 @@ class st_batch_options(C.Structure):
     _fields_ = [("stream", C.c_void_p), ("device_outputs", C.c_int), ("tile_shape", C.c_int), ("chunk", C.c_int),
                 ("use_graph", C.c_int), ("batch_ms", C.c_float), ("rays", C.c_uint64),
                 ("tile_shape_used", C.c_int), ("chunk_used", C.c_int), ("graph_replayed", C.c_int),
-                ("stack_placement", C.c_int), ("stack_placement_used", C.c_int)]
+                ("stack_placement", C.c_int), ("stack_placement_used", C.c_int),
+                ("launch_mode", C.c_int), ("launch_mode_used", C.c_int)]
 
 
 class st_serve_config(C.Structure):
     _fields_ = [("max_in_flight", C.c_int), ("max_views_per_batch", C.c_int), ("frame_budget", C.c_uint64),
-                ("tile_shape", C.c_int), ("chunk", C.c_int), ("refit_fraction", C.c_double)]
+                ("tile_shape", C.c_int), ("chunk", C.c_int), ("refit_fraction", C.c_double), ("launch_mode", C.c_int)]
 
 
 class st_request(C.Structure):
@@ -266,7 +267,8 @@ class Renderer:
         return opt
 
 
-def render_batch(renderer, items, tile_shape=-1, chunk=0, use_graph=False, device_outputs=False, stack_placement=-1):
+def render_batch(renderer, items, tile_shape=-1, chunk=0, use_graph=False, device_outputs=False, stack_placement=-1,
+                 launch_mode=-1):
     """st_render_batch over items = [(slot, SceneData, Frame)]; outputs go to each Frame's buffers
     (host) unless device_outputs, in which case Frame.grid pointers are used as device pointers."""
     keep = []
@@ -282,6 +284,7 @@ def render_batch(renderer, items, tile_shape=-1, chunk=0, use_graph=False, devic
     opt = st_batch_options()
     opt.tile_shape, opt.chunk, opt.use_graph, opt.device_outputs = tile_shape, chunk, int(use_graph), int(device_outputs)
     opt.stack_placement = stack_placement
+    opt.launch_mode = launch_mode
     renderer._check(renderer.L.st_render_batch(renderer.ctx, views, len(items), C.byref(opt)), "st_render_batch")
     return opt
 
@@ -296,10 +299,11 @@ class Server:
     the Renderer takes no other calls."""
 
     def __init__(self, renderer, max_in_flight=3, max_views_per_batch=64, frame_budget=0, tile_shape=-1, chunk=0,
-                 refit_fraction=0.25):
+                 refit_fraction=0.25, launch_mode=0):
         self.r = renderer
         self.L = renderer.L
-        cfg = st_serve_config(max_in_flight, max_views_per_batch, frame_budget, tile_shape, chunk, refit_fraction)
+        cfg = st_serve_config(max_in_flight, max_views_per_batch, frame_budget, tile_shape, chunk, refit_fraction,
+                              launch_mode)
         renderer._check(self.L.st_serve_start(renderer.ctx, C.byref(cfg)), "st_serve_start")
         self._keep = {}
         self.running = True

@@ -75,6 +75,10 @@ struct BatchState {
     BatchView *staging = nullptr;       // pinned host copy of the device view table
     size_t staging_cap = 0;
     BatchTable host_table;              // the view table of the launch group being issued (a kernel parameter)
+    // launch mode 1 (one kernel per view): the streams the views are spread over and the events that
+    // fork them from and join them back to the launching stream (created on first use)
+    cudaStream_t aux[kAuxStreams] = {};
+    cudaEvent_t fork_ev = nullptr, join_ev[kAuxStreams] = {};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     std::map<std::string, std::pair<int, int>> tuned;   // scene-class key -> (kernel variant, chunk)
@@ -100,6 +104,27 @@ struct ServeReq {
     uint32_t *mapped_u8 = nullptr;     // the device view of a page-locked out_u8 (written by the resolve kernel)
     bool pinned_float = false;         // out_float is page-locked (one direct device-to-host copy)
 };
+
+cudaError_t ensure_aux(BatchState &B) {
+    if (B.fork_ev) return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < kAuxStreams && e == cudaSuccess; i++) {
+        e = cudaStreamCreateWithFlags(&B.aux[i], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&B.join_ev[i], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&B.fork_ev, cudaEventDisableTiming);
+    return e;
+}
+void release_aux(BatchState &B) {
+    for (int i = 0; i < kAuxStreams; i++) {
+        if (B.aux[i]) cudaStreamDestroy(B.aux[i]);
+        if (B.join_ev[i]) cudaEventDestroy(B.join_ev[i]);
+        B.aux[i] = nullptr;
+        B.join_ev[i] = nullptr;
+    }
+    if (B.fork_ev) cudaEventDestroy(B.fork_ev);
+    B.fork_ev = nullptr;
+}
 
 struct InFlight {
     bool busy = false;
@@ -340,6 +365,7 @@ int st_init(st_ctx **out, const st_config *cfg) {
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&ctx->ev[i]);
+
     if (e != cudaSuccess) {
         delete ctx;
         return ST_ERR_CUDA;
@@ -380,6 +406,7 @@ void st_shutdown(st_ctx *ctx) {
     if (ctx->batch.graph) cudaGraphDestroy(ctx->batch.graph);
     if (ctx->batch.staging) cudaFreeHost(ctx->batch.staging);
     for (auto &e : ctx->ev) if (e) cudaEventDestroy(e);
+    release_aux(ctx->batch);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -1121,6 +1148,40 @@ int plan_batch(st_ctx *ctx, const st_view *views, int n, int tile, const st_batc
 int launch_groups(st_ctx *ctx, BatchState &B, const BatchPlan &p, int tile, u32t chunk, unsigned *status,
                   cudaStream_t st) {
     const int n = (int)p.table.size();
+    if (tile == kPerViewVariant) {
+        // one per-frame trace kernel per view, the views spread over the auxiliary streams (the
+        // kernels run side by side wherever one leaves SMs idle), between the set-up and the resolves
+        for (int g0 = 0; g0 < n; g0 += kTableViews) {
+            const int gn = std::min(kTableViews, n - g0);
+            u32t max_prims = 0, max_rows = 0, max_w = 0, max_h = 0;
+            for (int i = 0; i < gn; i++) {
+                const BatchView &b = p.table[g0 + i];
+                B.host_table.v[i] = b;
+                max_prims = std::max(max_prims, b.scene.n_prims);
+                max_rows = std::max(max_rows, b.view.grid_h);
+                if (b.out_u8) {
+                    max_w = std::max(max_w, b.view.grid_w - 1);
+                    max_h = std::max(max_h, b.view.grid_h - 1);
+                }
+            }
+            launch_batch_setup(B.host_table, (u32t)gn, max_prims, max_rows, st);
+            ST_CUDA(ensure_aux(B));
+            ST_CUDA(cudaEventRecord(B.fork_ev, st));
+            const int streams = std::min(gn, kAuxStreams);
+            for (int k = 0; k < streams; k++) ST_CUDA(cudaStreamWaitEvent(B.aux[k], B.fork_ev, 0));
+            for (int i = 0; i < gn; i++) {
+                const BatchView &b = B.host_table.v[i];
+                launch_trace(b.scene, b.view, b.ssb, b.dirs, b.out, nullptr, status, P<unsigned long long>(ctx->counters),
+                             false, B.aux[i % streams]);
+            }
+            for (int k = 0; k < streams; k++) {
+                ST_CUDA(cudaEventRecord(B.join_ev[k], B.aux[k]));
+                ST_CUDA(cudaStreamWaitEvent(st, B.join_ev[k], 0));
+            }
+            if (max_w) launch_batch_resolve(B.host_table, (u32t)gn, max_w, max_h, st);
+        }
+        return ST_CUDA_LAST();
+    }
     const u32t blocks = (u32t)(ctx->sm_count * ctx->blocks_per_sm[tile]);
     // the device copy of the table, tile numbers rebased per group, for the trace kernel
     for (int i = 0; i < n; i++) {
@@ -1202,20 +1263,29 @@ int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *
     memset(&dflt, 0, sizeof(dflt));
     dflt.tile_shape = -1;
     dflt.stack_placement = -1;
+    dflt.launch_mode = -1;
     st_batch_options &o = opt ? *opt : dflt;
     cudaStream_t st = o.stream ? (cudaStream_t)o.stream : ctx->stream;
     BatchState &B = ctx->batch;
     // the kernel variant (tile shape, stack placement) and queue chunk: given, cached for this scene
     // class, or tuned now
-    if (o.tile_shape >= TILE_SHAPES || o.stack_placement >= STACK_PLACEMENTS) return ST_ERR_INVALID_ARG;
+    if (o.tile_shape >= TILE_SHAPES || o.stack_placement >= STACK_PLACEMENTS || o.launch_mode > 1) return ST_ERR_INVALID_ARG;
     BatchPlan p;
-    int tile = (o.tile_shape >= 0 && o.stack_placement >= 0) ? o.tile_shape + TILE_SHAPES * o.stack_placement : -1;
-    u32t chunk = o.chunk > 0 ? (u32t)o.chunk : 0;
+    // launch mode 1 (one kernel per view) has no tile shape, stack placement or chunk to choose; mode
+    // 0 with every knob given needs no tuning; otherwise the choice is cached per scene class or tuned
+    const bool fixed_tile = o.tile_shape >= 0 || o.stack_placement >= 0;
+    int tile = o.launch_mode == 1 ? kPerViewVariant
+               : (o.tile_shape >= 0 && o.stack_placement >= 0) ? o.tile_shape + TILE_SHAPES * o.stack_placement : -1;
+    u32t chunk = o.launch_mode == 1 ? 1u : o.chunk > 0 ? (u32t)o.chunk : 0;
     ST_TRY(plan_batch(ctx, views, n, o.tile_shape >= 0 ? o.tile_shape : 0, o, p));
     if (tile < 0 || chunk == 0) {
         auto it = B.tuned.find(p.class_key);
-        const bool fits = it != B.tuned.end() && (o.tile_shape < 0 || variant_tile(it->second.first) == o.tile_shape) &&
-                          (o.stack_placement < 0 || variant_stack(it->second.first) == o.stack_placement);
+        const bool per_view = it != B.tuned.end() && it->second.first == kPerViewVariant;
+        const bool fits = it != B.tuned.end() &&
+                          (per_view ? (o.launch_mode != 0 && !fixed_tile && !o.chunk)
+                                    : (o.launch_mode != 1 &&
+                                       (o.tile_shape < 0 || variant_tile(it->second.first) == o.tile_shape) &&
+                                       (o.stack_placement < 0 || variant_stack(it->second.first) == o.stack_placement)));
         if (fits) {
             if (tile < 0) tile = it->second.first;
             if (!chunk) chunk = (u32t)it->second.second;
@@ -1245,7 +1315,19 @@ int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *
                     }
                 }
             }
-            if (o.tile_shape < 0 && o.stack_placement < 0 && !o.chunk) {
+            if (o.launch_mode < 0 && !fixed_tile && !o.chunk) {   // one kernel per view
+                BatchPlan q;
+                ST_TRY(plan_batch(ctx, views, n, kPerViewVariant, o, q));
+                ST_TRY(batch_reserve(ctx, B, q, n));
+                ST_CUDA(cudaEventRecord(ctx->ev[0], st));
+                ST_TRY(enqueue_batch(ctx, B, P<unsigned>(ctx->status), views, n, q, kPerViewVariant, 1, st, o));
+                ST_CUDA(cudaEventRecord(ctx->ev[1], st));
+                ST_CUDA(cudaStreamSynchronize(st));
+                float ms = 0;
+                cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+                if (ms < best) { best = ms; best_variant = kPerViewVariant; best_chunk = 1; }
+            }
+            if (o.tile_shape < 0 && o.stack_placement < 0 && !o.chunk && o.launch_mode < 0) {
                 B.tuned[p.class_key] = {best_variant, (int)best_chunk};
                 if (const char *path = getenv("ST_AUTOTUNE_CACHE")) {
                     std::ofstream f(path, std::ios::app);
@@ -1307,8 +1389,9 @@ int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *
     ST_CUDA(cudaStreamSynchronize(st));
     cudaEventElapsedTime(&o.batch_ms, ctx->ev[0], ctx->ev[1]);
     o.rays = p.rays;
-    o.tile_shape_used = variant_tile(tile);
-    o.stack_placement_used = variant_stack(tile);
+    o.launch_mode_used = tile == kPerViewVariant ? 1 : 0;
+    o.tile_shape_used = tile == kPerViewVariant ? -1 : variant_tile(tile);
+    o.stack_placement_used = tile == kPerViewVariant ? -1 : variant_stack(tile);
     o.chunk_used = (int)chunk;
     if (status[0] & S_STACK_OVERFLOW) return ST_ERR_STACK_OVERFLOW;
     return ST_OK;
@@ -1669,7 +1752,7 @@ int launch_flight(st_ctx *ctx, int f, std::vector<std::shared_ptr<ServeReq>> &re
     // view table and arena layout
     const int n = (int)reqs.size();
     BatchPlan p;
-    int tile = V.cfg.tile_shape >= 0 ? V.cfg.tile_shape : TILE_8x4;
+    int tile = V.cfg.launch_mode == 0 ? kPerViewVariant : V.cfg.tile_shape >= 0 ? V.cfg.tile_shape : TILE_8x4;
     u32t chunk = V.cfg.chunk > 0 ? (u32t)V.cfg.chunk : 1;
     std::ostringstream cls;
     size_t dev = 0, host = 64;
@@ -1683,9 +1766,9 @@ int launch_flight(st_ctx *ctx, int f, std::vector<std::shared_ptr<ServeReq>> &re
         for (u32t x = tris; x > 1; x >>= 1) tb++;
         cls << "p" << pb << "t" << tb << "d" << r->view.depth << ";";
     }
-    if (V.cfg.tile_shape < 0 || V.cfg.chunk <= 0) {
+    if (V.cfg.launch_mode != 0 && (V.cfg.tile_shape < 0 || V.cfg.chunk <= 0)) {
         auto it = ctx->batch.tuned.find(cls.str());
-        if (it != ctx->batch.tuned.end()) {
+        if (it != ctx->batch.tuned.end() && it->second.first != kPerViewVariant) {
             if (V.cfg.tile_shape < 0) tile = it->second.first;
             if (V.cfg.chunk <= 0) chunk = (u32t)it->second.second;
         }
@@ -1827,6 +1910,7 @@ int st_serve_start(st_ctx *ctx, const st_serve_config *cfg) {
     if (V.cfg.max_views_per_batch <= 0) V.cfg.max_views_per_batch = 64;
     if (V.cfg.refit_fraction <= 0) V.cfg.refit_fraction = 0.25;
     if (!cfg) { V.cfg.tile_shape = -1; V.cfg.chunk = 0; }
+    if (V.cfg.launch_mode < 0 || V.cfg.launch_mode > 1) return ST_ERR_INVALID_ARG;
     V.frame_budget = V.cfg.frame_budget ? V.cfg.frame_budget
                                         : (ctx->budget > ctx->in_use ? ctx->budget - ctx->in_use : 0);
     V.flights.resize(V.cfg.max_in_flight);
@@ -1960,6 +2044,7 @@ int st_serve_stop(st_ctx *ctx) {
     for (InFlight &F : V.flights) {
         if (F.pinned) cudaFreeHost(F.pinned);
         if (F.B.staging) cudaFreeHost(F.B.staging);
+        release_aux(F.B);
         for (DevBuf *b : {&F.B.table, &F.B.counter, &F.status}) release(ctx, *b);
         if (F.done_ev) cudaEventDestroy(F.done_ev);
         if (F.stream) cudaStreamDestroy(F.stream);

@@ -52,6 +52,10 @@ constexpr int STACK_PLACEMENTS = 2;
 constexpr int BATCH_VARIANTS = TILE_SHAPES * STACK_PLACEMENTS;
 inline int variant_tile(int variant) { return variant % TILE_SHAPES; }
 inline int variant_stack(int variant) { return variant / TILE_SHAPES; }
+// The other launch mode of a batch: one per-frame trace kernel per view, views spread over
+// kAuxStreams streams.
+constexpr int kPerViewVariant = BATCH_VARIANTS;
+constexpr int kAuxStreams = 8;
 
 void launch_ssb(const SceneDev &S, const ViewDev &v, int4 *ssb, cudaStream_t st);
 int launch_batch(const BatchView *views, u32t n_views, u32t total_tiles, int variant, u32t chunk, u32t grid_blocks,

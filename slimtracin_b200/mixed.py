@@ -134,7 +134,7 @@ class Batch:
     """The same views in one st_render_batch call (device outputs, autotuned, CUDA graph)."""
 
     def __init__(self, renderer, items, out_float_ptrs, out_u8_ptrs, use_graph=True, tile_shape=-1, chunk=0,
-                 stack_placement=-1):
+                 stack_placement=-1, launch_mode=-1):
         self.r = renderer
         self.views = (api.st_view * len(items))()
         self.keep = items
@@ -146,6 +146,7 @@ class Batch:
         self.opt.device_outputs, self.opt.use_graph = 1, int(use_graph)
         self.opt.tile_shape, self.opt.chunk = tile_shape, chunk
         self.opt.stack_placement = stack_placement
+        self.opt.launch_mode = launch_mode
 
     def run(self):
         s = self.r.L.st_render_batch(self.r.ctx, self.views, len(self.views), C.byref(self.opt))
@@ -159,10 +160,11 @@ class Stream:
     resolution, bounces, camera) plus a transform update of 0..64 primitives, delivered as a
     resolved u8 frame into host memory."""
 
-    def __init__(self, residents, slots, rate, count, seed, refit_fraction=0.25):
+    def __init__(self, residents, slots, rate, count, seed, refit_fraction=0.25, launch_mode=0):
         rng = np.random.default_rng(seed)
         self.residents, self.slots, self.rate = residents, slots, rate
         self.refit_fraction = refit_fraction
+        self.launch_mode = launch_mode
         self.arrivals = poisson_arrivals(rng, rate, count)
         # one page-locked frame per resolution, shared by the requests (the kernels write it directly)
         import torch
@@ -192,7 +194,7 @@ class Stream:
         (arrival, completion, rays, status, width, height, batch size)."""
         L, ctx = renderer.L, renderer.ctx
         srv = api.Server(renderer, max_in_flight=max_in_flight, max_views_per_batch=max_views_per_batch,
-                         refit_fraction=self.refit_fraction)
+                         refit_fraction=self.refit_fraction, launch_mode=self.launch_mode)
         tickets = []
         try:
             t0 = L.st_clock() + 0.02

@@ -271,6 +271,14 @@ def test_batch_equals_per_frame_renders(renderer):
                     assert opt.tile_shape_used == tile
                 if stack >= 0:
                     assert opt.stack_placement_used == stack
+    for graph in (False, True, True):        # one trace kernel per view, on concurrent streams
+        frames = [scenes.Frame(w, h, cam, depth=d, mode=m) for slot, sd, cam, w, h, d, m in specs]
+        opt = api.render_batch(renderer, [(sp[0], sp[1], fr) for sp, fr in zip(specs, frames)], use_graph=graph,
+                               launch_mode=1)
+        assert opt.launch_mode_used == 1
+        for a, b in zip(frames, singles):
+            assert np.array_equal(a.float_pixels.view(np.uint8), b.float_pixels.view(np.uint8)), ("per view", graph)
+            assert np.array_equal(a.pixels.view(np.uint8), b.pixels.view(np.uint8))
 
 
 def test_pinned_host_outputs_written_by_the_kernels(renderer):
