@@ -694,11 +694,12 @@ __device__ __forceinline__ void flush_counters(TState<CNT, SHS> &t, unsigned *st
     }
 }
 
-// Resident 128-thread blocks per SM the register allocation must allow.  Six (85 registers, more
-// spills) beat the compiler's own choice of 128 registers (four blocks) on the 1080p mesh frame:
-// 2.44 vs 2.62 ms; 5, 7 and 8 blocks measured 2.52, 2.45 and 2.38 ms, 2 blocks 5.6 ms.
+// Resident 128-thread blocks per SM the register allocation must allow.  Eight (64 registers, more
+// spills) beat the compiler's own choice of 128 registers (four blocks) on the 1080p mesh frame
+// (2.38 vs 2.62 ms), and six and seven blocks (2.42, 2.40 ms) there, on the 64-view mixed batch and
+// on the served stream; 5 blocks measured 2.52 ms, 2 blocks 5.6 ms.
 #ifndef ST_TRACE_MIN_BLOCKS
-#define ST_TRACE_MIN_BLOCKS 6
+#define ST_TRACE_MIN_BLOCKS 8
 #endif
 #define ST_TRACE_BOUNDS __launch_bounds__(128, ST_TRACE_MIN_BLOCKS)
 template <bool CNT>
