@@ -175,7 +175,7 @@ ST_API int st_render_scene(st_ctx *ctx, int slot, const Scene *scene, Viewport *
 ST_API int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *viewport,
                  st_render_options *options);
 
-/* ---- batched views: many views of resident scenes in one persistent launch --------------------- */
+/* ---- batched views: many views of resident scenes in one call ------------------------------------ */
 typedef struct st_view {
     int slot;                   /* resident scene */
     const Scene *scene;         /* per-frame values (ambient light); NULL -> the uploaded ones */
@@ -202,9 +202,11 @@ typedef struct st_batch_options {
     int launch_mode_used;       /* out (with launch mode 1, tile_shape_used and stack_placement_used are -1) */
 } st_batch_options;
 
-/* Render `view_count` views (different sizes, scenes, render modes and bounce counts) with one
- * persistent kernel over a shared tile queue.  No reference counterpart: the reference renders one
- * viewport per renderScene call (raytracer.h:302); each view's output equals st_render_ex's. */
+/* Render `view_count` views (different sizes, scenes, render modes and bounce counts) in one call:
+ * one persistent kernel over a shared tile queue, or one trace kernel per view on concurrent
+ * streams (launch_mode; the views' set-up and resolves are one launch each per 64 views).  No
+ * reference counterpart: the reference renders one viewport per renderScene call (raytracer.h:302);
+ * each view's output equals st_render_ex's. */
 ST_API int st_render_batch(st_ctx *ctx, const st_view *views, int view_count, st_batch_options *options);
 
 /* LBVH30 over device-resident boxes with no allocation.  No counterpart in the reference: its
@@ -243,8 +245,9 @@ ST_API int st_pick(st_ctx *ctx, int slot, const Scene *scene, const Viewport *vi
  * A worker thread inside the library takes submitted requests in order, admits them while the
  * device-memory budget for in-flight frame/ray buffers allows, applies their transform updates,
  * refits (few moved primitives) or rebuilds (many) the TLAS of exactly the scenes that changed,
- * and launches each batch with the persistent multi-view kernel on one of `max_in_flight` streams,
- * so requests that arrive while other batches run are launched beside them.  An update to a scene
+ * and launches each batch (one trace kernel per view on the batch's own streams, or the persistent
+ * multi-view kernel) from one of `max_in_flight` streams, so requests that arrive while other
+ * batches run are launched beside them.  An update to a scene
  * that batches in flight still read goes to a new copy of the scene's primitive and TLAS arrays
  * (a scene version; at most one per batch in flight, counted against the context's budget), so it
  * never waits for them.  A request never shares a batch with a request that changes its scene
