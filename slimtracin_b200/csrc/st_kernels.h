@@ -53,9 +53,12 @@ constexpr int BATCH_VARIANTS = TILE_SHAPES * STACK_PLACEMENTS;
 inline int variant_tile(int variant) { return variant % TILE_SHAPES; }
 inline int variant_stack(int variant) { return variant / TILE_SHAPES; }
 // The other launch mode of a batch: one per-frame trace kernel per view, views spread over
-// kAuxStreams streams.
+// kAuxStreams streams (16 streams measured the same as 8 on the 64-view mix and the served stream).
 constexpr int kPerViewVariant = BATCH_VARIANTS;
-constexpr int kAuxStreams = 8;
+#ifndef ST_AUX_STREAMS
+#define ST_AUX_STREAMS 8
+#endif
+constexpr int kAuxStreams = ST_AUX_STREAMS;
 
 void launch_ssb(const SceneDev &S, const ViewDev &v, int4 *ssb, cudaStream_t st);
 int launch_batch(const BatchView *views, u32t n_views, u32t total_tiles, int variant, u32t chunk, u32t grid_blocks,
