@@ -277,3 +277,29 @@ def test_overlays_match_reference(which):
         changed = np.count_nonzero(a.float_pixels.view(np.uint8).reshape(len(a.float_pixels), -1)
                                    != a.base.view(np.uint8).reshape(len(a.base), -1), axis=1)
         assert np.count_nonzero(changed) > 100, "the overlay drew almost nothing"
+
+
+def test_overlays_far_plane_matches_reference():
+    """drawBVH / drawSSB with a far clipping plane inside the scene (cullAndClipEdge's far branch,
+    shapes/edge.h:23-29): the oracle still equals the reference's own drawing."""
+    if not oracle.reference_available():
+        pytest.skip("reference harness not built")
+    sd, cam = H.overlay_scene("config0")
+    H.tlas_sah(sd, "ref")
+    out = {}
+    for which in ("orc", "ref"):
+        fr = H.oracle_frame(sd, cam, 160, 120, depth=1)
+        fr.viewport.settings.far_clipping_plane_distance = np.float32(16.0)
+        scenes.set_projection_matrix(fr.viewport, fr.camera, fr.grid.dimensions)
+        base = fr.float_pixels.copy()
+        lib = oracle.restatement() if which == "orc" else oracle.reference()
+        d = sd.copy()
+        sc, keep = d.to_ctypes()
+        (lib.orc_update_scene_ssb if which == "orc" else lib.ref_update_scene_ssb)(C.byref(sc), C.byref(fr.viewport))
+        if which == "orc":
+            lib.orc_draw_overlays(C.byref(sc), C.byref(fr.viewport), 3)
+        else:
+            assert lib.ref_draw_overlays(C.byref(sc), C.byref(fr.viewport), 3) == 0
+        out[which] = fr.float_pixels.copy()
+        assert np.count_nonzero(out[which].view(np.uint8) != base.view(np.uint8)) > 100
+    assert out["orc"].tobytes() == out["ref"].tobytes()
