@@ -23,12 +23,15 @@ config0    config 0: 16 implicit primitives, 3 point lights, 640x480, depth 2: t
 dynamic    config 2: 4096 moving primitives, TLAS rebuilt (LBVH30, binned SAH) or refit every frame,
            1280x720 depth 2, 300 frames: build ms (API wall time) and trace ms (device events)
 batched    64 views (resolutions from 256x256 to 1920x1080, 1-6 bounces) over 8 resident scenes:
-           one st_render_batch call (persistent kernel, autotuned, CUDA graph) against one
-           st_render_ex call per view, both timed with device events around the whole sequence
+           one st_render_batch call (launch mode, tile shape, queue depth and stack placement
+           autotuned, CUDA graph) against one st_render_ex call per view, both timed with device
+           events around the whole sequence
 served     Poisson request streams (--rates) over the same 8 scenes, each request a view plus a
            transform update of 0-64 primitives, u8 frames to host: the library's server against
            the same requests one at a time; p50/p99 latency from arrival to completion (library
            clock) and Mrays/s over the stream
+ingest     texture baking (st_bake_texture, 1024x1024) and OBJ conversion (st_obj_to_mesh at 20,480
+           and 327,680 triangles) beside the reference's loadTexture and obj2mesh on the host
 """
 import argparse
 import ctypes as C
