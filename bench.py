@@ -13,8 +13,10 @@ value      primary rays of all ranks / (max over ranks of the device time of K r
 e2e        the same through st_render_scene with host buffers: each step uploads the primitive
            records (H2D) and reads back the float grid and the u8 frame (D2H)
 roofline   the trace kernel: algorithmic bytes per frame (device event counters on the reference
-           traversal, bytes per event as defined in DESIGN.md) / its CUDA-event time, against the
-           measured HBM copy bandwidth
+           traversal times the bytes per event of BYTES below: 32 per AABB test, 64 per triangle
+           test, 72 per implicit-primitive test, 4 per leaf id, 148 per shaded hit, 12 per texel
+           fetch, 24 per primary ray) / its CUDA-event time, against the measured HBM copy
+           bandwidth and an L2-resident read rate measured in the same run
 cpu_baseline / --impl reference
            the reference's own renderer (oracle/_ref, compiled from the reference sources) on the
            same scene bytes, all host threads, over a bounded sample of rows
