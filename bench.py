@@ -5,7 +5,7 @@
 Workload (one step = one frame): 1920x1080 viewport = 1921x1081 QCAA grid of primary rays,
 trace.depth 4, one displaced icosphere of 1,310,720 triangles in 8 instances (4 Cook-Torrance,
 2 glass, 2 mirror), two 1024^2 textures with 9-level mip chains, 2 emissive quads.  Seeded
-synthetic data (scenes.config1); the BLAS is built on the device (binned SAH) once, before timing.
+synthetic data (scenes.mesh_scene); the BLAS is built on the device (binned SAH) once, before timing.
 
 value      primary rays of all ranks / (max over ranks of the device time of K renders), inputs
            resident, outputs to device buffers; L2 flushed (256 MiB write) before every step,
@@ -20,7 +20,7 @@ roofline   the trace kernel: algorithmic bytes per frame (device event counters 
 cpu_baseline / --impl reference
            the reference's own renderer (oracle/_ref, compiled from the reference sources) on the
            same scene bytes, all host threads, over a bounded sample of rows
-config0    config 0: 16 implicit primitives, 3 point lights, 640x480, depth 2: the device frame beside
+implicit16 16 implicit primitives, 3 point lights, 640x480, depth 2: the device frame beside
            the reference's CPU renderer (all host threads, and one thread)
 dynamic    config 2: 4096 moving primitives, TLAS rebuilt (LBVH30, binned SAH) or refit every frame,
            1280x720 depth 2, 300 frames: build ms (API wall time) and trace ms (device events)
@@ -64,7 +64,7 @@ def dist_env():
 
 
 def build_scene(seed_offset=0):
-    sd, cam = scenes.config1(seed_offset=seed_offset)
+    sd, cam = scenes.mesh_scene(seed_offset=seed_offset)
     return sd, cam
 
 
@@ -182,8 +182,8 @@ def run_reference_arm(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
             "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * grid / (value * 1e6),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded config1 scene bytes, identical to the device arm)",
-            "config": {"workload": "config1 1080p PBR mesh scene, depth 4, 1.31M-triangle BLAS x 8 instances",
+            "data": "synthetic (seeded mesh-scene bytes, identical to the device arm)",
+            "config": {"workload": "1080p PBR mesh scene, depth 4, 1.31M-triangle BLAS x 8 instances",
                        "width": WIDTH, "height": HEIGHT, "depth": DEPTH, "rays_per_frame": grid},
             "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": "reference",
                              "sample": f"{steps} whole frames ({rows} QCAA rows each), reference rayTrace "
@@ -271,7 +271,7 @@ def dynamic_tlas(r, frames, cpu_reference):
     slot = 12
     for name, mode in (("lbvh30", api.ST_BVH_LBVH30), ("binned_sah", api.ST_BVH_BINNED_SAH),
                        ("refit", api.ST_BVH_REFIT)):
-        sd, cam = scenes.config2()
+        sd, cam = scenes.moving_scene()
         r.upload(slot, sd, tlas=None)
         r.build_tlas(slot, sd, api.ST_BVH_LBVH30)     # the topology a refit keeps
         fr = scenes.Frame(1280, 720, cam, depth=2, with_pixels=False, with_float=False)
@@ -282,7 +282,7 @@ def dynamic_tlas(r, frames, cpu_reference):
         opt.device_outputs, opt.out_float, opt.out_u8 = 1, dev_f.data_ptr(), dev_u.data_ptr()
         up_ms, build_ms, trace_ms = [], [], []
         for _ in range(frames):
-            scenes.advance_config2(sd, 1)           # in place: sc.primitives sees the new records
+            scenes.advance_moving_scene(sd, 1)           # in place: sc.primitives sees the new records
             t0 = time.perf_counter()
             r._check(L.st_upload_primitives(r.ctx, slot, C.byref(sc)), "st_upload_primitives")
             t1 = time.perf_counter()
@@ -303,11 +303,11 @@ def dynamic_tlas(r, frames, cpu_reference):
             import oracle
             if oracle.reference_available():
                 ref = oracle.reference()
-                sd, _ = scenes.config2()
+                sd, _ = scenes.moving_scene()
                 sc, keep = sd.to_ctypes()
                 ts = []
                 for _ in range(5):
-                    scenes.advance_config2(sd, 1)
+                    scenes.advance_moving_scene(sd, 1)
                     t = time.perf_counter()
                     ref.ref_update_scene_bvh(C.byref(sc))
                     ts.append((time.perf_counter() - t) * 1e3)
@@ -317,12 +317,12 @@ def dynamic_tlas(r, frames, cpu_reference):
     return out
 
 
-def config0_section(r, cpu_reference):
+def implicit16_section(r, cpu_reference):
     """Config 0 (16 implicit primitives, 3 point lights, 640x480, depth 2): the device frame (device
     outputs, trace kernel by CUDA events) beside the reference's CPU renderer on the same scene."""
     import torch
     from slimtracin_b200 import api
-    sd, cam = scenes.config0()
+    sd, cam = scenes.implicit16_scene()
     slot = 13
     r.upload(slot, sd, tlas=None)
     r.build_tlas(slot, sd, api.ST_BVH_BINNED_SAH)
@@ -580,7 +580,7 @@ def main():
     dynamic = dynamic_tlas(r, args.dynamic_frames, rank == 0 and world == 1 and not args.no_cpu_baseline) \
         if args.dynamic_frames > 0 else None
     l2_gbs = measure_l2_gbs()
-    cfg0 = config0_section(r, rank == 0 and world == 1 and not args.no_cpu_baseline)
+    cfg0 = implicit16_section(r, rank == 0 and world == 1 and not args.no_cpu_baseline)
     ingest = ingest_section(r, rank == 0 and world == 1 and not args.no_cpu_baseline)
 
     # ---- roofline of the trace kernel -----------------------------------------------------------
@@ -589,7 +589,7 @@ def main():
     peak = peaks["hbm_gbs"] if peaks and "hbm_gbs" in peaks else 6650.0
     achieved = bytes_alg / (trace_avg_ms / 1e3) / 1e9
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "trace_kernel_config1_traffic.json")
+    prof = os.path.join(ROOT, "profiles", "trace_kernel_mesh_1080p_traffic.json")
     if os.path.exists(prof):
         try:
             traffic = json.load(open(prof)).get("dram_bytes_per_launch")
@@ -619,8 +619,8 @@ def main():
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded config1 scene: displaced icosphere, Perlin textures; no dataset)",
-            "config": {"workload": "config1 1080p PBR mesh scene, depth 4, 1.31M-triangle BLAS x 8 instances",
+            "data": "synthetic (seeded mesh scene: displaced icosphere, Perlin textures; no dataset)",
+            "config": {"workload": "1080p PBR mesh scene, depth 4, 1.31M-triangle BLAS x 8 instances",
                        "width": WIDTH, "height": HEIGHT, "depth": DEPTH, "rays_per_frame": grid,
                        "triangles": sd.meshes[0].triangle_count, "instances": 8, "parallelism": f"replicas x{world}",
                        "l2": "flushed before every step (256 MiB write, outside the timed events)",
@@ -636,7 +636,7 @@ def main():
                          "l2_peak": l2_gbs, "l2_frac": achieved / l2_gbs,
                          "l2_peak_source": "48 MB L2-resident read (torch.sum), measured in this run"},
             "counters": counters,
-            "config0": cfg0,
+            "implicit16": cfg0,
             "dynamic_tlas": dynamic,
             "ingest": ingest,
             "batched": mixed["batched"] if mixed else None,

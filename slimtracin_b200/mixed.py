@@ -35,15 +35,15 @@ def resident_scenes(mesh_subdivisions=(6, 7, 8), texture_size=1024, big=None):
     """The eight scenes (a prebuilt 1.31M-triangle scene may be passed as `big`)."""
     out = []
     for k in range(4):
-        sd, _ = scenes.config0(seed_offset=100 + k)
+        sd, _ = scenes.implicit16_scene(seed_offset=100 + k)
         out.append(Resident(f"implicit16-{k}", sd, (0.0, 0.0, 0.0), 15.0, 2.0, "sah"))
     for sub in mesh_subdivisions:
         if big is not None and sub == 8:
             sd = big
         else:
-            sd, _ = scenes.config1(seed_offset=200 + sub, subdivisions=sub, texture_size=texture_size)
+            sd, _ = scenes.mesh_scene(seed_offset=200 + sub, subdivisions=sub, texture_size=texture_size)
         out.append(Resident(f"mesh{sd.meshes[0].triangle_count}", sd, (0.0, 1.5, 0.0), 15.0, 8.0, "sah"))
-    sd, _ = scenes.config2(seed_offset=300)
+    sd, _ = scenes.moving_scene(seed_offset=300)
     out.append(Resident("implicit4096", sd, (0.0, 0.0, 0.0), 20.0, 3.0, "sah"))
     return out
 

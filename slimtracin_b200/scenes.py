@@ -4,13 +4,13 @@ One generator feeds the device path, the oracle and the reference harness with t
 PCG32 (O'Neill 2014, XSH-RR output) with seed 0x5EED0000 + config drives every draw; rotations are
 uniform unit quaternions by Shoemake's method.  No public dataset is involved.
 
-Configs (sizes as the benchmark names them; tests use the `scale` arguments to shrink them):
-  config0  16 implicit primitives (4 each of sphere/box/quad/tetrahedron), 3 point lights,
-           Lambert/Blinn/Phong materials, 640x480, depth 2.
-  config1  one displaced icosphere mesh (subdivision 8 = 1,310,720 triangles) in 8 instances,
-           4 Cook-Torrance + 2 glass + 2 mirror materials with 1024^2 albedo/normal textures,
-           2 emissive quads, 1920x1080, depth 4.
-  config2  4096 implicit primitives moving every frame, 1280x720, depth 2.
+Scenes (sizes as the benchmark uses them; tests use the size arguments to shrink them):
+  implicit16_scene  16 implicit primitives (4 each of sphere/box/quad/tetrahedron), 3 point
+                    lights, Lambert/Blinn/Phong materials, 640x480, depth 2.
+  mesh_scene        one displaced icosphere mesh (subdivision 8 = 1,310,720 triangles) in 8
+                    instances, 4 Cook-Torrance + 2 glass + 2 mirror materials with 1024^2
+                    albedo/normal textures, 2 emissive quads, 1920x1080, depth 4.
+  moving_scene      4096 implicit primitives moving every frame, 1280x720, depth 2.
 
 The reference has no shininess field: the Blinn/Phong exponent is {16,4}*(1-roughness)
 (render/shaders/common.h:294-316), so "shininess U[2,128]" maps to roughness U[0, 0.875].
@@ -458,19 +458,19 @@ def _point_lights(rng: PCG32, n):
     return lights
 
 
-def config0(seed_offset=0):
+def implicit16_scene(seed_offset=0):
     """16 implicit primitives (4 of each type in blocks), 3 point lights, 16 classic materials."""
     rng = PCG32(0x5EED0000 + 0 + seed_offset)
     prims = _random_implicit(rng, 16, blocks=True)
     prims["material_id"] = np.arange(16)
     mats = _classic_materials(rng, 16)
     lights = _point_lights(rng, 3)
-    sd = SceneData(prims, mats, lights, ambient=(0.004, 0.004, 0.007), name="config0")
+    sd = SceneData(prims, mats, lights, ambient=(0.004, 0.004, 0.007), name="implicit16")
     return sd, CameraSpec((0.0, 0.0, -15.0), 0.0, 0.0, 2.0)
 
 
-def config2(seed_offset=0, count=4096, spread=5.0):
-    """`count` implicit primitives of uniformly drawn types, same distributions as config0, plus
+def moving_scene(seed_offset=0, count=4096, spread=5.0):
+    """`count` implicit primitives of uniformly drawn types, same distributions as implicit16_scene, plus
     per-primitive velocities (units/frame) and angular velocities (axis, rad/frame)."""
     rng = PCG32(0x5EED0000 + 2 + seed_offset)
     prims = default_primitives(count)
@@ -488,14 +488,14 @@ def config2(seed_offset=0, count=4096, spread=5.0):
     mats = _classic_materials(rng, 16)
     prims["material_id"] = np.arange(count) % 16
     lights = _point_lights(rng, 3)
-    sd = SceneData(prims, mats, lights, ambient=(0.004, 0.004, 0.007), name="config2")
+    sd = SceneData(prims, mats, lights, ambient=(0.004, 0.004, 0.007), name="moving")
     sd.velocities = vel
     sd.angular = ang
     return sd, CameraSpec((0.0, 0.0, -15.0 - spread), 0.0, 0.0, 2.0)
 
 
-def advance_config2(sd: SceneData, frames=1):
-    """Integrate the config2 motion by `frames` steps in float32 on the host."""
+def advance_moving_scene(sd: SceneData, frames=1):
+    """Integrate the moving scene's motion by `frames` steps in float32 on the host."""
     p = sd.primitives
     for _ in range(frames):
         p["position"] = (p["position"] + sd.velocities.astype(F32)).astype(F32)
@@ -687,7 +687,7 @@ def bake_texture(rgb, wrap=True, mipmap=True):
     return TextureData(width, height, wrap, mipmap, mips)
 
 
-def config1(seed_offset=0, subdivisions=8, texture_size=1024, instances=8, radius=2.5):
+def mesh_scene(seed_offset=0, subdivisions=8, texture_size=1024, instances=8, radius=2.5):
     """The 1080p PBR mesh scene (sizes at the defaults).  The icosphere has radius 2.5 and the camera
     frames the instances (about 42% of primary rays hit, 27% a mesh instance at 1080p); neither is
     fixed by the benchmark's description."""
@@ -746,7 +746,7 @@ def config1(seed_offset=0, subdivisions=8, texture_size=1024, instances=8, radiu
     albedo, normal = perlin_textures(texture_size, seed=rng.next_u32())
     textures = [bake_texture(albedo, True, True), bake_texture(normal, True, True)]
     sd = SceneData(prims, mats, default_lights(0), ambient=(0.004, 0.004, 0.007),
-                   meshes=[mesh], textures=textures, name="config1")
+                   meshes=[mesh], textures=textures, name="mesh")
     cam = look_at((0.0, 8.0, -15.0), (0.0, 1.5, 0.0))
     return sd, cam
 

@@ -36,24 +36,24 @@ def render_cases():
     """(name, scene builder, camera, w, h, depth, mode) of the golden renders."""
     cases = []
     for mode, mname in ((S.RM_BEAUTY, "beauty"), (S.RM_DEPTH, "depth"), (S.RM_NORMALS, "normals"), (S.RM_UVS, "uvs")):
-        cases.append((f"config0_{mname}", "config0", 96, 72, 2, mode))
+        cases.append((f"implicit16_{mname}", "implicit16", 96, 72, 2, mode))
     cases.append(("area_lights_beauty_d3", "area", 96, 72, 3, S.RM_BEAUTY))
-    cases.append(("config1_tiny_beauty_d4", "config1_tiny", 96, 54, 4, S.RM_BEAUTY))
-    cases.append(("config1_tiny_normals", "config1_tiny", 96, 54, 4, S.RM_NORMALS))
-    cases.append(("config2_256_beauty", "config2_256", 96, 54, 2, S.RM_BEAUTY))
+    cases.append(("mesh_tiny_beauty_d4", "mesh_tiny", 96, 54, 4, S.RM_BEAUTY))
+    cases.append(("mesh_tiny_normals", "mesh_tiny", 96, 54, 4, S.RM_NORMALS))
+    cases.append(("moving256_beauty", "moving256", 96, 54, 2, S.RM_BEAUTY))
     return cases
 
 
 def make_scene(kind, which="ref"):
-    if kind == "config0":
-        sd, cam = scenes.config0()
+    if kind == "implicit16":
+        sd, cam = scenes.implicit16_scene()
     elif kind == "area":
         sd, cam = scenes.example_area_lights()
-    elif kind == "config1_tiny":
-        sd, cam = scenes.config1(subdivisions=2, texture_size=32)
+    elif kind == "mesh_tiny":
+        sd, cam = scenes.mesh_scene(subdivisions=2, texture_size=32)
         H.blas_sah(sd.meshes[0], which)
-    elif kind == "config2_256":
-        sd, cam = scenes.config2(count=256)
+    elif kind == "moving256":
+        sd, cam = scenes.moving_scene(count=256)
     else:
         raise ValueError(kind)
     H.tlas_sah(sd, which)
@@ -72,7 +72,7 @@ def main():
                                 "float_sha256": sha(fr.float_pixels),
                                 "tlas_sha256": sha(sd.tlas_nodes[:sd.tlas_node_count])}
         frames[name] = np.stack([fr.pixels["R"], fr.pixels["G"], fr.pixels["B"]], -1).reshape(h, w, 3)
-    for kind in ("config0", "config2_256"):
+    for kind in ("implicit16", "moving256"):
         sd, _ = make_scene(kind, "ref")
         out["tlas"][kind] = {"node_count": int(sd.tlas_node_count), "height": int(sd.tlas_height),
                              "nodes_sha256": sha(sd.tlas_nodes[:sd.tlas_node_count]),

@@ -107,10 +107,10 @@ def assert_parity(m, mode, id_min=0.9999, u8_min=0.999, rel_min=0.999):
         assert m["u8_within1"] >= u8_min, m
 
 
-def small_config1(subdivisions=3, texture_size=64, blas="orc"):
-    """config1 at test scale: a small displaced icosphere, 64^2 textures, the same 8 instances,
+def small_mesh_scene(subdivisions=3, texture_size=64, blas="orc"):
+    """The mesh scene at test scale: a small displaced icosphere, 64^2 textures, the same 8 instances,
     materials and emissive quads."""
-    sd, cam = scenes.config1(subdivisions=subdivisions, texture_size=texture_size)
+    sd, cam = scenes.mesh_scene(subdivisions=subdivisions, texture_size=texture_size)
     if blas in ("orc", "ref"):
         blas_sah(sd.meshes[0], blas)
     return sd, cam
@@ -164,17 +164,17 @@ def overlay_frame(sd, cam, w, h, what, which="orc", depth=1, mode=S.RM_BEAUTY):
 
 
 def overlay_scene(which):
-    """Scenes of the overlay tests: config0, the area-light example, config1 at test scale (reference
+    """Scenes of the overlay tests: the 16-primitive scene, the area-light example, the mesh scene at test scale (reference
     BLAS), cameras inside them (edges cut by the near and side planes), and 384 primitives (a TLAS
     past the reference's 255-node drawBVH limit)."""
-    if which in ("config0", "inside"):
-        sd, cam = scenes.config0()
+    if which in ("implicit16", "inside"):
+        sd, cam = scenes.implicit16_scene()
     elif which == "area":
         sd, cam = scenes.example_area_lights()
-    elif which == "config2":
-        sd, cam = scenes.config2(count=384, spread=6.0)
+    elif which == "moving":
+        sd, cam = scenes.moving_scene(count=384, spread=6.0)
     else:
-        sd, cam = small_config1(subdivisions=3, texture_size=64, blas="ref" if oracle.reference_available() else "orc")
+        sd, cam = small_mesh_scene(subdivisions=3, texture_size=64, blas="ref" if oracle.reference_available() else "orc")
     if which == "inside":
         cam = scenes.CameraSpec((0.5, 0.3, -1.0), 0.4, 0.2, 2.0)
     elif which == "inside_mesh":

@@ -34,17 +34,17 @@ def _frames(lib, sd, cam, w, h, depth, mode):
     return out
 
 
-@pytest.mark.parametrize("which,mode", [("config0", S.RM_BEAUTY), ("config0", S.RM_NORMALS), ("area", S.RM_BEAUTY),
-                                        ("config1", S.RM_BEAUTY), ("config1", S.RM_UVS)])
+@pytest.mark.parametrize("which,mode", [("implicit16", S.RM_BEAUTY), ("implicit16", S.RM_NORMALS), ("area", S.RM_BEAUTY),
+                                        ("mesh", S.RM_BEAUTY), ("mesh", S.RM_UVS)])
 def test_dropin_host_gpu_equals_its_cpu(dropin, which, mode):
-    if which == "config0":
-        sd, cam = scenes.config0()
+    if which == "implicit16":
+        sd, cam = scenes.implicit16_scene()
         depth = 2
     elif which == "area":
         sd, cam = scenes.example_area_lights()
         depth = 2
     else:
-        sd, cam = H.small_config1(subdivisions=3, texture_size=64, blas="ref")
+        sd, cam = H.small_mesh_scene(subdivisions=3, texture_size=64, blas="ref")
         depth = 4
     gpu, cpu = _frames(dropin, sd, cam, 320, 240, depth, mode)
     m = H.compare(gpu, cpu, mode)

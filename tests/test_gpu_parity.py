@@ -14,14 +14,14 @@ MODES = [S.RM_BEAUTY, S.RM_DEPTH, S.RM_NORMALS, S.RM_UVS]
 
 
 @pytest.mark.parametrize("mode", MODES)
-def test_config0_all_modes(renderer, mode):
-    sd, cam = scenes.config0()
+def test_implicit16_all_modes(renderer, mode):
+    sd, cam = scenes.implicit16_scene()
     H.tlas_sah(sd)
     renderer.upload(0, sd, tlas="host")
     g = H.gpu_frame(renderer, 0, sd, cam, 640, 480, depth=2, mode=mode)
     o = H.oracle_frame(sd, cam, 640, 480, depth=2, mode=mode)
     m = H.compare(g, o, mode)
-    print("config0", mode, m)
+    print("implicit16", mode, m)
     H.assert_parity(m, mode)
     if mode != S.RM_BEAUTY:
         # no libm call on these paths: every byte equals the oracle's
@@ -43,22 +43,22 @@ def test_point_and_area_lights(renderer, depth):
 
 
 @pytest.mark.parametrize("mode", [S.RM_BEAUTY, S.RM_NORMALS, S.RM_UVS])
-def test_config1_small_reference_blas(renderer, mode):
+def test_mesh_scene_small_reference_blas(renderer, mode):
     """Meshes, Cook-Torrance, glass and mirror bounces, textures, emissive quads, BLAS from the
     reference's SAH builder."""
-    sd, cam = H.small_config1(subdivisions=3, texture_size=64, blas="orc")
+    sd, cam = H.small_mesh_scene(subdivisions=3, texture_size=64, blas="orc")
     H.tlas_sah(sd)
     renderer.upload(2, sd, tlas="host")
     g = H.gpu_frame(renderer, 2, sd, cam, 320, 180, depth=4, mode=mode)
     o = H.oracle_frame(sd, cam, 320, 180, depth=4, mode=mode)
     m = H.compare(g, o, mode)
-    print("config1-small", mode, m)
+    print("mesh-small", mode, m)
     H.assert_parity(m, mode)
 
 
 def test_counters_match_oracle(renderer):
     """Same traversal, same work: every event counter equals the oracle's."""
-    sd, cam = H.small_config1(subdivisions=2, texture_size=32, blas="orc")
+    sd, cam = H.small_mesh_scene(subdivisions=2, texture_size=32, blas="orc")
     H.tlas_sah(sd)
     renderer.upload(3, sd, tlas="host")
     g = H.gpu_frame(renderer, 3, sd, cam, 160, 90, depth=4, counters=True)
@@ -73,16 +73,16 @@ def test_counters_match_oracle(renderer):
     assert np.array_equal(g.counters[:10], o.counters[:10]), (g.counters[:10], o.counters[:10])
 
 
-def test_config2_primary_tlas(renderer):
+def test_moving_scene_primary_tlas(renderer):
     """Hundreds of primitives: primary rays walk the TLAS with the SSB cull instead of the
     reference's brute-force loop; results must not change."""
-    sd, cam = scenes.config2(count=384, spread=6.0)
+    sd, cam = scenes.moving_scene(count=384, spread=6.0)
     H.tlas_sah(sd)
     renderer.upload(4, sd, tlas="host")
     g = H.gpu_frame(renderer, 4, sd, cam, 320, 180, depth=2)
     o = H.oracle_frame(sd, cam, 320, 180, depth=2)
     m = H.compare(g, o, S.RM_BEAUTY)
-    print("config2-384", m)
+    print("moving-384", m)
     H.assert_parity(m, S.RM_BEAUTY)
 
 
@@ -90,7 +90,7 @@ def test_lbvh_tlas_bit_exact(renderer):
     """The device LBVH30 TLAS: node array, leaf order and height equal the oracle's specification."""
     orc = oracle.restatement()
     for count in (2, 3, 16, 384, 4096):
-        sd, cam = scenes.config2(count=count)
+        sd, cam = scenes.moving_scene(count=count)
         renderer.upload(5, sd, tlas=None)
         renderer.build_tlas(5, sd, api.ST_BVH_LBVH30)
         sc, keep = sd.to_ctypes()
@@ -113,7 +113,7 @@ def test_lbvh_tlas_bit_exact(renderer):
 def test_render_with_lbvh_tlas(renderer):
     """Any-hit shadow rays take the first occluder found, so with a different TLAS the oracle is
     given the same (device-built) TLAS."""
-    sd, cam = scenes.config0()
+    sd, cam = scenes.implicit16_scene()
     renderer.upload(6, sd, tlas=None)
     renderer.build_tlas(6, sd, api.ST_BVH_LBVH30)
     g = H.gpu_frame(renderer, 6, sd, cam, 320, 240, depth=2)
@@ -141,7 +141,7 @@ def test_blas_lbvh_triangle_records(renderer):
 
 
 def test_render_with_lbvh_blas(renderer):
-    sd, cam = H.small_config1(subdivisions=3, texture_size=64, blas=None)
+    sd, cam = H.small_mesh_scene(subdivisions=3, texture_size=64, blas=None)
     renderer.build_blas(sd.meshes[0])
     H.tlas_sah(sd)
     renderer.upload(7, sd, tlas="host")
@@ -152,10 +152,10 @@ def test_render_with_lbvh_blas(renderer):
 
 
 def test_refit_after_motion(renderer):
-    sd, cam = scenes.config2(count=256)
+    sd, cam = scenes.moving_scene(count=256)
     renderer.upload(8, sd, tlas=None)
     renderer.build_tlas(8, sd, api.ST_BVH_LBVH30)
-    scenes.advance_config2(sd, 3)
+    scenes.advance_moving_scene(sd, 3)
     renderer.update_primitives(8, sd.primitives, np.arange(256))
     renderer.build_tlas(8, sd, api.ST_BVH_REFIT)
     # every leaf box contains its primitives' boxes and every parent contains its children
@@ -225,13 +225,13 @@ def test_binned_sah_bit_exact(renderer, n, max_leaf):
 
 def test_binned_sah_tlas_and_blas_render(renderer):
     """A binned-SAH TLAS (4096 moving primitives) and BLAS render like the oracle given the same BVHs."""
-    sd, cam = scenes.config2(count=1024)
+    sd, cam = scenes.moving_scene(count=1024)
     renderer.upload(9, sd, tlas=None)
     renderer.build_tlas(9, sd, api.ST_BVH_BINNED_SAH)
     g = H.gpu_frame(renderer, 9, sd, cam, 256, 144, depth=2)
     o = H.oracle_frame(sd, cam, 256, 144, depth=2)
     H.assert_parity(H.compare(g, o, S.RM_BEAUTY), S.RM_BEAUTY)
-    sd1, cam1 = H.small_config1(subdivisions=3, texture_size=64, blas=None)
+    sd1, cam1 = H.small_mesh_scene(subdivisions=3, texture_size=64, blas=None)
     renderer.build_blas(sd1.meshes[0], api.ST_BVH_BINNED_SAH)
     renderer.upload(10, sd1, tlas=None)
     renderer.build_tlas(10, sd1, api.ST_BVH_BINNED_SAH)
@@ -244,13 +244,13 @@ def test_batch_equals_per_frame_renders(renderer):
     """st_render_batch over views of different scenes, sizes, modes and bounce counts: every view's
     float grid and u8 frame equal the per-frame render's, for every tile shape, with and without
     the CUDA graph (the second graph call replays the captured graph)."""
-    c0, cam0 = scenes.config0()
+    c0, cam0 = scenes.implicit16_scene()
     H.tlas_sah(c0)
     renderer.upload(11, c0, tlas="host")
-    c1, cam1 = H.small_config1(subdivisions=3, texture_size=64, blas="orc")
+    c1, cam1 = H.small_mesh_scene(subdivisions=3, texture_size=64, blas="orc")
     H.tlas_sah(c1)
     renderer.upload(12, c1, tlas="host")
-    c2, cam2 = scenes.config2(count=300)
+    c2, cam2 = scenes.moving_scene(count=300)
     H.tlas_sah(c2)
     renderer.upload(13, c2, tlas="host")
     specs = [(11, c0, cam0, 96, 64, 2, S.RM_BEAUTY), (12, c1, cam1, 160, 90, 4, S.RM_BEAUTY),
@@ -285,7 +285,7 @@ def test_pinned_host_outputs_written_by_the_kernels(renderer):
     """Page-locked host buffers are written by the trace and resolve kernels directly (no copy after
     the trace); the frame equals the one rendered into pageable buffers."""
     import torch
-    c1, cam1 = H.small_config1(subdivisions=3, texture_size=64, blas="orc")
+    c1, cam1 = H.small_mesh_scene(subdivisions=3, texture_size=64, blas="orc")
     H.tlas_sah(c1)
     renderer.upload(14, c1, tlas="host")
     pageable = scenes.Frame(320, 180, cam1, depth=4)
@@ -300,14 +300,14 @@ def test_pinned_host_outputs_written_by_the_kernels(renderer):
     assert np.array_equal(pu.numpy(), pageable.pixels.view(np.uint8))
 
 
-@pytest.mark.parametrize("which", ["config0", "config1"])
+@pytest.mark.parametrize("which", ["implicit16", "mesh"])
 def test_pick_equals_oracle(renderer, which):
     """st_pick (manipulateSelection's picking ray on the device) equals the oracle's pick bit for bit
     on scattered pixels and on pixels whose ray hits a light's glow sphere."""
-    if which == "config0":
-        sd, cam = scenes.config0()
+    if which == "implicit16":
+        sd, cam = scenes.implicit16_scene()
     else:
-        sd, cam = H.small_config1(subdivisions=3, texture_size=64, blas="orc")
+        sd, cam = H.small_mesh_scene(subdivisions=3, texture_size=64, blas="orc")
     H.tlas_sah(sd)
     renderer.upload(15, sd, tlas="host")
     w, h = 160, 120
@@ -321,12 +321,12 @@ def test_pick_equals_oracle(renderer, which):
     assert any(k[0] for k in dev)
 
 
-@pytest.mark.parametrize("which", ["config0", "area", "config1", "inside", "inside_mesh", "config2"])
+@pytest.mark.parametrize("which", ["implicit16", "area", "mesh", "inside", "inside_mesh", "moving"])
 @pytest.mark.parametrize("what", [1, 2, 3])
 def test_overlays_equal_oracle(renderer, which, what):
     """drawBVH / drawSSB (render/raytracer.h:46, render/SSB.h:175) drawn by the device over a
     byte-exact render (normals mode): the float grid equals the oracle's overlaid grid byte for
-    byte.  config2 has 384 primitives, a TLAS past the reference's 255-node drawBVH limit."""
+    byte.  "moving" has 384 primitives, a TLAS past the reference's 255-node drawBVH limit."""
     sd, cam = H.overlay_scene(which)
     H.tlas_sah(sd)
     renderer.upload(4, sd, tlas="host")
@@ -343,7 +343,7 @@ def test_overlays_over_beauty_add_no_difference(renderer):
     """Over a beauty render (within tolerance of the oracle, not byte-exact), the overlays add no
     difference of their own: every pixel where the overlaid grids differ already differs without
     the overlays."""
-    sd, cam = H.overlay_scene("config1")
+    sd, cam = H.overlay_scene("mesh")
     H.tlas_sah(sd)
     renderer.upload(4, sd, tlas="host")
     g0 = H.gpu_frame(renderer, 4, sd, cam, 320, 180, depth=4)
@@ -359,7 +359,7 @@ def test_overlays_over_beauty_add_no_difference(renderer):
 def test_render_scene_draws_overlays_from_viewport_settings(renderer):
     """st_render_scene draws drawBVH / drawSSB when viewport->settings.show_BVH / show_SSB are set,
     as st_render_ex does with the overlay bits."""
-    sd, cam = H.overlay_scene("config0")
+    sd, cam = H.overlay_scene("implicit16")
     H.tlas_sah(sd)
     renderer.upload(4, sd, tlas="host")
     a = H.gpu_frame(renderer, 4, sd, cam, 200, 150, depth=1, mode=S.RM_NORMALS, overlays=3)
@@ -375,10 +375,10 @@ def test_render_scene_draws_overlays_from_viewport_settings(renderer):
 def test_graph_replay_follows_new_views(renderer):
     """A batch replayed through its CUDA graph with the same shapes but other cameras renders the
     new views: every launch parameter (view tables, cameras, outputs) comes from the call."""
-    c0, cam0 = scenes.config0()
+    c0, cam0 = scenes.implicit16_scene()
     H.tlas_sah(c0)
     renderer.upload(13, c0, tlas="host")
-    c1, cam1 = H.small_config1(subdivisions=3, texture_size=64, blas="orc")
+    c1, cam1 = H.small_mesh_scene(subdivisions=3, texture_size=64, blas="orc")
     H.tlas_sah(c1)
     renderer.upload(14, c1, tlas="host")
     rng = np.random.default_rng(5)
@@ -398,7 +398,7 @@ def test_graph_replay_follows_new_views(renderer):
 def test_batch_larger_than_one_view_table(renderer):
     """More views than one launch's view table holds (64): the batch runs as several launches and
     every view equals its single render."""
-    c0, cam0 = scenes.config0()
+    c0, cam0 = scenes.implicit16_scene()
     H.tlas_sah(c0)
     renderer.upload(15, c0, tlas="host")
     rng = np.random.default_rng(9)

@@ -13,11 +13,11 @@ REFIT_FRACTION = 0.25
 
 
 def _scenes():
-    c0, cam0 = scenes.config0()
+    c0, cam0 = scenes.implicit16_scene()
     H.tlas_sah(c0)
-    c1, cam1 = H.small_config1(subdivisions=3, texture_size=64, blas="orc")
+    c1, cam1 = H.small_mesh_scene(subdivisions=3, texture_size=64, blas="orc")
     H.tlas_sah(c1)
-    c2, cam2 = scenes.config2(count=300)
+    c2, cam2 = scenes.moving_scene(count=300)
     return [(c0, cam0, "host"), (c1, cam1, "host"), (c2, cam2, "lbvh")]
 
 
@@ -50,7 +50,7 @@ def test_served_views_equal_views_rendered_alone():
         if moved is None:
             updates.append(None)
         else:
-            scenes.advance_config2(motion, 1)
+            scenes.advance_moving_scene(motion, 1)
             updates.append(motion.primitives[moved].copy())
 
     served = api.Renderer(device=0)
@@ -97,7 +97,7 @@ def test_served_views_equal_views_rendered_alone():
 
 
 def test_request_over_frame_budget_is_refused():
-    sd, cam = scenes.config0()
+    sd, cam = scenes.implicit16_scene()
     H.tlas_sah(sd)
     r = api.Renderer(device=0)
     try:
@@ -117,7 +117,7 @@ def test_served_views_into_page_locked_buffers():
     """Requests whose output frames are page-locked are resolved straight into them (no staging);
     each equals the same view rendered alone."""
     import torch
-    sd, cam = scenes.config0()
+    sd, cam = scenes.implicit16_scene()
     H.tlas_sah(sd)
     r = api.Renderer(device=0)
     try:

@@ -18,7 +18,7 @@ needs_ref = pytest.mark.skipif(not oracle.reference_available(), reason="referen
 
 def _mesh():
     """A small displaced icosphere with its BLAS (the oracle's SAH) and a few edges."""
-    sd, cam = scenes.config1(subdivisions=2, texture_size=8)
+    sd, cam = scenes.mesh_scene(subdivisions=2, texture_size=8)
     md = sd.meshes[0]
     H.blas_sah(md, "orc")
     keep = []
@@ -187,8 +187,8 @@ def test_texture_file_matches_bmp2texture(tmp_path, w, h, wrap, mip):
 
 
 def _scene_file_scene():
-    """config0 with its camera (a scene file holds settings, cameras and primitives)."""
-    sd, spec = scenes.config0()
+    """The 16-primitive scene with its camera (a scene file holds settings, cameras and primitives)."""
+    sd, spec = scenes.implicit16_scene()
     sc, keep = sd.to_ctypes()
     cams = (S.Camera * 1)()
     scenes.fill_camera(cams[0], spec)

@@ -34,22 +34,22 @@ def test_oracle_reproduces_golden_renders(name):
 
 
 @needs_ref
-@pytest.mark.parametrize("case", ["config0", "area", "config1_small", "config2_320"])
+@pytest.mark.parametrize("case", ["implicit16", "area", "mesh_small", "moving320"])
 @pytest.mark.parametrize("mode", [S.RM_BEAUTY, S.RM_NORMALS])
 def test_oracle_matches_reference_live(case, mode):
     """Larger renders than the fixtures, oracle vs the reference run here, every byte equal."""
-    if case == "config0":
-        sd, cam = scenes.config0()
+    if case == "implicit16":
+        sd, cam = scenes.implicit16_scene()
         w, h, depth = 320, 240, 2
     elif case == "area":
         sd, cam = scenes.example_area_lights()
         w, h, depth = 240, 180, 4
-    elif case == "config1_small":
-        sd, cam = scenes.config1(subdivisions=3, texture_size=64)
+    elif case == "mesh_small":
+        sd, cam = scenes.mesh_scene(subdivisions=3, texture_size=64)
         H.blas_sah(sd.meshes[0], "ref")
         w, h, depth = 192, 108, 4
     else:
-        sd, cam = scenes.config2(count=320)
+        sd, cam = scenes.moving_scene(count=320)
         w, h, depth = 128, 72, 2
     H.tlas_sah(sd, "ref")
     r = H.reference_frame(sd, cam, w, h, depth=depth, mode=mode)
@@ -147,7 +147,7 @@ def test_projection_plane_matches_reference():
 @needs_ref
 def test_ssb_matches_reference():
     ref, orc = oracle.reference(), oracle.restatement()
-    for sd, cam in (scenes.config0(), scenes.config2(count=512), scenes.config1(subdivisions=1, texture_size=8)):
+    for sd, cam in (scenes.implicit16_scene(), scenes.moving_scene(count=512), scenes.mesh_scene(subdivisions=1, texture_size=8)):
         for w, h in ((640, 480), (320, 180)):
             a, b = sd.copy(), sd.copy()
             sa, ka = a.to_ctypes()
@@ -218,19 +218,19 @@ def test_bvh_oracle_structure(n, max_leaf, builder):
     assert height == max(depth_max, 1)
 
 
-@pytest.mark.parametrize("which", ["config0", "area", "config1"])
+@pytest.mark.parametrize("which", ["implicit16", "area", "mesh"])
 def test_pick_matches_reference(which):
     """manipulateSelection's picking ray (viewport/manipulation.h:55-123): the oracle's pick equals
     the reference's own hitPrimitives + glow-sphere sequence bit for bit, on scattered pixels and on
     pixels that hit a light."""
     if not oracle.reference_available():
         pytest.skip("reference harness not built")
-    if which == "config0":
-        sd, cam = scenes.config0()
+    if which == "implicit16":
+        sd, cam = scenes.implicit16_scene()
     elif which == "area":
         sd, cam = scenes.example_area_lights()
     else:
-        sd, cam = H.small_config1(subdivisions=3, texture_size=64, blas="ref")
+        sd, cam = H.small_mesh_scene(subdivisions=3, texture_size=64, blas="ref")
     H.tlas_sah(sd, "ref")
     w, h = 160, 120
     rng = np.random.default_rng(11)
@@ -241,7 +241,7 @@ def test_pick_matches_reference(which):
     b = [H.pick_key(r) for r in H.picks(sd, cam, w, h, coords, "ref")]
     assert a == b
     assert any(k[0] for k in a)
-    if which == "config0":
+    if which == "implicit16":
         assert any(k[1] == 6 for k in a), "no pixel hit a light"
 
 
@@ -251,7 +251,7 @@ def test_projection_matrix_matches_begin_drawing():
     if not oracle.reference_available():
         pytest.skip("reference harness not built")
     ref = oracle.reference()
-    sd, cam = scenes.config0()
+    sd, cam = scenes.implicit16_scene()
     for cube in (0, 1):
         fr = scenes.Frame(200, 150, cam, with_pixels=False)
         fr.viewport.settings.use_cube_NDC = cube
@@ -261,7 +261,7 @@ def test_projection_matrix_matches_begin_drawing():
         assert bytes(fr.viewport.projection_matrix) == mine
 
 
-@pytest.mark.parametrize("which", ["config0", "area", "config1", "inside", "inside_mesh"])
+@pytest.mark.parametrize("which", ["implicit16", "area", "mesh", "inside", "inside_mesh"])
 def test_overlays_match_reference(which):
     """drawBVH and drawSSB (render/raytracer.h:46, render/SSB.h:175): the oracle's overlays leave
     the float grid byte-identical to the reference's own drawing over the same render, for the
@@ -284,7 +284,7 @@ def test_overlays_far_plane_matches_reference():
     shapes/edge.h:23-29): the oracle still equals the reference's own drawing."""
     if not oracle.reference_available():
         pytest.skip("reference harness not built")
-    sd, cam = H.overlay_scene("config0")
+    sd, cam = H.overlay_scene("implicit16")
     H.tlas_sah(sd, "ref")
     out = {}
     for which in ("orc", "ref"):
