@@ -413,3 +413,31 @@ def test_batch_larger_than_one_view_table(renderer):
     for a, b in zip(frames, singles):
         assert np.array_equal(a.float_pixels.view(np.uint8), b.float_pixels.view(np.uint8))
         assert np.array_equal(a.pixels.view(np.uint8), b.pixels.view(np.uint8))
+
+
+@pytest.mark.parametrize("w,h", [(1, 1), (2, 3), (33, 17), (127, 65)])
+def test_ragged_viewports(renderer, w, h):
+    """Grids that fill no whole block or tile: every edge lane traces the right point, none past it."""
+    sd, cam = scenes.implicit16_scene()
+    H.tlas_sah(sd)
+    renderer.upload(0, sd, tlas="host")
+    for mode in (S.RM_NORMALS, S.RM_BEAUTY):
+        g = H.gpu_frame(renderer, 0, sd, cam, w, h, depth=2, mode=mode)
+        o = H.oracle_frame(sd, cam, w, h, depth=2, mode=mode)
+        m = H.compare(g, o, mode)
+        H.assert_parity(m, mode)
+        if mode != S.RM_BEAUTY:
+            assert m["exact"] == 1.0, (w, h, m)
+
+
+def test_camera_facing_away_misses_everything(renderer):
+    """A view with no hit: every grid point keeps the background and infinite depth, as the oracle's."""
+    sd, _ = scenes.implicit16_scene()
+    H.tlas_sah(sd)
+    renderer.upload(0, sd, tlas="host")
+    cam = scenes.CameraSpec((0.0, 0.0, -15.0), float(np.pi), 0.0, 2.0)
+    g = H.gpu_frame(renderer, 0, sd, cam, 64, 48, depth=3)
+    o = H.oracle_frame(sd, cam, 64, 48, depth=3)
+    assert not np.isfinite(g.float_pixels["depth"]).any()
+    assert g.float_pixels.tobytes() == o.float_pixels.tobytes()
+    assert g.pixels.tobytes() == o.pixels.tobytes()
