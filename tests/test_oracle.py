@@ -58,6 +58,20 @@ def test_oracle_matches_reference_live(case, mode):
     assert np.array_equal(r.pixels.view(np.uint8).reshape(-1, 4)[:, :3], o.pixels.view(np.uint8).reshape(-1, 4)[:, :3])
 
 
+@needs_ref
+@pytest.mark.parametrize("w,h,yaw", [(1, 1, 0.0), (2, 3, 0.0), (33, 17, 0.0), (127, 65, 0.0), (64, 48, float(np.pi))])
+def test_oracle_matches_reference_ragged_and_empty_views(w, h, yaw):
+    """Grids smaller than a block or tile, and a camera facing away from every primitive."""
+    sd, cam = scenes.implicit16_scene()
+    cam = scenes.CameraSpec(cam.position, yaw, cam.pitch, cam.focal_length)
+    H.tlas_sah(sd, "ref")
+    for mode in (S.RM_BEAUTY, S.RM_NORMALS):
+        r = H.reference_frame(sd, cam, w, h, depth=3, mode=mode)
+        o = H.oracle_frame(sd, cam, w, h, depth=3, mode=mode)
+        assert np.array_equal(r.float_pixels.view(np.uint8), o.float_pixels.view(np.uint8)), (w, h, yaw, mode)
+        assert np.array_equal(r.pixels.view(np.uint8), o.pixels.view(np.uint8)), (w, h, yaw, mode)
+
+
 @pytest.mark.parametrize("kind", sorted(GOLDEN["tlas"]))
 def test_sah_tlas_matches_golden(kind):
     g = GOLDEN["tlas"][kind]
