@@ -176,6 +176,13 @@ ST_API int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewpor
                  st_render_options *options);
 
 /* ---- batched views: many views of resident scenes in one call ------------------------------------ */
+/* How a batch's views are launched (st_batch_options.launch_mode, st_serve_config.launch_mode). */
+enum st_launch_mode {
+    ST_LAUNCH_AUTOTUNED = -1,   /* st_render_batch only: timed per scene class and cached */
+    ST_LAUNCH_PER_VIEW = 0,     /* one trace kernel per view, the views on concurrent streams */
+    ST_LAUNCH_PERSISTENT = 1    /* one persistent kernel over a shared tile queue */
+};
+
 typedef struct st_view {
     int slot;                   /* resident scene */
     const Scene *scene;         /* per-frame values (ambient light); NULL -> the uploaded ones */
@@ -197,9 +204,10 @@ typedef struct st_batch_options {
     int stack_placement;        /* -1: autotuned; 0: traversal stacks in local memory; 1: their first 16
                                    entries in shared memory (the traversal is the same either way) */
     int stack_placement_used;   /* out */
-    int launch_mode;            /* -1: autotuned; 0: one persistent kernel over a shared tile queue; 1: one
-                                   trace kernel per view, the views on concurrent streams */
-    int launch_mode_used;       /* out (with launch mode 1, tile_shape_used and stack_placement_used are -1) */
+    int launch_mode;            /* st_launch_mode: ST_LAUNCH_AUTOTUNED (-1), ST_LAUNCH_PER_VIEW (0) or
+                                   ST_LAUNCH_PERSISTENT (1); tile_shape, chunk and stack_placement apply to
+                                   the persistent kernel */
+    int launch_mode_used;       /* out (per view: tile_shape_used and stack_placement_used are -1) */
 } st_batch_options;
 
 /* Render `view_count` views (different sizes, scenes, render modes and bounce counts) in one call:
@@ -262,8 +270,8 @@ typedef struct st_serve_config {
     int tile_shape, chunk;      /* -1 / 0: the autotuned choice for the scene class, else 8x4 and 1 */
     double refit_fraction;      /* primitives moved since the scene's last full TLAS build, as a fraction of
                                    all, below which the TLAS is refit, else rebuilt (LBVH30); 0 -> 0.25 */
-    int launch_mode;            /* 0: one trace kernel per view on concurrent streams; 1: one persistent
-                                   kernel over a shared tile queue (tile_shape and chunk apply) */
+    int launch_mode;            /* st_launch_mode: ST_LAUNCH_PER_VIEW (0) or ST_LAUNCH_PERSISTENT (1; tile_shape
+                                   and chunk apply) */
 } st_serve_config;
 
 typedef struct st_request {

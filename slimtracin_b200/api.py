@@ -35,6 +35,7 @@ class st_render_options(C.Structure):
 
 
 OVERLAY_BVH, OVERLAY_SSB = 1, 2     # enum st_overlay
+LAUNCH_AUTOTUNED, LAUNCH_PER_VIEW, LAUNCH_PERSISTENT = -1, 0, 1   # enum st_launch_mode
 
 
 class st_view(C.Structure):
@@ -268,7 +269,7 @@ class Renderer:
 
 
 def render_batch(renderer, items, tile_shape=-1, chunk=0, use_graph=False, device_outputs=False, stack_placement=-1,
-                 launch_mode=-1):
+                 launch_mode=LAUNCH_AUTOTUNED):
     """st_render_batch over items = [(slot, SceneData, Frame)]; outputs go to each Frame's buffers
     (host) unless device_outputs, in which case Frame.grid pointers are used as device pointers."""
     keep = []
@@ -299,7 +300,7 @@ class Server:
     the Renderer takes no other calls."""
 
     def __init__(self, renderer, max_in_flight=3, max_views_per_batch=64, frame_budget=0, tile_shape=-1, chunk=0,
-                 refit_fraction=0.25, launch_mode=0):
+                 refit_fraction=0.25, launch_mode=LAUNCH_PER_VIEW):
         self.r = renderer
         self.L = renderer.L
         cfg = st_serve_config(max_in_flight, max_views_per_batch, frame_budget, tile_shape, chunk, refit_fraction,

@@ -1284,27 +1284,29 @@ int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *
     memset(&dflt, 0, sizeof(dflt));
     dflt.tile_shape = -1;
     dflt.stack_placement = -1;
-    dflt.launch_mode = -1;
+    dflt.launch_mode = ST_LAUNCH_AUTOTUNED;
     st_batch_options &o = opt ? *opt : dflt;
     cudaStream_t st = o.stream ? (cudaStream_t)o.stream : ctx->stream;
     BatchState &B = ctx->batch;
     // the kernel variant (tile shape, stack placement) and queue chunk: given, cached for this scene
     // class, or tuned now
-    if (o.tile_shape >= TILE_SHAPES || o.stack_placement >= STACK_PLACEMENTS || o.launch_mode > 1) return ST_ERR_INVALID_ARG;
+    if (o.tile_shape >= TILE_SHAPES || o.stack_placement >= STACK_PLACEMENTS || o.launch_mode < ST_LAUNCH_AUTOTUNED ||
+        o.launch_mode > ST_LAUNCH_PERSISTENT)
+        return ST_ERR_INVALID_ARG;
     BatchPlan p;
-    // launch mode 1 (one kernel per view) has no tile shape, stack placement or chunk to choose; mode
-    // 0 with every knob given needs no tuning; otherwise the choice is cached per scene class or tuned
+    // one kernel per view has no tile shape, stack placement or chunk to choose; the persistent kernel
+    // with every knob given needs no tuning; otherwise the choice is cached per scene class or tuned
     const bool fixed_tile = o.tile_shape >= 0 || o.stack_placement >= 0;
-    int tile = o.launch_mode == 1 ? kPerViewVariant
+    int tile = o.launch_mode == ST_LAUNCH_PER_VIEW ? kPerViewVariant
                : (o.tile_shape >= 0 && o.stack_placement >= 0) ? o.tile_shape + TILE_SHAPES * o.stack_placement : -1;
-    u32t chunk = o.launch_mode == 1 ? 1u : o.chunk > 0 ? (u32t)o.chunk : 0;
+    u32t chunk = o.launch_mode == ST_LAUNCH_PER_VIEW ? 1u : o.chunk > 0 ? (u32t)o.chunk : 0;
     ST_TRY(plan_batch(ctx, views, n, o.tile_shape >= 0 ? o.tile_shape : 0, o, p));
     if (tile < 0 || chunk == 0) {
         auto it = B.tuned.find(p.class_key);
         const bool per_view = it != B.tuned.end() && it->second.first == kPerViewVariant;
         const bool fits = it != B.tuned.end() &&
-                          (per_view ? (o.launch_mode != 0 && !fixed_tile && !o.chunk)
-                                    : (o.launch_mode != 1 &&
+                          (per_view ? (o.launch_mode != ST_LAUNCH_PERSISTENT && !fixed_tile && !o.chunk)
+                                    : (o.launch_mode != ST_LAUNCH_PER_VIEW &&
                                        (o.tile_shape < 0 || variant_tile(it->second.first) == o.tile_shape) &&
                                        (o.stack_placement < 0 || variant_stack(it->second.first) == o.stack_placement)));
         if (fits) {
@@ -1396,7 +1398,7 @@ int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *
     ST_CUDA(cudaStreamSynchronize(st));
     cudaEventElapsedTime(&o.batch_ms, ctx->ev[0], ctx->ev[1]);
     o.rays = p.rays;
-    o.launch_mode_used = tile == kPerViewVariant ? 1 : 0;
+    o.launch_mode_used = tile == kPerViewVariant ? ST_LAUNCH_PER_VIEW : ST_LAUNCH_PERSISTENT;
     o.tile_shape_used = tile == kPerViewVariant ? -1 : variant_tile(tile);
     o.stack_placement_used = tile == kPerViewVariant ? -1 : variant_stack(tile);
     o.chunk_used = (int)chunk;
@@ -1759,7 +1761,7 @@ int launch_flight(st_ctx *ctx, int f, std::vector<std::shared_ptr<ServeReq>> &re
     // view table and arena layout
     const int n = (int)reqs.size();
     BatchPlan p;
-    int tile = V.cfg.launch_mode == 0 ? kPerViewVariant : V.cfg.tile_shape >= 0 ? V.cfg.tile_shape : TILE_8x4;
+    int tile = V.cfg.launch_mode == ST_LAUNCH_PER_VIEW ? kPerViewVariant : V.cfg.tile_shape >= 0 ? V.cfg.tile_shape : TILE_8x4;
     u32t chunk = V.cfg.chunk > 0 ? (u32t)V.cfg.chunk : 1;
     std::ostringstream cls;
     size_t dev = 0, host = 64;
@@ -1773,7 +1775,7 @@ int launch_flight(st_ctx *ctx, int f, std::vector<std::shared_ptr<ServeReq>> &re
         for (u32t x = tris; x > 1; x >>= 1) tb++;
         cls << "p" << pb << "t" << tb << "d" << r->view.depth << ";";
     }
-    if (V.cfg.launch_mode != 0 && (V.cfg.tile_shape < 0 || V.cfg.chunk <= 0)) {
+    if (V.cfg.launch_mode == ST_LAUNCH_PERSISTENT && (V.cfg.tile_shape < 0 || V.cfg.chunk <= 0)) {
         auto it = ctx->batch.tuned.find(cls.str());
         if (it != ctx->batch.tuned.end() && it->second.first != kPerViewVariant) {
             if (V.cfg.tile_shape < 0) tile = it->second.first;
@@ -1917,7 +1919,7 @@ int st_serve_start(st_ctx *ctx, const st_serve_config *cfg) {
     if (V.cfg.max_views_per_batch <= 0) V.cfg.max_views_per_batch = 64;
     if (V.cfg.refit_fraction <= 0) V.cfg.refit_fraction = 0.25;
     if (!cfg) { V.cfg.tile_shape = -1; V.cfg.chunk = 0; }
-    if (V.cfg.launch_mode < 0 || V.cfg.launch_mode > 1) return ST_ERR_INVALID_ARG;
+    if (V.cfg.launch_mode != ST_LAUNCH_PER_VIEW && V.cfg.launch_mode != ST_LAUNCH_PERSISTENT) return ST_ERR_INVALID_ARG;
     V.frame_budget = V.cfg.frame_budget ? V.cfg.frame_budget
                                         : (ctx->budget > ctx->in_use ? ctx->budget - ctx->in_use : 0);
     V.flights.resize(V.cfg.max_in_flight);

@@ -134,7 +134,7 @@ class Batch:
     """The same views in one st_render_batch call (device outputs, autotuned, CUDA graph)."""
 
     def __init__(self, renderer, items, out_float_ptrs, out_u8_ptrs, use_graph=True, tile_shape=-1, chunk=0,
-                 stack_placement=-1, launch_mode=-1):
+                 stack_placement=-1, launch_mode=api.LAUNCH_AUTOTUNED):
         self.r = renderer
         self.views = (api.st_view * len(items))()
         self.keep = items
@@ -160,7 +160,7 @@ class Stream:
     resolution, bounces, camera) plus a transform update of 0..64 primitives, delivered as a
     resolved u8 frame into host memory."""
 
-    def __init__(self, residents, slots, rate, count, seed, refit_fraction=0.25, launch_mode=0):
+    def __init__(self, residents, slots, rate, count, seed, refit_fraction=0.25, launch_mode=api.LAUNCH_PER_VIEW):
         rng = np.random.default_rng(seed)
         self.residents, self.slots, self.rate = residents, slots, rate
         self.refit_fraction = refit_fraction

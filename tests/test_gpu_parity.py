@@ -274,8 +274,8 @@ def test_batch_equals_per_frame_renders(renderer):
     for graph in (False, True, True):        # one trace kernel per view, on concurrent streams
         frames = [scenes.Frame(w, h, cam, depth=d, mode=m) for slot, sd, cam, w, h, d, m in specs]
         opt = api.render_batch(renderer, [(sp[0], sp[1], fr) for sp, fr in zip(specs, frames)], use_graph=graph,
-                               launch_mode=1)
-        assert opt.launch_mode_used == 1
+                               launch_mode=api.LAUNCH_PER_VIEW)
+        assert opt.launch_mode_used == api.LAUNCH_PER_VIEW
         for a, b in zip(frames, singles):
             assert np.array_equal(a.float_pixels.view(np.uint8), b.float_pixels.view(np.uint8)), ("per view", graph)
             assert np.array_equal(a.pixels.view(np.uint8), b.pixels.view(np.uint8))
