@@ -72,3 +72,51 @@ def test_null_arguments_are_rejected(L):
     assert L.st_upload_scene(None, 0, None) == 1
     assert L.st_layout_query(None) == -1
     assert L.st_layout_query(b"NoSuchStruct") == -1
+
+
+API_STRUCTS = ["st_config", "st_render_options", "st_view", "st_batch_options", "st_serve_config", "st_request",
+               "st_result", "st_pick_result"]
+
+
+def _header_enums():
+    """Every `NAME = value` of the header's enums."""
+    text = open(os.path.join(ROOT, "include", "slimtracin_b200.h")).read()
+    out = {}
+    for body in re.findall(r"enum \w+ \{(.*?)\};", text, re.S):
+        for name, value in re.findall(r"(ST_\w+)\s*=\s*(-?\d+)", body):
+            out[name] = int(value)
+    return out
+
+
+def test_api_structs_and_enums_match_the_header(tmp_path):
+    """The ctypes mirror of the entry points' own structs (api.py) against the header compiled by gcc:
+    every size and field offset, and every enum constant the binding names."""
+    lines = []
+    for s in API_STRUCTS:
+        cls = getattr(api, s)
+        lines.append(f'printf("{s} %zu\\n", sizeof({s}));')
+        for f, _ in cls._fields_:
+            lines.append(f'printf("{s}.{f} %zu\\n", offsetof({s}, {f}));')
+    src = tmp_path / "probe.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "slimtracin_b200.h"\nint main(void) {\n'
+                   + "\n".join(lines) + "\nreturn 0;\n}\n")
+    exe = tmp_path / "probe"
+    assert os.system(f"gcc -std=c11 -I{ROOT}/include {src} -o {exe}") == 0
+    got = dict(line.split() for line in os.popen(str(exe)).read().splitlines())
+    for s in API_STRUCTS:
+        cls = getattr(api, s)
+        assert int(got[s]) == C.sizeof(cls), s
+        for f, _ in cls._fields_:
+            assert int(got[f"{s}.{f}"]) == getattr(cls, f).offset, (s, f)
+    enums = _header_enums()
+    py = {"ST_OK": api.ST_OK, "ST_ERR_INVALID_ARG": api.ST_ERR_INVALID_ARG, "ST_ERR_BUDGET": api.ST_ERR_BUDGET,
+          "ST_ERR_BAD_SCENE": api.ST_ERR_BAD_SCENE, "ST_ERR_IO": api.ST_ERR_IO,
+          "ST_ERR_NOT_READY": api.ST_ERR_NOT_READY, "ST_ERR_TIMEOUT": api.ST_ERR_TIMEOUT,
+          "ST_BVH_LBVH30": api.ST_BVH_LBVH30, "ST_BVH_BINNED_SAH": api.ST_BVH_BINNED_SAH,
+          "ST_BVH_REFIT": api.ST_BVH_REFIT, "ST_OVERLAY_BVH": api.OVERLAY_BVH, "ST_OVERLAY_SSB": api.OVERLAY_SSB,
+          "ST_LAUNCH_AUTOTUNED": api.LAUNCH_AUTOTUNED, "ST_LAUNCH_PER_VIEW": api.LAUNCH_PER_VIEW,
+          "ST_LAUNCH_PERSISTENT": api.LAUNCH_PERSISTENT}
+    for name, value in py.items():
+        assert enums[name] == value, name
+    counters = sorted((v, k) for k, v in enums.items() if k.startswith("ST_CNT_") and k != "ST_CNT_COUNT")
+    assert [k[len("ST_CNT_"):].lower() for _, k in counters] == api.COUNTER_NAMES[:len(counters)]
