@@ -1,4 +1,4 @@
-"""Benchmark: Mrays/s of the 1080p PBR mesh scene (config 1) on B200.
+"""Benchmark: Mrays/s of the 1080p PBR mesh scene on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -22,7 +22,7 @@ cpu_baseline / --impl reference
            same scene bytes, all host threads, over a bounded sample of rows
 implicit16 16 implicit primitives, 3 point lights, 640x480, depth 2: the device frame beside
            the reference's CPU renderer (all host threads, and one thread)
-dynamic    config 2: 4096 moving primitives, TLAS rebuilt (LBVH30, binned SAH) or refit every frame,
+dynamic    4096 moving primitives, TLAS rebuilt (LBVH30, binned SAH) or refit every frame,
            1280x720 depth 2, 300 frames: build ms (API wall time) and trace ms (device events)
 batched    64 views (resolutions from 256x256 to 1920x1080, 1-6 bounces) over 8 resident scenes:
            one st_render_batch call (launch mode, tile shape, queue depth and stack placement
@@ -32,6 +32,9 @@ served     Poisson request streams (--rates) over the same 8 scenes, each reques
            transform update of 0-64 primitives, u8 frames to host: the library's server against
            the same requests one at a time; p50/p99 latency from arrival to completion (library
            clock) and Mrays/s over the stream
+ray_segments
+           primary + point-light shadow + bounce rays per frame (device counters of the same frame)
+           and the value and e2e rates restated in those segments
 ingest     texture baking (st_bake_texture, 1024x1024) and OBJ conversion (st_obj_to_mesh at 20,480
            and 327,680 triangles) beside the reference's loadTexture and obj2mesh on the host
 """
@@ -260,7 +263,7 @@ def mixed_workloads(r, big_sd, stream, rates):
 
 
 def dynamic_tlas(r, frames, cpu_reference):
-    """Config 2: 4096 moving implicit primitives, the TLAS rebuilt (LBVH30 or binned SAH) or refit
+    """The moving scene: 4096 implicit primitives, the TLAS rebuilt (LBVH30 or binned SAH) or refit
     every frame, 1280x720 depth 2.  Per frame: the primitive records go up (whole array), the TLAS
     is updated through st_update_scene_bvh (wall time of the call, which includes its validity
     check of the new node array), and the frame is traced (device events)."""
@@ -318,8 +321,9 @@ def dynamic_tlas(r, frames, cpu_reference):
 
 
 def implicit16_section(r, cpu_reference):
-    """Config 0 (16 implicit primitives, 3 point lights, 640x480, depth 2): the device frame (device
-    outputs, trace kernel by CUDA events) beside the reference's CPU renderer on the same scene."""
+    """The implicit16 scene (16 implicit primitives, 3 point lights, 640x480, depth 2): the device
+    frame (device outputs, trace kernel by CUDA events) beside the reference's CPU renderer on the
+    same scene."""
     import torch
     from slimtracin_b200 import api
     sd, cam = scenes.implicit16_scene()
@@ -353,7 +357,7 @@ def implicit16_section(r, cpu_reference):
 
 
 def ingest_section(r, cpu_reference):
-    """Texture ingestion: loadTexture (bmp2texture.c:324) of the 1024x1024 RGB texture config 1 uses,
+    """Texture ingestion: loadTexture (bmp2texture.c:324) of the 1024x1024 RGB texture the mesh scene uses,
     on the device through st_bake_texture (API wall time: image upload, bake, quads download into
     host memory) beside the reference's CPU baker on one thread."""
     import ctypes as C
@@ -502,6 +506,7 @@ def main():
     opt = r.render(0, sd, ctr_frame, count_work=True, skip_float_copy=True)
     counters = api.counters_dict(opt)
     bytes_alg = sum(BYTES[k] * counters[k] for k in BYTES)
+    segments = counters["primary_rays"] + counters["shadow_rays"] + counters["bounce_rays"]
 
     def step():
         with torch.cuda.stream(stream):
@@ -636,6 +641,9 @@ def main():
                          "l2_peak": l2_gbs, "l2_frac": achieved / l2_gbs,
                          "l2_peak_source": "48 MB L2-resident read (torch.sum), measured in this run"},
             "counters": counters,
+            "ray_segments": {"per_frame": segments, "mrays_s": value * segments / grid,
+                             "e2e_mrays_s": e2e_value * segments / grid,
+                             "counted": "primary + point-light shadow + bounce rays, device counters"},
             "implicit16": cfg0,
             "dynamic_tlas": dynamic,
             "ingest": ingest,
