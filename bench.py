@@ -585,7 +585,7 @@ def main():
     dynamic = dynamic_tlas(r, args.dynamic_frames, rank == 0 and world == 1 and not args.no_cpu_baseline) \
         if args.dynamic_frames > 0 else None
     l2_gbs = measure_l2_gbs()
-    cfg0 = implicit16_section(r, rank == 0 and world == 1 and not args.no_cpu_baseline)
+    implicit16 = implicit16_section(r, rank == 0 and world == 1 and not args.no_cpu_baseline)
     ingest = ingest_section(r, rank == 0 and world == 1 and not args.no_cpu_baseline)
 
     # ---- roofline of the trace kernel -----------------------------------------------------------
@@ -644,7 +644,7 @@ def main():
             "ray_segments": {"per_frame": segments, "mrays_s": value * segments / grid,
                              "e2e_mrays_s": e2e_value * segments / grid,
                              "counted": "primary + point-light shadow + bounce rays, device counters"},
-            "implicit16": cfg0,
+            "implicit16": implicit16,
             "dynamic_tlas": dynamic,
             "ingest": ingest,
             "batched": mixed["batched"] if mixed else None,
