@@ -878,7 +878,6 @@ __global__ void batch_resolve_kernel(const BatchTable T, u32t n_views) {
         resolve_one(B.out, B.view.grid_w, B.view.grid_w - 1, B.out_u8, x, y);
 }
 
-#ifndef ST_HOST_EMU
 // ---- launchers -------------------------------------------------------------------------------
 void launch_ssb(const SceneDev &S, const ViewDev &v, int4 *ssb, cudaStream_t st) {
     if (!S.n_prims) return;
@@ -947,5 +946,4 @@ void launch_resolve(const FloatPixel *in, u32t grid_w, u32t width, u32t height, 
     resolve_kernel<<<grid, 128, 0, st>>>(in, grid_w, width, height, out);
 }
 
-#endif  // ST_HOST_EMU
 }  // namespace st
