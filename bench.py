@@ -197,8 +197,8 @@ def run_reference_arm(args):
 
 
 def mixed_workloads(r, big_sd, stream, rates):
-    """The batched-views workload (64 views over 8 resident scenes, one graph-captured persistent
-    launch vs one st_render_ex per view) and the served stream (Poisson arrivals at `rates` with
+    """The batched-views workload (64 views over 8 resident scenes, one graph-launched
+    st_render_batch call with its launch mode autotuned vs one st_render_ex per view) and the served stream (Poisson arrivals at `rates` with
     transform updates, the library's server vs one request at a time), both with device-event or
     library-clock timing."""
     import torch
