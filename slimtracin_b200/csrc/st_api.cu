@@ -1142,9 +1142,10 @@ int plan_batch(st_ctx *ctx, const st_view *views, int n, int tile, const st_batc
     return ST_OK;
 }
 
-// A batch's launches, kTableViews views at a time: the views' SSBs and ray-row starts, the
-// persistent trace kernel over the group's tiles, and the resolves of the views that want a frame.
-// Every launch carries the group's view table as its kernel parameter.
+// A batch's launches, kTableViews views at a time: the views' SSBs and ray-row starts, the trace
+// (the persistent kernel over the group's tiles, or with kPerViewVariant one trace kernel per view
+// spread over the batch's aux streams), and the resolves of the views that want a frame.  The
+// set-up and resolve launches carry the group's view table as their kernel parameter.
 int launch_groups(st_ctx *ctx, BatchState &B, const BatchPlan &p, int tile, u32t chunk, unsigned *status,
                   cudaStream_t st) {
     const int n = (int)p.table.size();
@@ -1704,8 +1705,9 @@ int new_scene_version(st_ctx *ctx, int slot) {
     return ST_OK;
 }
 
-// Enqueue one admitted batch on its flight's stream: view table, per-view SSB and ray rows, the
-// persistent tile-queue kernel, resolves, and the copies of every output into pinned staging.
+// Enqueue one admitted batch on its flight's stream: per-view SSB and ray rows, the trace (per view
+// or persistent, as launch_groups does it), resolves, and the copies of every output into pinned
+// staging.
 int enqueue_flight(st_ctx *ctx, InFlight &F, BatchPlan &p, std::vector<std::shared_ptr<ServeReq>> &reqs, int tile,
                    u32t chunk, char *arena) {
     const int n = (int)reqs.size();
