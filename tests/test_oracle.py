@@ -188,6 +188,55 @@ def _lbvh(boxes, max_leaf, builder="lbvh"):
     return codes, order, nodes[:info[0]], leaf, int(info[0]), int(info[1])
 
 
+def _morton30_numpy(boxes):
+    """The 30-bit Morton code of the LBVH specification, restated independently with numpy float32:
+    centroid (min + max) * 0.5; per axis t = (c - lo) * (1024 / (hi - lo)) over the union box (scale
+    0 on a flat axis); q = 0 unless t > 0, 1023 from t >= 1023, else t truncated; x takes the
+    highest bit of each triple."""
+    b = np.asarray(boxes, np.float32)
+    lo, hi = b[:, :3].min(0), b[:, 3:].max(0)
+    ext = (hi - lo).astype(np.float32)
+    with np.errstate(divide="ignore"):
+        scale = np.where(ext > 0, np.float32(1024.0) / ext, np.float32(0.0)).astype(np.float32)
+    c = ((b[:, :3] + b[:, 3:]) * np.float32(0.5)).astype(np.float32)
+    t = ((c - lo) * scale).astype(np.float32)
+    q = np.where(t > 0, np.where(t >= 1023, 1023, np.trunc(np.where(t > 0, t, 0))), 0).astype(np.uint32)
+    code = np.zeros(len(b), np.uint32)
+    for bit in range(10):
+        for axis, shift in ((0, 2), (1, 1), (2, 0)):
+            code |= ((q[:, axis] >> bit) & 1) << (3 * bit + shift)
+    return code
+
+
+MORTON_CASES = ["random", "flat_axis", "identical", "wide_range", "clustered"]
+
+
+@pytest.mark.parametrize("case", MORTON_CASES)
+def test_lbvh_codes_match_an_independent_restatement(case):
+    """The oracle's Morton codes (orc_lbvh30) equal the numpy restatement bit for bit, including a flat
+    axis (scale 0), identical boxes, coordinates spanning many binades and tight clusters."""
+    rng = np.random.default_rng(1000 + MORTON_CASES.index(case))
+    n = 3000
+    c = rng.uniform(-10, 10, (n, 3))
+    if case == "flat_axis":
+        c[:, 1] = 2.5
+    elif case == "identical":
+        c[:] = (1.0, -2.0, 3.0)
+    elif case == "wide_range":
+        c = rng.choice([-1, 1], (n, 3)) * 10.0 ** rng.uniform(-6, 6, (n, 3))
+    elif case == "clustered":
+        c = rng.integers(0, 4, (n, 1)) * 100.0 + rng.normal(0, 1e-3, (n, 3))
+    e = rng.uniform(0.0, 0.5, (n, 3)) if case != "identical" else np.full((n, 3), 0.25)
+    if case == "flat_axis":
+        e[:, 1] = 0.0
+    boxes = np.concatenate([c - e, c + e], 1).astype(np.float32)
+    codes, order, *_ = _lbvh(boxes, 2)
+    want = _morton30_numpy(boxes)
+    assert np.array_equal(codes, want), int((codes != want).sum())
+    keys = want.astype(np.uint64) << np.uint64(32) | np.arange(n, dtype=np.uint64)
+    assert np.array_equal(order, np.argsort(keys, kind="stable").astype(np.uint32))
+
+
 @pytest.mark.parametrize("builder", ["lbvh", "binned_sah"])
 @pytest.mark.parametrize("n,max_leaf", [(1, 2), (2, 2), (3, 2), (17, 2), (1000, 2), (5000, 4), (4096, 2)])
 def test_bvh_oracle_structure(n, max_leaf, builder):
