@@ -237,6 +237,83 @@ def test_lbvh_codes_match_an_independent_restatement(case):
     assert np.array_equal(order, np.argsort(keys, kind="stable").astype(np.uint32))
 
 
+def _lbvh_top_down(boxes, max_leaf):
+    """The LBVH30 topology and layout, restated top-down: the binary radix tree of the sorted
+    (code << 32 | index) keys splits a range [f, l] after the last key that shares a longer prefix
+    with key f than key l does; internal node g + (0 or 1) is the child range that does not start or
+    end at a leaf (Karras's numbering).  Ranges of more than max_leaf items are kept, ranked in
+    internal-node order; kept node r's children go to slots 1 + 2r and 2 + 2r; every node's box is
+    the union of its items' boxes; depth counts ancestors."""
+    b = np.asarray(boxes, np.float32)
+    n = len(b)
+    keys = [(int(c) << 32) | i for i, c in enumerate(_morton30_numpy(b))]
+    keys.sort()
+    order = np.array([k & 0xFFFFFFFF for k in keys], np.uint32)
+    nodes = np.zeros(max(1, 2 * n), dtype=S.BVHNODE_DT)
+
+    def box(f, l):
+        items = b[order[f:l + 1]]
+        return np.concatenate([items[:, :3].min(0), items[:, 3:].max(0)])
+
+    if n <= max_leaf:
+        if n:
+            nodes[0]["aabb"] = box(0, n - 1)
+        nodes[0]["child_count"] = n
+        return order, nodes[:1], 1
+    internal = {}                         # internal node index -> (first, last, left, right, depth)
+
+    def build(idx, f, l, depth):
+        prefix = 64 - (keys[f] ^ keys[l]).bit_length()
+        g = f
+        while g + 1 < l and 64 - (keys[f] ^ keys[g + 1]).bit_length() > prefix:
+            g += 1
+        left = ("leaf", g) if g == f else ("node", g)
+        right = ("leaf", g + 1) if g + 1 == l else ("node", g + 1)
+        internal[idx] = (f, l, left, right, depth)
+        if left[0] == "node":
+            build(g, f, g, depth + 1)
+        if right[0] == "node":
+            build(g + 1, g + 1, l, depth + 1)
+
+    build(0, 0, n - 1, 0)
+    kept = sorted(k for k, v in internal.items() if v[1] - v[0] + 1 > max_leaf)
+    rank = {k: r for r, k in enumerate(kept)}
+    nodes[0]["aabb"] = box(0, n - 1)
+    nodes[0]["first_child_id"] = 1
+    height = 0
+    for k in kept:
+        f, l, left, right, depth = internal[k]
+        g = left[1]
+        for c, (kind, idx), (cf, cl) in ((0, left, (f, g)), (1, right, (g + 1, l))):
+            o = nodes[1 + 2 * rank[k] + c]
+            o["depth"] = depth + 1
+            height = max(height, depth + 1)
+            o["aabb"] = box(cf, cl)
+            if kind == "node" and idx in rank:
+                o["first_child_id"] = 1 + 2 * rank[idx]
+            else:
+                o["first_child_id"] = cf
+                o["child_count"] = cl - cf + 1
+    return order, nodes[:1 + 2 * len(kept)], height
+
+
+@pytest.mark.parametrize("n,max_leaf", [(1, 2), (2, 2), (3, 1), (3, 2), (17, 2), (300, 1), (1000, 2), (2000, 4)])
+@pytest.mark.parametrize("case", ["random", "clustered"])
+def test_lbvh_topology_matches_a_top_down_restatement(n, max_leaf, case):
+    """orc_lbvh30's nodes (Karras-style per-node search) equal the top-down radix-tree restatement
+    byte for byte, with distinct and with heavily repeated Morton codes."""
+    rng = np.random.default_rng(7 * n + max_leaf)
+    c = rng.uniform(-10, 10, (n, 3)) if case == "random" else \
+        rng.integers(0, 3, (n, 1)) * 50.0 + rng.uniform(0.5, 0.6, (n, 3))
+    e = rng.uniform(0.01, 0.5, (n, 3))
+    boxes = np.concatenate([c - e, c + e], 1).astype(np.float32)
+    _, order, nodes, _, count, height = _lbvh(boxes, max_leaf)
+    want_order, want_nodes, want_height = _lbvh_top_down(boxes, max_leaf)
+    assert np.array_equal(order, want_order)
+    assert (count, height) == (len(want_nodes), want_height)
+    assert nodes.tobytes() == want_nodes.tobytes()
+
+
 @pytest.mark.parametrize("builder", ["lbvh", "binned_sah"])
 @pytest.mark.parametrize("n,max_leaf", [(1, 2), (2, 2), (3, 2), (17, 2), (1000, 2), (5000, 4), (4096, 2)])
 def test_bvh_oracle_structure(n, max_leaf, builder):
