@@ -314,6 +314,100 @@ def test_lbvh_topology_matches_a_top_down_restatement(n, max_leaf, case):
     assert nodes.tobytes() == want_nodes.tobytes()
 
 
+def _half_area(lo, hi):
+    """halfArea (AABB.h:39) in float32, the reference's order: ex*ey + ey*ez + ez*ex."""
+    e = (hi - lo).astype(np.float32)
+    return (e[..., 0] * e[..., 1] + e[..., 1] * e[..., 2] + e[..., 2] * e[..., 0]).astype(np.float32)
+
+
+def _binned_sah_numpy(boxes, max_leaf, bins=32):
+    """The binned-SAH specification restated with numpy float32: level by level, a range of more
+    than max_leaf items is split on the axis and bin boundary of least halfArea(L)*nL +
+    halfArea(R)*nR over 32 bins of its centroid extent (axes with zero extent skipped, empty sides
+    skipped, first minimum in (axis, bin) order wins), else at its middle; the partition is stable
+    and each level's split nodes get child pairs in order."""
+    b = np.asarray(boxes, np.float32)
+    n = len(b)
+    f32 = np.float32
+    cent = ((b[:, :3] + b[:, 3:]) * f32(0.5)).astype(f32)
+    ids = np.arange(n)
+    nodes = np.zeros(max(1, 2 * n), dtype=S.BVHNODE_DT)
+    tasks, pairs, height, level = [(0, n, 0)], 0, 1, 0
+    while tasks:
+        nxt = []
+        for begin, end, slot in tasks:
+            it = ids[begin:end]
+            nodes[slot]["aabb"] = np.concatenate([b[it, :3].min(0), b[it, 3:].max(0)]) if len(it) else 0
+            nodes[slot]["depth"] = level
+            if end - begin <= max_leaf:
+                nodes[slot]["first_child_id"] = begin
+                nodes[slot]["child_count"] = end - begin
+                height = max(height, level)
+                continue
+            c = cent[it]
+            lo = c.min(0)
+            ext = (c.max(0) - lo).astype(f32)
+            best_cost, best_axis, best_k, best_bins = np.inf, -1, -1, None
+            for a in range(3):
+                if not ext[a] > 0:
+                    continue
+                t = ((c[:, a] - lo[a]) * (f32(bins) / ext[a])).astype(f32)
+                bv = np.where(t >= bins - 1, bins - 1, np.trunc(np.maximum(t, 0))).astype(np.int64)
+                bv[~(t > 0)] = 0
+                cnt = np.bincount(bv, minlength=bins)
+                bmin = np.full((bins, 3), np.inf, f32)
+                bmax = np.full((bins, 3), -np.inf, f32)
+                np.minimum.at(bmin, bv, b[it, :3])
+                np.maximum.at(bmax, bv, b[it, 3:])
+                lmin, lmax = np.minimum.accumulate(bmin, 0), np.maximum.accumulate(bmax, 0)
+                rmin, rmax = np.minimum.accumulate(bmin[::-1], 0)[::-1], np.maximum.accumulate(bmax[::-1], 0)[::-1]
+                nl = np.cumsum(cnt)
+                nr = np.cumsum(cnt[::-1])[::-1]
+                k = np.arange(bins - 1)
+                ok = (nl[k] > 0) & (nr[k + 1] > 0)
+                with np.errstate(invalid="ignore", over="ignore"):
+                    cost = (_half_area(lmin[k], lmax[k]) * nl[k].astype(f32) +
+                            _half_area(rmin[k + 1], rmax[k + 1]) * nr[k + 1].astype(f32)).astype(f32)
+                cost[~ok] = np.inf
+                j = int(np.argmin(cost))
+                if cost[j] < best_cost:
+                    best_cost, best_axis, best_k, best_bins = cost[j], a, j, bv
+            if best_axis >= 0:
+                left = best_bins <= best_k
+                ids[begin:end] = np.concatenate([it[left], it[~left]])
+                mid = begin + int(left.sum())
+            else:
+                mid = begin + (end - begin) // 2
+            nodes[slot]["first_child_id"] = 1 + 2 * pairs
+            nxt += [(begin, mid, 1 + 2 * pairs), (mid, end, 2 + 2 * pairs)]
+            pairs += 1
+        tasks = nxt
+        level += 1
+    return ids.astype(np.uint32), nodes[:1 + 2 * pairs], height
+
+
+@pytest.mark.parametrize("n,max_leaf", [(1, 2), (2, 1), (3, 2), (17, 2), (700, 2), (2000, 4)])
+@pytest.mark.parametrize("case", ["random", "flat_axis", "same_centroid", "clustered"])
+def test_binned_sah_matches_a_numpy_restatement(n, max_leaf, case):
+    """orc_binned_sah's order and node arrays equal the numpy restatement byte for byte, including
+    axes of zero centroid extent and ranges that fall back to the middle split."""
+    rng = np.random.default_rng(11 * n + max_leaf)
+    c = rng.uniform(-10, 10, (n, 3))
+    if case == "flat_axis":
+        c[:, 2] = 1.25
+    elif case == "same_centroid":
+        c[:] = (0.5, -1.5, 2.5)
+    elif case == "clustered":
+        c = rng.integers(0, 3, (n, 1)) * 40.0 + rng.uniform(0.5, 0.5001, (n, 3))
+    e = rng.uniform(0.01, 0.5, (n, 3))
+    boxes = np.concatenate([c - e, c + e], 1).astype(np.float32)
+    _, order, nodes, _, count, height = _lbvh(boxes, max_leaf, "binned_sah")
+    want_order, want_nodes, want_height = _binned_sah_numpy(boxes, max_leaf)
+    assert np.array_equal(order, want_order)
+    assert (count, height) == (len(want_nodes), want_height)
+    assert nodes.tobytes() == want_nodes.tobytes()
+
+
 @pytest.mark.parametrize("builder", ["lbvh", "binned_sah"])
 @pytest.mark.parametrize("n,max_leaf", [(1, 2), (2, 2), (3, 2), (17, 2), (1000, 2), (5000, 4), (4096, 2)])
 def test_bvh_oracle_structure(n, max_leaf, builder):
