@@ -239,3 +239,53 @@ def test_scene_file_matches_reference(tmp_path):
     target.cameras = C.addressof(cams)
     ref.ref_load_scene(C.byref(target), ours)
     assert bytes(prims) == C.string_at(sc.primitives, 72 * n)
+
+
+def test_texture_file_refusals(tmp_path):
+    """Truncated texture files (inside the header, a mip's size, its quads), a missing file and a
+    destination one byte too small are refused, never read past."""
+    L = api.lib()
+    rng = np.random.default_rng(5)
+    keep = []
+    tex = _texture_ctypes(scenes.bake_texture(rng.integers(0, 256, (24, 16, 3), dtype=np.uint8), True, True), keep)
+    path = str(tmp_path / "t.texture").encode()
+    assert L.st_write_texture_file(path, C.byref(tex)) == 0
+    data = open(path, "rb").read()
+    need = L.st_texture_file_bytes(path)
+    mem = np.zeros(need + 64, dtype=np.uint8)
+    back = S.Texture()
+    assert L.st_read_texture_file(path, C.byref(back), mem.ctypes.data, need - 1) == api.ST_ERR_BUDGET
+    for cut in (3, 9, len(data) // 2, len(data) - 1):
+        short = str(tmp_path / f"short{cut}.texture").encode()
+        open(short, "wb").write(data[:cut])
+        got = L.st_texture_file_bytes(short)
+        if got < 0:
+            assert L.st_read_texture_file(short, C.byref(back), mem.ctypes.data, need) == api.ST_ERR_IO, cut
+        else:
+            assert L.st_read_texture_file(short, C.byref(back), mem.ctypes.data, len(mem)) == api.ST_ERR_IO, cut
+    none = str(tmp_path / "none.texture").encode()
+    assert L.st_texture_file_bytes(none) == -1
+    assert L.st_read_texture_file(none, C.byref(back), mem.ctypes.data, need) == api.ST_ERR_IO
+
+
+def test_scene_file_refusals(tmp_path):
+    """Truncated scene files and a missing file are refused with ST_ERR_IO."""
+    L = api.lib()
+    sd, sc, keep = _scene_file_scene()
+    path = str(tmp_path / "a.scene").encode()
+    assert L.st_write_scene_file(path, C.byref(sc)) == 0
+    data = open(path, "rb").read()
+    n = sc.settings.primitives
+    prims = (S.Primitive * n)()
+    cams = (S.Camera * 1)()
+    for cut in (5, len(data) // 2, len(data) - 1):
+        short = str(tmp_path / f"short{cut}.scene").encode()
+        open(short, "wb").write(data[:cut])
+        target = S.Scene()
+        target.primitives = C.addressof(prims)
+        target.cameras = C.addressof(cams)
+        assert L.st_read_scene_file(short, C.byref(target), 1, n) == api.ST_ERR_IO, cut
+    target = S.Scene()
+    target.primitives = C.addressof(prims)
+    target.cameras = C.addressof(cams)
+    assert L.st_read_scene_file(str(tmp_path / "none.scene").encode(), C.byref(target), 1, n) == api.ST_ERR_IO
