@@ -72,6 +72,11 @@ def test_null_arguments_are_rejected(L):
     assert L.st_upload_scene(None, 0, None) == 1
     assert L.st_layout_query(None) == -1
     assert L.st_layout_query(b"NoSuchStruct") == -1
+    # ingestion: host-side checks that need no device
+    assert L.st_obj_mesh_bytes(b"/nonexistent/none.obj") == -1
+    assert L.st_obj_mesh_bytes(None) == -1
+    assert L.st_obj_to_mesh(None, b"x.obj", 0, api.ST_BVH_LBVH30, None, None, 0) == 1
+    assert L.st_bake_texture(None, None, 4, 4, 24, 1, 1, None, None, 0) == 1
 
 
 API_STRUCTS = ["st_config", "st_render_options", "st_view", "st_batch_options", "st_serve_config", "st_request",
