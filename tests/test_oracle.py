@@ -34,7 +34,7 @@ def test_oracle_reproduces_golden_renders(name):
 
 
 @needs_ref
-@pytest.mark.parametrize("case", ["implicit16", "area", "mesh_small", "moving320"])
+@pytest.mark.parametrize("case", ["implicit16", "area", "mesh_small", "mesh_small_depth6", "moving320"])
 @pytest.mark.parametrize("mode", [S.RM_BEAUTY, S.RM_NORMALS])
 def test_oracle_matches_reference_live(case, mode):
     """Larger renders than the fixtures, oracle vs the reference run here, every byte equal."""
@@ -44,10 +44,10 @@ def test_oracle_matches_reference_live(case, mode):
     elif case == "area":
         sd, cam = scenes.example_area_lights()
         w, h, depth = 240, 180, 4
-    elif case == "mesh_small":
+    elif case.startswith("mesh_small"):
         sd, cam = scenes.mesh_scene(subdivisions=3, texture_size=64)
         H.blas_sah(sd.meshes[0], "ref")
-        w, h, depth = 192, 108, 4
+        w, h, depth = (192, 108, 4) if case == "mesh_small" else (160, 90, 6)
     else:
         sd, cam = scenes.moving_scene(count=320)
         w, h, depth = 128, 72, 2
