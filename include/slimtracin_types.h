@@ -6,8 +6,9 @@
  * Layout.  The reference targets Win32, where `unsigned long` is 32 bits, so its `u32`/`i32`
  * (core/base.h:95,98) are 32-bit there.  This header fixes that layout on every platform:
  * u32 = uint32_t, i32 = int32_t, pointers native.  A Linux build of the reference is
- * layout-compatible when it is compiled with 32-bit u32/i32; the sizes below
- * are asserted at compile time and exported at run time by st_layout_sizeof().
+ * layout-compatible when it is compiled with 32-bit u32/i32 (for instance by `#define long` empty
+ * around the reference's includes, after the system headers); the sizes below are asserted at
+ * compile time and exported at run time by st_layout_query().
  *
  * Source of every struct: core/base.h:93-365,742-753 and core/types.h:56-374 of the reference.
  * Unions with aliased member names in the reference (vec2/vec3/vec4/mat3) are written here as plain

@@ -5,8 +5,8 @@
  * reference's own headers, with the reference's scene, camera and viewport code, its top-down SAH
  * TLAS build and its per-frame sequence (updateSceneSSB, beginDrawing, renderScene,
  * drawViewportToWindowContent) — and the GPU seams bound to libslimtracin_b200 through the C ABI
- * as INTEGRATION.md describes (residency through st_allocate_device_scene / st_upload_*, the frame
- * through st_render_scene).  The test compares its GPU frames with the same host's CPU frames.
+ * (allocateDeviceScene and the upload* stubs forward to st_allocate_device_scene / st_upload_*,
+ * renderScene to st_render_scene).  The test compares its GPU frames with the same host's CPU frames.
  *
  * Built by oracle/Makefile into oracle/_ref/libdropin.so (it needs the reference sources; the
  * reference's 32-bit `u32` is obtained as in ref_harness.c).

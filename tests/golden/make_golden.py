@@ -25,7 +25,7 @@ import oracle  # noqa: E402
 from slimtracin_b200 import scenes, structs as S  # noqa: E402
 from tests import helpers as H  # noqa: E402
 
-MONKEY = "/root/reference/src/examples/monkey.mesh"
+MONKEY = os.path.join(os.environ.get("ST_REFERENCE_SRC", "/root/reference/src"), "examples", "monkey.mesh")
 
 
 def sha(a):

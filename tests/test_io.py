@@ -92,7 +92,8 @@ def test_mesh_file_matches_reference(tmp_path):
 def test_reads_the_reference_monkey_mesh():
     """The one .mesh file the reference ships (src/examples/monkey.mesh) reads like
     loadMeshFromFile reads it."""
-    path = os.path.join(os.environ.get("ST_REFERENCE_SRC", "/root/reference/src"), "examples", "monkey.mesh")
+    from tests.golden import make_golden as G
+    path = G.MONKEY
     if not os.path.exists(path):
         pytest.skip("reference sources not present")
     L, ref = api.lib(), oracle.reference()
