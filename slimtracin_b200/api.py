@@ -178,6 +178,13 @@ class Renderer:
         except Exception:
             pass
 
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+        return False
+
     @property
     def stream(self):
         return self.L.st_get_stream(self.ctx)
@@ -352,6 +359,13 @@ class Server:
             self.r._check(self.L.st_serve_stop(self.r.ctx), "st_serve_stop")
             self.running = False
             self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.stop()
+        return False
 
 
 def clock():

@@ -125,3 +125,19 @@ def test_api_structs_and_enums_match_the_header(tmp_path):
         assert enums[name] == value, name
     counters = sorted((v, k) for k, v in enums.items() if k.startswith("ST_CNT_") and k != "ST_CNT_COUNT")
     assert [k[len("ST_CNT_"):].lower() for _, k in counters] == api.COUNTER_NAMES[:len(counters)]
+
+
+def test_renderer_is_a_context_manager(L):
+    """Without a device the constructor raises STError (ST_ERR_NO_DEVICE); the with-statement
+    protocol closes a context exactly once."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(api.STError):
+        api.Renderer(device=0)
+    r = api.Renderer.__new__(api.Renderer)
+    r.L, r.ctx = L, C.c_void_p()
+    with r as same:
+        assert same is r
+    r.close()                       # idempotent on a closed context
+    assert not r.ctx
