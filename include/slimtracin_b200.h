@@ -159,6 +159,14 @@ ST_API int st_update_mesh_bvh(st_ctx *ctx, Mesh *mesh, int mode);
 ST_API int st_build_bvh(st_ctx *ctx, int mode, const float *aabbs, uint32_t n, uint32_t max_leaf, uint32_t *codes,
                         uint32_t *order, BVHNode *nodes, uint32_t info[2]);
 
+/* Validate a BVH in the reference's layout the way the uploads do (st_upload_scene_bvh,
+ * st_upload_mesh_bvhs), on the host, with no context: every children pair reached from the root
+ * lies inside `nodes[node_count]` and is reached once, every leaf range lies inside `items`, and
+ * both `height` and the depth the walk reaches leave room in the 64-entry traversal stacks (depth
+ * + 2 <= 64).  ST_OK, ST_ERR_BAD_SCENE, or ST_ERR_INVALID_ARG for a null array.  No reference
+ * counterpart: a host can check a loaded .mesh or .scene BVH before it uploads it. */
+ST_API int st_validate_bvh(const BVHNode *nodes, uint32_t node_count, uint32_t items, uint32_t height);
+
 /* ---- render: render/raytracer.h:302 ------------------------------------------------------------ */
 /* renderScene (raytracer.h:302) + the QCAA resolve of drawViewportToWindowContent (viewport.h:12).
  * Renders the scene resident in `slot` from viewport->camera into viewport->frame_buffer:

@@ -112,6 +112,7 @@ def lib():
             "st_update_mesh_bvh": (i, [vp, vp, i]),
             "st_render_scene": (i, [vp, i, vp, vp]),
             "st_build_bvh": (i, [vp, i, vp, u32, u32, vp, vp, vp, vp]),
+            "st_validate_bvh": (i, [vp, u32, u32, u32]),
             "st_build_lbvh_noalloc": (i, [vp, vp, u32, u32, vp, vp, vp, vp, vp]),
             "st_render_ex": (i, [vp, i, vp, vp, C.POINTER(st_render_options)]),
             "st_render_batch": (i, [vp, vp, i, C.POINTER(st_batch_options)]),

@@ -540,28 +540,40 @@ int st_upload_scene(st_ctx *ctx, int slot, const Scene *scene) {
 
 // A reference-layout BVH is safe to walk when, starting from the root, every internal node's
 // children pair lies inside the array and is reached exactly once (no cycles, no sharing), every
-// leaf range lies inside the item array, and the height leaves stack room.
+// leaf range lies inside the item array, and both the stated height and the depth the walk
+// actually reaches leave stack room.  The walked depth is checked because the reference's
+// top-down SAH builder states heights (and node depth fields) below the depth its trees reach:
+// 11 against 15 for a 4096-primitive TLAS.  The walk keeps at most one pending sibling per level,
+// so a tree whose deepest node is at depth d needs d stack entries; d + 2 <= kStack keeps the
+// reference's two entries of slack.
 static bool check_bvh(const BVHNode *nodes, u32t count, u32t items, u32t height) {
-    if (!count || height + 2 > (u32t)kStack) return false;
+    if (!nodes || !count || height + 2 > (u32t)kStack) return false;
     if (nodes[0].child_count) return (uint64_t)nodes[0].first_child_id + nodes[0].child_count <= items;
     std::vector<uint8_t> seen(count, 0);
-    std::vector<u32t> stack;
-    stack.push_back(0);
+    std::vector<std::pair<u32t, u32t>> stack;    // (node, its depth)
+    stack.push_back({0u, 0u});
     seen[0] = 1;
     while (!stack.empty()) {
-        const BVHNode &n = nodes[stack.back()];
+        const u32t at = stack.back().first, depth = stack.back().second;
         stack.pop_back();
+        const BVHNode &n = nodes[at];
         if (n.child_count) {
             if ((uint64_t)n.first_child_id + n.child_count > items) return false;
             continue;
         }
+        if (depth + 1 + 2 > (u32t)kStack) return false;
         const u32t f = n.first_child_id;
         if (!(f & 1u) || (uint64_t)f + 1 >= count || seen[f] || seen[f + 1]) return false;
         seen[f] = seen[f + 1] = 1;
-        stack.push_back(f);
-        stack.push_back(f + 1);
+        stack.push_back({f, depth + 1});
+        stack.push_back({f + 1, depth + 1});
     }
     return true;
+}
+
+int st_validate_bvh(const BVHNode *nodes, uint32_t node_count, uint32_t items, uint32_t height) {
+    if (!nodes) return ST_ERR_INVALID_ARG;
+    return check_bvh(nodes, node_count, items, height) ? ST_OK : ST_ERR_BAD_SCENE;
 }
 
 static int finish_tlas(st_ctx *ctx, SceneSlot &S) {

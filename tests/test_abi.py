@@ -4,6 +4,7 @@ import ctypes as C
 import os
 import re
 
+import numpy as np
 import pytest
 
 import oracle
@@ -141,3 +142,48 @@ def test_renderer_is_a_context_manager(L):
         assert same is r
     r.close()                       # idempotent on a closed context
     assert not r.ctx
+
+
+def _chain(depth):
+    """A reference-layout BVH whose every internal node has a one-item leaf on the left and the next
+    internal node on the right, down to depth `depth` (its last pair is two leaves)."""
+    nodes = np.zeros(1 + 2 * depth, dtype=S.BVHNODE_DT)
+    item = 0
+    for d in range(depth):
+        f = 1 + 2 * d
+        nodes[2 * d if d else 0]["first_child_id"] = f
+        nodes[f]["first_child_id"], nodes[f]["child_count"] = item, 1
+        item += 1
+    nodes[2 * depth]["first_child_id"], nodes[2 * depth]["child_count"] = item, 1
+    return nodes, item + 1
+
+
+def test_validate_bvh(L):
+    """st_validate_bvh: the host-side check the uploads make, without a device."""
+    ok = api.ST_OK
+    bad = api.ST_ERR_BAD_SCENE
+    nodes, items = _chain(5)
+    assert L.st_validate_bvh(nodes.ctypes.data, len(nodes), items, 5) == ok
+    assert L.st_validate_bvh(None, len(nodes), items, 5) == api.ST_ERR_INVALID_ARG
+    assert L.st_validate_bvh(nodes.ctypes.data, 0, items, 5) == bad
+    assert L.st_validate_bvh(nodes.ctypes.data, len(nodes), items - 1, 5) == bad      # a leaf past the items
+    assert L.st_validate_bvh(nodes.ctypes.data, len(nodes), items, 63) == bad         # stated height too large
+    broken = nodes.copy()
+    broken[2]["first_child_id"] = len(nodes) - 1                                      # a pair past the array
+    assert L.st_validate_bvh(broken.ctypes.data, len(nodes), items, 5) == bad
+    shared = nodes.copy()
+    shared[2]["first_child_id"] = 1                                                   # a cycle back to pair 1
+    assert L.st_validate_bvh(shared.ctypes.data, len(nodes), items, 5) == bad
+    even = nodes.copy()
+    even[0]["first_child_id"] = 2                                                     # pairs start at odd slots
+    assert L.st_validate_bvh(even.ctypes.data, len(nodes), items, 5) == bad
+    # the walked depth bounds the stacks whatever height is stated: 62 levels fit, 63 do not
+    deep, n_items = _chain(62)
+    assert L.st_validate_bvh(deep.ctypes.data, len(deep), n_items, 3) == ok
+    deeper, n_items = _chain(63)
+    assert L.st_validate_bvh(deeper.ctypes.data, len(deeper), n_items, 3) == bad
+    # a root leaf
+    leaf = np.zeros(1, dtype=S.BVHNODE_DT)
+    leaf[0]["child_count"] = 2
+    assert L.st_validate_bvh(leaf.ctypes.data, 1, 2, 1) == ok
+    assert L.st_validate_bvh(leaf.ctypes.data, 1, 1, 1) == bad

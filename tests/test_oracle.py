@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import oracle
-from slimtracin_b200 import scenes, structs as S
+from slimtracin_b200 import api, scenes, structs as S
 from tests import helpers as H
 from tests.golden import make_golden as G
 
@@ -537,3 +537,60 @@ def test_overlays_far_plane_matches_reference():
         out[which] = fr.float_pixels.copy()
         assert np.count_nonzero(out[which].view(np.uint8) != base.view(np.uint8)) > 100
     assert out["orc"].tobytes() == out["ref"].tobytes()
+
+
+def _deepest(nodes, count):
+    """Depth of the deepest node reachable from the root (root = 0), walking child pairs."""
+    deepest, stack = 0, [(0, 0)]
+    while stack:
+        i, d = stack.pop()
+        deepest = max(deepest, d)
+        if not nodes[i]["child_count"] and count > 1:
+            f = int(nodes[i]["first_child_id"])
+            stack += [(f, d + 1), (f + 1, d + 1)]
+    return deepest
+
+
+def test_project_builders_state_exact_heights():
+    """LBVH30 and binned SAH (the project's builders): the stated height is the depth of the deepest
+    leaf (1 for a root leaf) and every node's depth field is its depth from the root."""
+    rng = np.random.default_rng(9)
+    for builder in ("lbvh", "binned_sah"):
+        for n, leaf in ((1, 2), (5, 2), (2000, 2), (3000, 4)):
+            c = rng.uniform(-10, 10, (n, 3))
+            boxes = np.concatenate([c - 0.1, c + 0.1], 1)
+            _, _, nodes, _, cnt, height = _lbvh(boxes, leaf, builder)
+            assert height == max(_deepest(nodes, cnt), 1), (builder, n)
+            stack = [(0, 0)]
+            while stack:
+                i, d = stack.pop()
+                assert nodes[i]["depth"] == d, (builder, n, i)
+                if not nodes[i]["child_count"] and cnt > 1:
+                    f = int(nodes[i]["first_child_id"])
+                    stack += [(f, d + 1), (f + 1, d + 1)]
+
+
+@pytest.mark.parametrize("which", ["orc", "ref"])
+def test_reference_sah_understates_heights(which):
+    """The reference's top-down SAH (builder_top_down.h:204; the oracle restates it) states heights
+    and node depth fields below the depth its trees reach, so the library bounds its traversal
+    stacks by the walked depth: st_validate_bvh accepts these trees and measures them itself."""
+    if which == "ref" and not oracle.reference_available():
+        pytest.skip("reference harness not built")
+    L = api.lib()
+    seen = []
+    for count in (16, 300, 4096):
+        sd, _ = scenes.moving_scene(count=count)
+        H.tlas_sah(sd, which)
+        n = sd.tlas_node_count
+        deepest = _deepest(sd.tlas_nodes, n)
+        assert deepest >= sd.tlas_height and int(sd.tlas_nodes[:n]["depth"].max()) <= deepest
+        seen.append(deepest - sd.tlas_height)
+        assert L.st_validate_bvh(sd.tlas_nodes.ctypes.data, n, count, sd.tlas_height) == api.ST_OK
+    for sub in (2, 4):
+        md = H.blas_sah(scenes.displaced_icosphere(sub, seed=3), which)
+        deepest = _deepest(md.nodes, md.node_count)
+        assert deepest >= md.height
+        seen.append(deepest - md.height)
+        assert L.st_validate_bvh(md.nodes.ctypes.data, md.node_count, md.triangle_count, md.height) == api.ST_OK
+    assert max(seen) >= 2          # 4096 primitives: height 11, walked depth 15
