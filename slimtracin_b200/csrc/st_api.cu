@@ -542,10 +542,12 @@ int st_upload_scene(st_ctx *ctx, int slot, const Scene *scene) {
 // children pair lies inside the array and is reached exactly once (no cycles, no sharing), every
 // leaf range lies inside the item array, and both the stated height and the depth the walk
 // actually reaches leave stack room.  The walked depth is checked because the reference's
-// top-down SAH builder states heights (and node depth fields) below the depth its trees reach:
-// 11 against 15 for a 4096-primitive TLAS.  The walk keeps at most one pending sibling per level,
-// so a tree whose deepest node is at depth d needs d stack entries; d + 2 <= kStack keeps the
-// reference's two entries of slack.
+// top-down SAH builder (builder_top_down.h:243-266) records as a node's depth, and as the height,
+// the index of its explicit build stack, where a left child keeps its parent's index and only a
+// right child takes the next: that counts the right turns on a node's path, not its depth (11
+// against 15 for a 4096-primitive TLAS).  A near-first walk keeps at most one pending sibling per
+// level, so a tree whose deepest node is at depth d needs d stack entries; d + 2 <= kStack keeps
+// the reference's two entries of slack.
 static bool check_bvh(const BVHNode *nodes, u32t count, u32t items, u32t height) {
     if (!nodes || !count || height + 2 > (u32t)kStack) return false;
     if (nodes[0].child_count) return (uint64_t)nodes[0].first_child_id + nodes[0].child_count <= items;
