@@ -1343,6 +1343,9 @@ static void build_bvh(BVH *bvh, OBuilder *b, u32 N, u16 max_leaf) {
     OIter *stack = b->iters;
     stack[0].start = 0; stack[0].end = middle; stack[0].node_id = 1;
     stack[1].start = middle; stack[1].end = N; stack[1].node_id = 2;
+    /* `depth` is the index into this explicit build stack, as in the reference: a left child keeps
+     * its parent's index and a right child takes the next, so the depth fields and the height
+     * written here count right turns on a path, not the tree depth */
     i32 depth = 1;
     u32 leaf_count = 0;
     bvh->height = 1;
