@@ -152,6 +152,30 @@ def cpu_reference_sample(sd, cam, threads, budget_s, width=WIDTH, height=HEIGHT,
     return rays, total, frames
 
 
+def bench_config(world, triangles, grid):
+    """The workload both arms report, key for key: the same scene bytes, BVHs and frame."""
+    return {"workload": "1080p PBR mesh scene, depth 4, 1.31M-triangle BLAS x 8 instances",
+            "width": WIDTH, "height": HEIGHT, "depth": DEPTH, "rays_per_frame": grid,
+            "triangles": triangles, "instances": 8, "parallelism": f"replicas x{world}",
+            "l2": "device arm: 256 MiB written before every step, outside the timed events; "
+                  "reference arm: host caches as they are",
+            "blas": "binned SAH, the same node and Triangle bytes in both arms",
+            "tlas": "LBVH30, the same node bytes in both arms"}
+
+
+def reference_scene():
+    """The benchmark scene with its BLAS and TLAS built on the host by the oracle's binned-SAH and
+    LBVH30 builders, which give the bytes the device builders give (the full-size BLAS is compared
+    byte for byte on the GPU).  The reference's own full-sweep SAH over 1.31M triangles takes more
+    than ten minutes, so it is not the arm's input."""
+    import tests.helpers as H
+    sd, cam = build_scene()
+    for md in sd.meshes:
+        H.blas_sah(md, "binned")
+    H.tlas_lbvh(sd)
+    return sd, cam
+
+
 def run_reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -161,36 +185,36 @@ def run_reference_arm(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libslimref.so is not built"}))
         return 0
     threads = os.cpu_count() or 1
-    sd, cam = build_scene()
-    blas_on_device(sd)
-    import tests.helpers as H
-    H.tlas_sah(sd, "ref")
+    sd, cam = reference_scene()
     ref, sc, fr, keep = reference_frame_setup(sd, cam)
-    # each step renders whole frames; steps are capped so the run stays within a few minutes
-    t0 = time.perf_counter()
-    ref.ref_render_rows(C.byref(sc), C.byref(fr.viewport), threads, 0, 1, fr.grid_h)
-    frame_s = time.perf_counter() - t0
-    steps = max(1, min(args.steps, int(120.0 / max(frame_s, 1e-3))))
-    for _ in range(min(args.warmup, 3)):
+
+    def frame():
         ref.ref_render_rows(C.byref(sc), C.byref(fr.viewport), threads, 0, 1, fr.grid_h)
+
+    # untimed warm-up frames; the last one's time caps the steps so that the timed region stays
+    # near two minutes at most
+    for _ in range(args.warmup):
+        t0 = time.perf_counter()
+        frame()
+        frame_s = time.perf_counter() - t0
+    steps = max(1, min(args.steps, int(120.0 / max(frame_s, 1e-3))))
     total, rays = 0.0, 0
     for _ in range(steps):
         t = time.perf_counter()
-        ref.ref_render_rows(C.byref(sc), C.byref(fr.viewport), threads, 0, 1, fr.grid_h)
+        frame()
         total += time.perf_counter() - t
         rays += fr.rays
     value = rays / total / 1e6
-    rows = fr.grid_h
     grid = (WIDTH + 1) * (HEIGHT + 1)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
-            "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * grid / (value * 1e6),
+            "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded mesh-scene bytes, identical to the device arm)",
-            "config": {"workload": "1080p PBR mesh scene, depth 4, 1.31M-triangle BLAS x 8 instances",
-                       "width": WIDTH, "height": HEIGHT, "depth": DEPTH, "rays_per_frame": grid},
+            "data": "synthetic (seeded mesh scene: displaced icosphere, Perlin textures; no dataset)",
+            "config": bench_config(world, sd.meshes[0].triangle_count, grid),
             "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": "reference",
-                             "sample": f"{steps} whole frames ({rows} QCAA rows each), reference rayTrace "
-                                       f"(raytracer.h:81) per pixel, {threads} threads, {total:.1f} s"},
+                             "sample": f"{steps} whole 1921x1081 frames, the reference's rayTrace "
+                                       f"(render/raytracer.h:81) per grid point on {threads} host threads, "
+                                       f"{total:.1f} s; {args.warmup} untimed frames before"},
             "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -241,11 +265,17 @@ def mixed_workloads(r, big_sd, stream, rates):
         return float(np.median(out))
 
     pf_ms = timed(per_frame.run)
+    # how busy the device is while the per-frame loop runs: if the views' renders already fill most
+    # of the elapsed time, no batching of the same rays can go faster than the busy time allows
+    pf_busy_ms, pf_trace_ms = per_frame.device_ms()
     b_ms = timed(batch.run)
     batched = {"views": len(views), "scenes": [x.name for x in residents], "rays": rays,
                "per_frame_ms": pf_ms, "batch_ms": b_ms,
                "per_frame_mrays_s": rays / pf_ms / 1e3, "batch_mrays_s": rays / b_ms / 1e3,
-               "speedup": pf_ms / b_ms, "tile_shape": batch.opt.tile_shape_used,
+               "speedup": pf_ms / b_ms,
+               "per_frame_busy_fraction": pf_busy_ms / pf_ms, "per_frame_trace_fraction": pf_trace_ms / pf_ms,
+               "speedup_bound_if_gaps_removed": pf_ms / pf_trace_ms,
+               "tile_shape": batch.opt.tile_shape_used,
                "stack_placement": batch.opt.stack_placement_used, "launch_mode": batch.opt.launch_mode_used,
                "chunk": batch.opt.chunk_used, "graph_replayed": batch.opt.graph_replayed}
     del fbuf, ubuf, one_f, one_u
@@ -259,7 +289,12 @@ def mixed_workloads(r, big_sd, stream, rates):
         srv = MX.latency_summary(stream_k.serve(r))
         pf = MX.latency_summary(stream_k.per_frame(r))
         served.append({"rate_req_s": rate, "requests": count, "served": srv, "per_frame": pf})
-    return {"batched": batched, "served": served}
+    # the highest swept rate at which 1080p requests still finish within 33 ms at the 99th percentile
+    ok = [x["rate_req_s"] for x in served if x["served"].get("p99_1080p_ms", 0.0) <= 33.0]
+    knee = {"served_max_rate_p99_1080p_le_33ms": max(ok) if ok else None,
+            "per_frame_max_rate_p99_1080p_le_33ms":
+                max([x["rate_req_s"] for x in served if x["per_frame"].get("p99_1080p_ms", 0.0) <= 33.0], default=None)}
+    return {"batched": batched, "served": served, "served_knee": knee}
 
 
 def dynamic_tlas(r, frames, cpu_reference):
@@ -433,31 +468,22 @@ def ingest_section(r, cpu_reference):
     return out
 
 
-def measure_l2_gbs():
-    """Read bandwidth of a 48 MB float32 array that stays in the 126 MB L2 (torch.sum, CUDA events):
-    the denominator of the trace kernel's L2 fraction."""
-    import torch
-    x = torch.ones(12 << 20, dtype=torch.float32, device="cuda")
-    for _ in range(5):
-        x.sum()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    reps = 200
-    e0.record()
-    for _ in range(reps):
-        x.sum()
-    e1.record()
-    torch.cuda.synchronize()
-    return x.numel() * 4 * reps / (e0.elapsed_time(e1) / 1e3) / 1e9
-
-
-def blas_on_device(sd):
-    from slimtracin_b200 import api
-    r = api.Renderer(device=int(os.environ.get("LOCAL_RANK", 0)))
-    try:
-        for md in sd.meshes:
-            r.build_blas(md, api.ST_BVH_BINNED_SAH)
-    finally:
-        r.close()
+def measure_l2_gbs(device):
+    """The L2 read rate: libst_peaks.so's kernel (csrc/st_peaks.cu) reads a 48 MB buffer, which stays
+    in the 126 MB L2, 400 times in one launch with 128-bit L1-bypassing loads (CUDA events).  The
+    denominator of the trace kernel's L2 fraction."""
+    from slimtracin_b200 import build
+    L = C.CDLL(build.PEAKS_LIB)
+    L.st_peak_l2_read_gbs.argtypes = [C.c_int, C.c_uint64, C.c_int, C.POINTER(C.c_double)]
+    L.st_peak_l2_read_gbs.restype = C.c_int
+    best = 0.0
+    for _ in range(3):
+        g = C.c_double()
+        st = L.st_peak_l2_read_gbs(device, 48 << 20, 400, C.byref(g))
+        if st != 0:
+            return None
+        best = max(best, g.value)
+    return best
 
 
 def main():
@@ -468,7 +494,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the batched-views and served-stream sections")
-    ap.add_argument("--rates", default="50,200,1000,2000", help="served-stream arrival rates (req/s)")
+    ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="served-stream arrival rates (req/s)")
     ap.add_argument("--dynamic-frames", type=int, default=300, help="config-2 frames (0 skips the section)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -584,7 +610,7 @@ def main():
     mixed = None if args.no_mixed else mixed_workloads(r, sd, stream, [float(x) for x in args.rates.split(",") if x])
     dynamic = dynamic_tlas(r, args.dynamic_frames, rank == 0 and world == 1 and not args.no_cpu_baseline) \
         if args.dynamic_frames > 0 else None
-    l2_gbs = measure_l2_gbs()
+    l2_gbs = measure_l2_gbs(local)
     implicit16 = implicit16_section(r, rank == 0 and world == 1 and not args.no_cpu_baseline)
     ingest = ingest_section(r, rank == 0 and world == 1 and not args.no_cpu_baseline)
 
@@ -593,11 +619,12 @@ def main():
     peaks = measured_peaks()
     peak = peaks["hbm_gbs"] if peaks and "hbm_gbs" in peaks else 6650.0
     achieved = bytes_alg / (trace_avg_ms / 1e3) / 1e9
-    traffic = None
+    traffic, l2_traffic = None, None
     prof = os.path.join(ROOT, "profiles", "trace_kernel_mesh_1080p_traffic.json")
     if os.path.exists(prof):
         try:
-            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+            pj = json.load(open(prof))
+            traffic, l2_traffic = pj.get("dram_bytes_per_launch"), pj.get("l2_bytes_per_launch")
         except Exception:
             traffic = None
 
@@ -609,11 +636,8 @@ def main():
                 import oracle
                 if oracle.reference_available():
                     threads = os.cpu_count() or 1
-                    ref_sd = sd.copy()
-                    ref_sd.meshes = sd.meshes
-                    import tests.helpers as H
-                    H.tlas_sah(ref_sd, "ref")
-                    rays, dt, frames = cpu_reference_sample(ref_sd, cam, threads, 10.0)
+                    # the device-built BLAS and TLAS as read back: the frame the device traced
+                    rays, dt, frames = cpu_reference_sample(sd, cam, threads, 10.0)
                     cpu = {"value": rays / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "reference",
                            "sample": f"{frames} whole 1921x1081 frames of the same scene bytes, "
                                      f"{dt:.1f} s on {threads} host threads"}
@@ -625,11 +649,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded mesh scene: displaced icosphere, Perlin textures; no dataset)",
-            "config": {"workload": "1080p PBR mesh scene, depth 4, 1.31M-triangle BLAS x 8 instances",
-                       "width": WIDTH, "height": HEIGHT, "depth": DEPTH, "rays_per_frame": grid,
-                       "triangles": sd.meshes[0].triangle_count, "instances": 8, "parallelism": f"replicas x{world}",
-                       "l2": "flushed before every step (256 MiB write, outside the timed events)",
-                       "blas": "binned SAH on device", "tlas": "LBVH30 on device"},
+            "config": bench_config(world, sd.meshes[0].triangle_count, grid),
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "api": "st_upload_primitives + st_render_scene, pinned host buffers"},
             "gpu_launches": 4 * args.steps,
@@ -638,8 +658,12 @@ def main():
                          "kernel": "trace_kernel", "kernel_ms": trace_avg_ms,
                          "bytes_alg_per_launch": bytes_alg,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6.65 TB/s",
-                         "l2_peak": l2_gbs, "l2_frac": achieved / l2_gbs,
-                         "l2_peak_source": "48 MB L2-resident read (torch.sum), measured in this run"},
+                         "l2_peak": l2_gbs, "l2_frac": achieved / l2_gbs if l2_gbs else None,
+                         "l2_traffic_frac": (l2_traffic / (trace_avg_ms / 1e3) / 1e9 / l2_gbs)
+                         if (l2_gbs and l2_traffic) else None,
+                         "l2_traffic": l2_traffic,
+                         "l2_peak_source": "48 MB L2-resident buffer read 400 times in one launch "
+                                           "(csrc/st_peaks.cu, CUDA events), measured in this run"},
             "counters": counters,
             "ray_segments": {"per_frame": segments, "mrays_s": value * segments / grid,
                              "e2e_mrays_s": e2e_value * segments / grid,
@@ -649,6 +673,7 @@ def main():
             "ingest": ingest,
             "batched": mixed["batched"] if mixed else None,
             "served": mixed["served"] if mixed else None,
+            "served_knee": mixed["served_knee"] if mixed else None,
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
         }

@@ -103,7 +103,8 @@ enum st_counter {
     ST_CNT_SHADED_HITS = 7,
     ST_CNT_TEXEL_FETCHES = 8,
     ST_CNT_MESH_ENTRIES = 9,    /* BLAS traversals started */
-    ST_CNT_COUNT = 10
+    ST_CNT_TEXEL_MIP_FETCHES = 10, /* the texel fetches of ST_CNT_TEXEL_FETCHES from a mip level above 0 */
+    ST_CNT_COUNT = 11
 };
 
 /* ---- context ---------------------------------------------------------------------------------- */
@@ -225,17 +226,18 @@ typedef struct st_batch_options {
  * each view's output equals st_render_ex's. */
 ST_API int st_render_batch(st_ctx *ctx, const st_view *views, int view_count, st_batch_options *options);
 
-/* LBVH30 over device-resident boxes with no allocation.  No counterpart in the reference: its
- * builders run on the CPU (builder_top_down.h:272,366).  Same inputs and outputs as st_build_bvh
- * (ST_BVH_LBVH30), but every pointer is DEVICE memory: aabbs (6 floats per item), codes (n, may be
- * null), order (n), nodes (2n BVHNodes); info[2] is host memory.  The scratch is a static device array
- * sized for ST_NOALLOC_LBVH_MAX_ITEMS items (about 4.8 MB), so the call makes no cudaMalloc/cudaFree
- * and grows no pool: for hosts that must not allocate while other streams are busy or whose budget is
- * reserved up front.  n > ST_NOALLOC_LBVH_MAX_ITEMS returns ST_ERR_INVALID_ARG before any work.
- * The first call on a device looks up the array's address (and may load the module): make it once at
- * set-up, before any stream capture.  Calls on one device share the array: overlapping calls (threads,
- * streams or contexts of one process) race and must be serialised by the caller.  Returns after
- * `stream` (null: the context's stream) has finished the build. */
+/* LBVH30 over device-resident boxes with no allocation.  No counterpart in the reference.
+ * Same inputs and outputs as st_build_bvh (ST_BVH_LBVH30), but every pointer is DEVICE memory:
+ * aabbs (6 floats per item), codes (n, may be null), order (n), nodes (2n BVHNodes); info[2] is
+ * host memory.  The scratch is a static device array sized for ST_NOALLOC_LBVH_MAX_ITEMS items
+ * (about 4.8 MB, held by every GPU that loads the library until the process exits), so the call
+ * makes no cudaMalloc/cudaFree and grows no pool: for hosts that must not allocate while other
+ * streams are busy or whose budget is reserved up front.  n > ST_NOALLOC_LBVH_MAX_ITEMS returns
+ * ST_ERR_INVALID_ARG before any work.  Every call looks up the array's device address
+ * (cudaGetSymbolAddress); the first call on a device may also load the module, so make it once at
+ * set-up, before any stream capture.  Calls on one device share the array: overlapping calls
+ * (threads, streams or contexts of one process) race and must be serialised by the caller.
+ * Returns after `stream` (null: the context's stream) has finished the build. */
 #define ST_NOALLOC_LBVH_MAX_ITEMS 65536u
 ST_API int st_build_lbvh_noalloc(st_ctx *ctx, const float *aabbs, uint32_t n, uint32_t max_leaf, uint32_t *codes,
                                  uint32_t *order, BVHNode *nodes, uint32_t info[2], void *stream);

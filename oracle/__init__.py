@@ -97,6 +97,8 @@ def restatement():
     lib.orc_primitive_aabbs.argtypes = [C.c_void_p, C.c_void_p]
     lib.orc_binned_sah.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.orc_binned_sah.restype = C.c_int
+    lib.orc_update_mesh_bvh_binned.argtypes = [C.c_void_p]
+    lib.orc_update_mesh_bvh_binned.restype = C.c_int
     lib.orc_pick.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
     lib.orc_pick.restype = C.c_int
     lib.orc_draw_overlays.argtypes = [C.c_void_p, C.c_void_p, C.c_int]

@@ -377,6 +377,7 @@ static vec3 sample_texture(const Texture *t, vec2 UV, vec2 dUV, OTrace *tr) { /*
         while (size > 1 && level < last) { size /= 2; level += 1; }
     }
     CNT(tr, ORC_TEXEL_FETCHES);
+    if (level) CNT(tr, ORC_TEXEL_MIP_FETCHES);
     return sample_mip(t->mips + level, UV);
 }
 static vec3 sample_normal(const Texture *t, vec2 uv, vec2 dUV, OTrace *tr) { /* surface.h:131 */
@@ -1781,6 +1782,35 @@ int orc_binned_sah(const float *aabbs, uint32_t n, uint32_t max_leaf, uint32_t *
     info[0] = 1 + 2 * pairs;
     info[1] = height;
     free(cent); free(ids); free(tmp); free(cur); free(next);
+    return 0;
+}
+
+/* updateMeshBVH (builder_top_down.h:272) with the binned-SAH topology in place of the full sweep:
+ * the same padded triangle boxes (:283-318), leaves of at most MAX_TRIANGLES_PER_MESH_BVH_NODE,
+ * Triangle records in leaf order with the same precompute (:330-363), and leaf_ids mapping each
+ * source triangle to its slot (:327). */
+int orc_update_mesh_bvh_binned(Mesh *m) {
+    u32 n = m->triangle_count;
+    if (!n) return -1;
+    float *boxes = (float*)malloc(sizeof(float) * 6 * n);
+    u32 *order = (u32*)malloc(sizeof(u32) * n);
+    if (!boxes || !order) { free(boxes); free(order); return -1; }
+    for (u32 i = 0; i < n; i++) {
+        const TriangleVertexIndices *ix = m->vertex_position_indices + i;
+        AABB a = triangle_aabb(m->vertex_positions + ix->ids[0], m->vertex_positions + ix->ids[1],
+                               m->vertex_positions + ix->ids[2]);
+        memcpy(boxes + 6 * i, &a, sizeof(float) * 6);
+    }
+    u32 info[2];
+    orc_binned_sah(boxes, n, MAX_TRIANGLES_PER_MESH_BVH_NODE, order, m->bvh.nodes, info);
+    m->bvh.node_count = info[0];
+    m->bvh.height = info[1];
+    for (u32 i = 0; i < n; i++) {
+        m->bvh.leaf_ids[order[i]] = i;
+        triangle_record(m, order[i], m->triangles + i);
+    }
+    free(boxes);
+    free(order);
     return 0;
 }
 

@@ -14,7 +14,8 @@ extern "C" {
 enum {
     ORC_PRIMARY_RAYS = 0, ORC_SHADOW_RAYS = 1, ORC_BOUNCE_RAYS = 2, ORC_AABB_TESTS = 3,
     ORC_TRIANGLE_TESTS = 4, ORC_PRIMITIVE_TESTS = 5, ORC_LEAF_ID_READS = 6, ORC_SHADED_HITS = 7,
-    ORC_TEXEL_FETCHES = 8, ORC_MESH_ENTRIES = 9, ORC_COUNTERS = 16
+    ORC_TEXEL_FETCHES = 8, ORC_MESH_ENTRIES = 9, ORC_TEXEL_MIP_FETCHES = 10,
+    ORC_COUNTERS = 16
 };
 
 /* Render the whole QCAA grid of viewport->frame_buffer (clear, trace every ray, resolve to
@@ -48,6 +49,11 @@ int orc_lbvh30(const float *aabbs, uint32_t n, uint32_t max_leaf, uint32_t *code
  * height}.  Returns 0. */
 int orc_binned_sah(const float *aabbs, uint32_t n, uint32_t max_leaf, uint32_t *order, BVHNode *nodes,
                    uint32_t *info);
+
+/* updateMeshBVH (builder_top_down.h:272) with the binned-SAH topology of orc_binned_sah: fills
+ * mesh->bvh (nodes, leaf_ids as source triangle -> slot, node_count, height) and mesh->triangles
+ * in leaf order, like the library's st_update_mesh_bvh(ST_BVH_BINNED_SAH).  Returns 0. */
+int orc_update_mesh_bvh_binned(Mesh *mesh);
 
 /* The object a click at pixel (x, y) selects (manipulateSelection, viewport/manipulation.h:55):
  * found, PrimitiveType (PrimitiveType_Light for a light's glow sphere), index, world position,

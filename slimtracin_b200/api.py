@@ -19,7 +19,8 @@ ST_OK = 0
 ST_ERR_INVALID_ARG, ST_ERR_BUDGET, ST_ERR_BAD_SCENE, ST_ERR_IO = 1, 5, 9, 13
 ST_BVH_LBVH30, ST_BVH_BINNED_SAH, ST_BVH_REFIT = 1, 2, 3
 COUNTER_NAMES = ["primary_rays", "shadow_rays", "bounce_rays", "aabb_tests", "triangle_tests",
-                 "primitive_tests", "leaf_id_reads", "shaded_hits", "texel_fetches", "mesh_entries"]
+                 "primitive_tests", "leaf_id_reads", "shaded_hits", "texel_fetches", "mesh_entries",
+                 "texel_mip_fetches"]
 
 
 class st_config(C.Structure):

@@ -595,6 +595,7 @@ int st_upload_scene_bvh(st_ctx *ctx, int slot, const Scene *scene) {
     const u32t n = scene->settings.primitives;
     if (!check_bvh(scene->bvh.nodes, scene->bvh.node_count, n, scene->bvh.height)) return ST_ERR_BAD_SCENE;
     for (u32t i = 0; i < n; i++) if (scene->bvh.leaf_ids[i] >= n) return ST_ERR_BAD_SCENE;
+    S->tlas_valid = false;                      // set again by finish_tlas once the copies are done
     S->tlas_node_count = scene->bvh.node_count;
     S->tlas_height = scene->bvh.height;
     ST_CUDA(cudaMemcpyAsync(S->tlas_nodes.ptr, scene->bvh.nodes, sizeof(BVHNode) * S->tlas_node_count, cudaMemcpyHostToDevice, ctx->stream));
@@ -713,6 +714,9 @@ int st_update_scene_bvh(st_ctx *ctx, int slot, Scene *scene, int mode) {
     for (u32t i = 0; i < n; i++)
         if (S->prims_host[i].type == PrimitiveType_Mesh && (!S->meshes_valid || S->prims_host[i].id >= S->n_meshes))
             return ST_ERR_NOT_RESIDENT;
+    // A rebuild overwrites the node and leaf arrays before it can check them: until finish_tlas
+    // accepts the new tree, neither a render nor a refit may use the slot's TLAS.
+    if (mode == ST_BVH_LBVH30 || mode == ST_BVH_BINNED_SAH) S->tlas_valid = false;
     if (mode == ST_BVH_LBVH30) {
         if (lbvh_reserve(ctx->lbvh, n) != cudaSuccess) return ST_ERR_OUT_OF_MEMORY;
         launch_prim_aabbs(P<Primitive>(S->prims_raw), P<MeshDev>(S->meshes), n, ctx->lbvh.aabbs, ctx->stream);
@@ -2103,23 +2107,16 @@ constexpr size_t kNoAllocScratchBytes = lbvh_scratch_bytes(ST_NOALLOC_LBVH_MAX_I
 // the height word).  Calls that overlap on one device share this array and race.
 static __device__ __align__(256) unsigned char g_lbvh_noalloc_scratch[kNoAllocScratchBytes];
 
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mutex;
-void *g_noalloc_ptr[kNoAllocMaxDevices] = {};
-
-// The array's device address on the current device, looked up once per device (the first call
-// may load the module); the symbol itself is never handed to a kernel.
+// The array's device address on the current device.  It is looked up on every call rather than
+// cached: a cudaDeviceReset or a primary-context teardown reloads the module at another address,
+// and after the first call (which may load the module) the lookup is cheap.  The symbol itself is
+// never handed to a kernel.
 int noalloc_scratch(st_ctx *ctx, void **out) {
-    if (ctx->device < 0 || ctx->device >= kNoAllocMaxDevices) return ST_ERR_INVALID_ARG;
-    std::lock_guard<std::mutex> lk(g_noalloc_mutex);
-    if (!g_noalloc_ptr[ctx->device]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_lbvh_noalloc_scratch);
-        if (e != cudaSuccess) return fail_cuda(ctx, e);
-        if (!p || (reinterpret_cast<uintptr_t>(p) & 255)) return fail_cuda(ctx, cudaErrorInvalidSymbol);
-        g_noalloc_ptr[ctx->device] = p;
-    }
-    *out = g_noalloc_ptr[ctx->device];
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_lbvh_noalloc_scratch);
+    if (e != cudaSuccess) return fail_cuda(ctx, e);
+    if (!p || (reinterpret_cast<uintptr_t>(p) & 255)) return fail_cuda(ctx, cudaErrorInvalidSymbol);
+    *out = p;
     return ST_OK;
 }
 

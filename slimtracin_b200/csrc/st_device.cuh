@@ -24,7 +24,7 @@ typedef uint32_t u32t;
 
 constexpr int kStack = 64;   // traversal stack entries; uploads and builds refuse BVHs with height + 2 > kStack
 constexpr unsigned kNoPair = 0xFFFFFFFFu;   // "no node pair": the walk has nothing left to visit
-enum Counter { C_PRIMARY = 0, C_SHADOW, C_BOUNCE, C_AABB, C_TRI, C_PRIM, C_LEAF, C_SHADE, C_TEXEL, C_MESH, C_COUNT };
+enum Counter { C_PRIMARY = 0, C_SHADOW, C_BOUNCE, C_AABB, C_TRI, C_PRIM, C_LEAF, C_SHADE, C_TEXEL, C_MESH, C_TEXEL_MIP, C_COUNT };
 enum Status { S_STACK_OVERFLOW = 1 };
 
 struct __align__(16) NodePair {

@@ -286,6 +286,7 @@ __device__ v3 sample_texture(TState<CNT, SHS> &t, const SceneDev &S, u32t tex, f
         while (size > 1 && level < last) { size /= 2; level += 1; }
     }
     t.count(C_TEXEL);
+    if (level) t.count(C_TEXEL_MIP);
     MipDev m = S.mips[T.mip_offset + level];                         // sampleTextureMip :5
     float u = U0, v = V0;
     if (u > 1) u -= (float)((u32t)u);

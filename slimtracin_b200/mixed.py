@@ -129,6 +129,11 @@ class PerFrame:
             if s:
                 self.r._check(s, "st_render_ex")
 
+    def device_ms(self):
+        """Of the last run: the summed CUDA-event times of the views' whole renders and of their
+        trace kernels alone."""
+        return sum(o.total_ms for o in self.opts), sum(o.trace_ms for o in self.opts)
+
 
 class Batch:
     """The same views in one st_render_batch call (device outputs, autotuned, CUDA graph)."""

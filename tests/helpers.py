@@ -19,20 +19,76 @@ def tlas_sah(sd, which="orc"):
 
 
 def blas_sah(md, which="orc"):
-    """The reference's BLAS build (updateMeshBVH) into md via the oracle or the reference."""
+    """The reference's BLAS build (updateMeshBVH) into md via the oracle or the reference;
+    which="binned": the oracle's updateMeshBVH with the binned-SAH topology (the library's
+    ST_BVH_BINNED_SAH build)."""
     keep = []
     md.allocate_bvh()
     m = md.to_ctypes(keep)
     if which == "orc":
         oracle.restatement().orc_update_mesh_bvh(C.byref(m))
+    elif which == "binned":
+        assert oracle.restatement().orc_update_mesh_bvh_binned(C.byref(m)) == 0
     else:
         oracle.reference().ref_update_mesh_bvh(C.byref(m))
     md.read_back(m)
     return md
 
 
-def oracle_frame(sd, cam, w, h, depth=2, mode=S.RM_BEAUTY, cone_angle=0.0, threads=8, counters=False):
+def tlas_lbvh(sd):
+    """The scene's TLAS as the library's ST_BVH_LBVH30 builds it (the oracle's LBVH30 over the
+    primitives' world boxes, leaves of at most 2), written into sd's BVH arrays."""
+    orc = oracle.restatement()
+    sc, keep = sd.to_ctypes()
+    n = len(sd.primitives)
+    boxes = np.zeros((n, 6), np.float32)
+    orc.orc_primitive_aabbs(C.byref(sc), boxes.ctypes.data)
+    codes, order = np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+    nodes, info = np.zeros(2 * n, dtype=S.BVHNODE_DT), np.zeros(2, np.uint32)
+    leaf = np.zeros(n, np.uint32)
+    orc.orc_lbvh30(boxes.ctypes.data, n, 2, codes.ctypes.data, order.ctypes.data, nodes.ctypes.data,
+                   leaf.ctypes.data, info.ctypes.data)
+    sd.tlas_nodes[:info[0]] = nodes[:info[0]]
+    sd.tlas_leaf_ids[:n] = leaf
+    sd.tlas_node_count, sd.tlas_height = int(info[0]), int(info[1])
+    return sd
+
+
+def tlas_binned(sd):
+    """The scene's TLAS as the library's ST_BVH_BINNED_SAH builds it (the oracle's binned SAH over
+    the primitives' world boxes, leaves of at most 2), written into sd's BVH arrays."""
+    orc = oracle.restatement()
+    sc, keep = sd.to_ctypes()
+    n = len(sd.primitives)
+    boxes = np.zeros((n, 6), np.float32)
+    orc.orc_primitive_aabbs(C.byref(sc), boxes.ctypes.data)
+    order = np.zeros(n, np.uint32)
+    nodes, info = np.zeros(2 * n, dtype=S.BVHNODE_DT), np.zeros(2, np.uint32)
+    orc.orc_binned_sah(boxes.ctypes.data, n, 2, order.ctypes.data, nodes.ctypes.data, info.ctypes.data)
+    sd.tlas_nodes[:info[0]] = nodes[:info[0]]
+    sd.tlas_leaf_ids[:n] = order
+    sd.tlas_node_count, sd.tlas_height = int(info[0]), int(info[1])
+    return sd
+
+
+def same_tlas(a, b):
+    """Two scenes hold byte-identical TLAS node arrays and leaf lists."""
+    n = len(a.primitives)
+    return (a.tlas_node_count == b.tlas_node_count and a.tlas_height == b.tlas_height
+            and a.tlas_nodes[:a.tlas_node_count].tobytes() == b.tlas_nodes[:b.tlas_node_count].tobytes()
+            and np.array_equal(a.tlas_leaf_ids[:n], b.tlas_leaf_ids[:n]))
+
+
+def cone_angle_for(height, focal_length):
+    """The ray-cone spread angle of one pixel row: atan(2 / (H * focal_length))."""
+    import math
+    return float(np.float32(math.atan(2.0 / (height * focal_length))))
+
+
+def oracle_frame(sd, cam, w, h, depth=2, mode=S.RM_BEAUTY, cone_angle=0.0, threads=None, counters=False):
     """The oracle's render: SSB update on a copy of the primitives, then the frame."""
+    import os
+    threads = threads or min(os.cpu_count() or 1, 64)
     orc = oracle.restatement()
     d = sd.copy()
     sc, keep = d.to_ctypes()

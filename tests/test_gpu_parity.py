@@ -63,14 +63,14 @@ def test_counters_match_oracle(renderer):
     renderer.upload(3, sd, tlas="host")
     g = H.gpu_frame(renderer, 3, sd, cam, 160, 90, depth=4, counters=True)
     o = H.oracle_frame(sd, cam, 160, 90, depth=4)
-    print("gpu", g.counters[:10], "oracle", o.counters[:10])
-    assert np.array_equal(g.counters[:10], o.counters[:10])
+    print("gpu", g.counters[:11], "oracle", o.counters[:11])
+    assert np.array_equal(g.counters[:11], o.counters[:11])
     sd0, cam0 = scenes.example_area_lights()
     H.tlas_sah(sd0)
     renderer.upload(3, sd0, tlas="host")
     g = H.gpu_frame(renderer, 3, sd0, cam0, 160, 120, depth=2, counters=True)
     o = H.oracle_frame(sd0, cam0, 160, 120, depth=2)
-    assert np.array_equal(g.counters[:10], o.counters[:10]), (g.counters[:10], o.counters[:10])
+    assert np.array_equal(g.counters[:11], o.counters[:11]), (g.counters[:11], o.counters[:11])
 
 
 def test_moving_scene_primary_tlas(renderer):

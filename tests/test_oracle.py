@@ -59,6 +59,30 @@ def test_oracle_matches_reference_live(case, mode):
 
 
 @needs_ref
+@pytest.mark.parametrize("mode", [S.RM_BEAUTY, S.RM_NORMALS])
+def test_oracle_matches_reference_with_ray_cones(mode):
+    """Ray-cone mip selection (common.h:336, texture.h:32): with projection_plane.cone_angle set to
+    atan(2 / (H * focal_length)) the footprint of a hit spans several texels of the 256^2 textures,
+    so mips above 0 are sampled; every byte equals the reference's, and the oracle's counters show
+    the fetches above mip 0."""
+    sd, cam = scenes.mesh_scene(subdivisions=3, texture_size=256)
+    H.blas_sah(sd.meshes[0], "ref")
+    H.tlas_sah(sd, "ref")
+    w, h = 192, 108
+    cone = H.cone_angle_for(h, cam.focal_length)
+    r = H.reference_frame(sd, cam, w, h, depth=4, mode=mode, cone_angle=cone)
+    o = H.oracle_frame(sd, cam, w, h, depth=4, mode=mode, cone_angle=cone)
+    assert np.array_equal(r.float_pixels.view(np.uint8), o.float_pixels.view(np.uint8))
+    assert np.array_equal(r.pixels.view(np.uint8).reshape(-1, 4)[:, :3], o.pixels.view(np.uint8).reshape(-1, 4)[:, :3])
+    fetches, above0 = int(o.counters[8]), int(o.counters[10])
+    assert fetches > 0 and 0 < above0 <= fetches, (fetches, above0)
+    # the same view without the cone samples mip 0 only, and looks different
+    o0 = H.oracle_frame(sd, cam, w, h, depth=4, mode=mode)
+    assert int(o0.counters[10]) == 0
+    assert not np.array_equal(o0.float_pixels.view(np.uint8), o.float_pixels.view(np.uint8))
+
+
+@needs_ref
 @pytest.mark.parametrize("w,h,yaw", [(1, 1, 0.0), (2, 3, 0.0), (33, 17, 0.0), (127, 65, 0.0), (64, 48, float(np.pi))])
 def test_oracle_matches_reference_ragged_and_empty_views(w, h, yaw):
     """Grids smaller than a block or tile, and a camera facing away from every primitive."""

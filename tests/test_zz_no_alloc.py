@@ -52,6 +52,35 @@ def test_noalloc_lbvh_equals_allocating_build_twice_in_a_row(renderer):
         assert np.array_equal(nodes.view(np.uint8), rn.view(np.uint8))
 
 
+def test_noalloc_lbvh_allocates_nothing():
+    """A fresh context (its pooled builder scratch never reserved): after a warm-up call has loaded the
+    module, a second call leaves the context's device bytes and the device's free memory unchanged."""
+    import torch
+    n, max_leaf = 20000, 2
+    boxes = _boxes(n, 11)
+    d_boxes = torch.from_numpy(boxes).cuda()
+    d_codes = torch.zeros(n, dtype=torch.int32, device="cuda")
+    d_order = torch.zeros(n, dtype=torch.int32, device="cuda")
+    d_nodes = torch.zeros(2 * n * S.BVHNODE_DT.itemsize, dtype=torch.uint8, device="cuda")
+    info = (C.c_uint32 * 2)()
+    with api.Renderer(device=0) as r:
+        def call():
+            r._check(r.L.st_build_lbvh_noalloc(r.ctx, d_boxes.data_ptr(), n, max_leaf, d_codes.data_ptr(),
+                                               d_order.data_ptr(), d_nodes.data_ptr(), info, None),
+                     "st_build_lbvh_noalloc")
+        call()
+        torch.cuda.synchronize()
+        in_use, free = int(r.L.st_device_bytes_in_use(r.ctx)), torch.cuda.mem_get_info()[0]
+        first = d_nodes.cpu().numpy().copy()
+        d_nodes.zero_()
+        torch.cuda.synchronize()
+        call()
+        torch.cuda.synchronize()
+        assert int(r.L.st_device_bytes_in_use(r.ctx)) == in_use
+        assert torch.cuda.mem_get_info()[0] == free
+        assert np.array_equal(d_nodes.cpu().numpy(), first)
+
+
 def test_noalloc_lbvh_refuses_more_than_its_scratch(renderer):
     import torch
     buf = torch.zeros(64, dtype=torch.int32, device="cuda")
