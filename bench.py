@@ -53,17 +53,13 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-from slimtracin_b200 import scenes, structs as S  # noqa: E402
+from slimtracin_b200 import dist as D, scenes, structs as S  # noqa: E402
 
 WIDTH, HEIGHT, DEPTH = 1920, 1080, 4
 METRIC = "Mrays/s at 1080p PBR mesh scene; p50/p99 latency, served vs per-frame launch"
 # bytes per event of the algorithmic traffic model (reference traversal, counted on the device)
 BYTES = {"aabb_tests": 32, "triangle_tests": 64, "primitive_tests": 72, "leaf_id_reads": 4,
          "shaded_hits": 84 + 64, "texel_fetches": 12, "primary_rays": 24}
-
-
-def dist_env():
-    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
 def build_scene(seed_offset=0):
@@ -177,7 +173,7 @@ def reference_scene():
 
 
 def run_reference_arm(args):
-    rank, world, _ = dist_env()
+    rank, world, _ = D.env()
     if rank != 0:
         return 0
     import oracle
@@ -277,7 +273,8 @@ def mixed_workloads(r, big_sd, stream, rates):
                "speedup_bound_if_gaps_removed": pf_ms / pf_trace_ms,
                "tile_shape": batch.opt.tile_shape_used,
                "stack_placement": batch.opt.stack_placement_used, "launch_mode": batch.opt.launch_mode_used,
-               "chunk": batch.opt.chunk_used, "graph_replayed": batch.opt.graph_replayed}
+               "chunk": batch.opt.chunk_used, "graph_replayed": batch.opt.graph_replayed,
+               "compaction_threshold": batch.opt.compaction_threshold_used, "parked_rays": batch.opt.parked_rays}
     del fbuf, ubuf, one_f, one_u
     served = []
     if rates:
@@ -505,7 +502,7 @@ def main():
     import torch.distributed as dist
     from slimtracin_b200 import api, build
 
-    rank, world, local = dist_env()
+    rank, world, local = D.env()
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
@@ -559,11 +556,8 @@ def main():
             trace_ms.append(o.trace_ms)
         torch.cuda.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in evs]
-    total_ms = sum(step_ms)
+    total_ms = D.max_over_ranks(sum(step_ms), device="cuda")       # the slowest rank's device time
     if world > 1:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
         dist.barrier()
     ms_per_step = total_ms / args.steps
     value = world * grid / (ms_per_step / 1e3) / 1e6
@@ -598,11 +592,7 @@ def main():
     with torch.cuda.stream(stream):
         e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = D.max_over_ranks(e0.elapsed_time(e1), device="cuda")
     e2e_value = world * grid * args.steps / (e2e_ms / 1e3) / 1e6
     h2d = len(prim_view) * S.PRIMITIVE_DT.itemsize
     d2h = grid * 24 + WIDTH * HEIGHT * 4

@@ -52,7 +52,10 @@ enum st_status {
 enum st_bvh_mode {
     ST_BVH_LBVH30 = 1,      /* 30-bit Morton LBVH: device radix sort, Karras topology, leaf collapse */
     ST_BVH_BINNED_SAH = 2,  /* breadth-first binned SAH (32 bins) on the device */
-    ST_BVH_REFIT = 3        /* keep the resident topology, recompute every AABB bottom-up */
+    ST_BVH_REFIT = 3,       /* keep the resident topology, recompute every AABB bottom-up */
+    ST_BVH_REF_SAH = 4      /* the reference's own full-sweep SAH (buildBVH, builder_top_down.h:204), node
+                               for node; for TLASes, whose topology decides which occluder a shadow ray
+                               meets first (st_update_scene_bvh, st_build_bvh; not for BLASes) */
 };
 
 typedef struct st_config {
@@ -217,6 +220,12 @@ typedef struct st_batch_options {
                                    ST_LAUNCH_PERSISTENT (1); tile_shape, chunk and stack_placement apply to
                                    the persistent kernel */
     int launch_mode_used;       /* out (per view: tile_shape_used and stack_placement_used are -1) */
+    int compaction_threshold;   /* persistent kernel, warp-vote ray compaction: at a bounce, a warp whose
+                                   lanes still tracing number fewer than this parks their paths in a queue
+                                   that a second persistent pass traces to the end (outputs unchanged);
+                                   -1: autotuned, 0: off, 1..32 */
+    int compaction_threshold_used;   /* out */
+    uint64_t parked_rays;       /* out: paths parked by the compaction and traced by the second pass */
 } st_batch_options;
 
 /* Render `view_count` views (different sizes, scenes, render modes and bounce counts) in one call:

@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(HERE, "libslimtracin_b200.so")
 
 ST_OK = 0
 ST_ERR_INVALID_ARG, ST_ERR_BUDGET, ST_ERR_BAD_SCENE, ST_ERR_IO = 1, 5, 9, 13
-ST_BVH_LBVH30, ST_BVH_BINNED_SAH, ST_BVH_REFIT = 1, 2, 3
+ST_BVH_LBVH30, ST_BVH_BINNED_SAH, ST_BVH_REFIT, ST_BVH_REF_SAH = 1, 2, 3, 4
 COUNTER_NAMES = ["primary_rays", "shadow_rays", "bounce_rays", "aabb_tests", "triangle_tests",
                  "primitive_tests", "leaf_id_reads", "shaded_hits", "texel_fetches", "mesh_entries",
                  "texel_mip_fetches"]
@@ -49,7 +49,9 @@ class st_batch_options(C.Structure):
                 ("use_graph", C.c_int), ("batch_ms", C.c_float), ("rays", C.c_uint64),
                 ("tile_shape_used", C.c_int), ("chunk_used", C.c_int), ("graph_replayed", C.c_int),
                 ("stack_placement", C.c_int), ("stack_placement_used", C.c_int),
-                ("launch_mode", C.c_int), ("launch_mode_used", C.c_int)]
+                ("launch_mode", C.c_int), ("launch_mode_used", C.c_int),
+                ("compaction_threshold", C.c_int), ("compaction_threshold_used", C.c_int),
+                ("parked_rays", C.c_uint64)]
 
 
 class st_serve_config(C.Structure):
@@ -278,7 +280,7 @@ class Renderer:
 
 
 def render_batch(renderer, items, tile_shape=-1, chunk=0, use_graph=False, device_outputs=False, stack_placement=-1,
-                 launch_mode=LAUNCH_AUTOTUNED):
+                 launch_mode=LAUNCH_AUTOTUNED, compaction_threshold=0):
     """st_render_batch over items = [(slot, SceneData, Frame)]; outputs go to each Frame's buffers
     (host) unless device_outputs, in which case Frame.grid pointers are used as device pointers."""
     keep = []
@@ -295,6 +297,7 @@ def render_batch(renderer, items, tile_shape=-1, chunk=0, use_graph=False, devic
     opt.tile_shape, opt.chunk, opt.use_graph, opt.device_outputs = tile_shape, chunk, int(use_graph), int(device_outputs)
     opt.stack_placement = stack_placement
     opt.launch_mode = launch_mode
+    opt.compaction_threshold = compaction_threshold
     renderer._check(renderer.L.st_render_batch(renderer.ctx, views, len(items), C.byref(opt)), "st_render_batch")
     return opt
 

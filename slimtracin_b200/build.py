@@ -14,7 +14,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libslimtracin_b200.so")
 PEAKS_LIB = os.path.join(HERE, "libst_peaks.so")      # bench.py's L2 read-rate measurement
 PEAKS_SRC = "st_peaks.cu"
-SOURCES = ["st_api.cu", "st_render.cu", "st_bvh.cu", "st_sah.cu", "st_overlay.cu", "st_texture.cu", "st_io.cu", "st_obj.cu"]
+SOURCES = ["st_api.cu", "st_render.cu", "st_bvh.cu", "st_sah.cu", "st_refsah.cu", "st_overlay.cu", "st_texture.cu", "st_io.cu", "st_obj.cu"]
 HEADERS = ["st_device.cuh", "st_trace.cuh", "st_kernels.h"]
 INCLUDES = [os.path.join(ROOT, "include"), CSRC]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",

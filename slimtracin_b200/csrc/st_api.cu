@@ -70,8 +70,15 @@ DevBuf *motion_field(SceneSlot &S, MotionBufs &m, int k, DevBuf **mine) {
 
 }  // namespace
 
+// A scene class's tuned batch launch: kernel variant (or kPerViewVariant), queue chunk and the
+// warp-vote compaction threshold (0: no parking).
+struct Tuned {
+    int variant = 0, chunk = 1, threshold = 0;
+};
+
 struct BatchState {
     DevBuf table, ssb, seg, out_float, out_u8, counter;
+    DevBuf park;                        // the parked-ray queue (ParkedRay records), when compaction is on
     BatchView *staging = nullptr;       // pinned host copy of the device view table
     size_t staging_cap = 0;
     BatchTable host_table;              // the view table of the launch group being issued (a kernel parameter)
@@ -81,7 +88,7 @@ struct BatchState {
     cudaEvent_t fork_ev = nullptr, join_ev[kAuxStreams] = {};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    std::map<std::string, std::pair<int, int>> tuned;   // scene-class key -> (kernel variant, chunk)
+    std::map<std::string, Tuned> tuned;                 // scene-class key -> tuned launch
 };
 
 struct ServeReq {
@@ -373,10 +380,18 @@ int st_init(st_ctx **out, const st_config *cfg) {
     cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
     for (int t = 0; t < BATCH_VARIANTS; t++) ctx->blocks_per_sm[t] = batch_blocks_per_sm(t);
     if (const char *path = getenv("ST_AUTOTUNE_CACHE")) {
+        // one line per scene class: key, kernel variant, chunk, compaction threshold
         std::ifstream f(path);
-        std::string key;
-        int tile, chunk;
-        while (f >> key >> tile >> chunk) ctx->batch.tuned[key] = {tile, chunk};
+        std::string line;
+        while (std::getline(f, line)) {
+            std::istringstream in(line);
+            std::string key;
+            Tuned t;
+            if (in >> key >> t.variant >> t.chunk) {
+                if (!(in >> t.threshold)) t.threshold = 0;
+                ctx->batch.tuned[key] = t;
+            }
+        }
     }
     int s = reserve(ctx, ctx->status, 16);
     if (s == ST_OK) s = reserve(ctx, ctx->counters, sizeof(unsigned long long) * 16);
@@ -595,13 +610,16 @@ int st_upload_scene_bvh(st_ctx *ctx, int slot, const Scene *scene) {
     const u32t n = scene->settings.primitives;
     if (!check_bvh(scene->bvh.nodes, scene->bvh.node_count, n, scene->bvh.height)) return ST_ERR_BAD_SCENE;
     for (u32t i = 0; i < n; i++) if (scene->bvh.leaf_ids[i] >= n) return ST_ERR_BAD_SCENE;
-    S->tlas_valid = false;                      // set again by finish_tlas once the copies are done
     S->tlas_node_count = scene->bvh.node_count;
     S->tlas_height = scene->bvh.height;
-    ST_CUDA(cudaMemcpyAsync(S->tlas_nodes.ptr, scene->bvh.nodes, sizeof(BVHNode) * S->tlas_node_count, cudaMemcpyHostToDevice, ctx->stream));
-    ST_CUDA(cudaMemcpyAsync(S->tlas_leaf_ids.ptr, scene->bvh.leaf_ids, sizeof(u32t) * n, cudaMemcpyHostToDevice, ctx->stream));
+    cudaError_t e = cudaMemcpyAsync(S->tlas_nodes.ptr, scene->bvh.nodes, sizeof(BVHNode) * S->tlas_node_count,
+                                    cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(S->tlas_leaf_ids.ptr, scene->bvh.leaf_ids, sizeof(u32t) * n, cudaMemcpyHostToDevice, ctx->stream);
     S->moved_since_build = 0;
-    return finish_tlas(ctx, *S);
+    const int status = e == cudaSuccess ? finish_tlas(ctx, *S) : fail_cuda(ctx, e);
+    if (status != ST_OK) S->tlas_valid = false;     // the arrays may hold part of the new tree
+    return status;
 }
 
 int st_upload_mesh_bvhs(st_ctx *ctx, int slot, const Scene *scene) {
@@ -705,18 +723,28 @@ int st_update_primitives(st_ctx *ctx, int slot, const Primitive *primitives, con
     return ST_CUDA_SYNC(ctx);
 }
 
+static int update_scene_bvh(st_ctx *ctx, SceneSlot *S, Scene *scene, int mode);
+
 int st_update_scene_bvh(st_ctx *ctx, int slot, Scene *scene, int mode) {
     SceneSlot *S = slot_of(ctx, slot);
     if (!S || !S->allocated) return ST_ERR_NOT_RESIDENT;
+    if (mode != ST_BVH_LBVH30 && mode != ST_BVH_BINNED_SAH && mode != ST_BVH_REFIT && mode != ST_BVH_REF_SAH)
+        return ST_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
     const u32t n = S->n_prims;
     if (!n) return ST_ERR_BAD_SCENE;
     for (u32t i = 0; i < n; i++)
         if (S->prims_host[i].type == PrimitiveType_Mesh && (!S->meshes_valid || S->prims_host[i].id >= S->n_meshes))
             return ST_ERR_NOT_RESIDENT;
-    // A rebuild overwrites the node and leaf arrays before it can check them: until finish_tlas
-    // accepts the new tree, neither a render nor a refit may use the slot's TLAS.
-    if (mode == ST_BVH_LBVH30 || mode == ST_BVH_BINNED_SAH) S->tlas_valid = false;
+    // An update writes the node and leaf arrays (or the boxes) before it can check them: one that
+    // fails part way leaves no TLAS that a render or a refit may use, until a later build succeeds.
+    const int status = update_scene_bvh(ctx, S, scene, mode);
+    if (status != ST_OK) S->tlas_valid = false;
+    return status;
+}
+
+static int update_scene_bvh(st_ctx *ctx, SceneSlot *S, Scene *scene, int mode) {
+    const u32t n = S->n_prims;
     if (mode == ST_BVH_LBVH30) {
         if (lbvh_reserve(ctx->lbvh, n) != cudaSuccess) return ST_ERR_OUT_OF_MEMORY;
         launch_prim_aabbs(P<Primitive>(S->prims_raw), P<MeshDev>(S->meshes), n, ctx->lbvh.aabbs, ctx->stream);
@@ -738,6 +766,15 @@ int st_update_scene_bvh(st_ctx *ctx, int slot, Scene *scene, int mode) {
         S->tlas_node_count = info[0];
         S->tlas_height = info[1];
         if (S->tlas_height + 2 > (u32t)kStack) return ST_ERR_BAD_SCENE;
+    } else if (mode == ST_BVH_REF_SAH) {
+        if (lbvh_reserve(ctx->lbvh, n) != cudaSuccess) return ST_ERR_OUT_OF_MEMORY;
+        launch_prim_aabbs(P<Primitive>(S->prims_raw), P<MeshDev>(S->meshes), n, ctx->lbvh.aabbs, ctx->stream);
+        u32t info[2];
+        cudaError_t e = refsah_build(ctx->lbvh.aabbs, n, MAX_OBJS_PER_SCENE_BVH_NODE, P<BVHNode>(S->tlas_nodes),
+                                     P<u32t>(S->tlas_leaf_ids), info, ctx->stream);
+        if (e != cudaSuccess) return fail_cuda(ctx, e);
+        S->tlas_node_count = info[0];
+        S->tlas_height = info[1];
     } else if (mode == ST_BVH_REFIT) {
         if (!S->tlas_valid) return ST_ERR_NOT_RESIDENT;
         launch_prim_aabbs(P<Primitive>(S->prims_raw), P<MeshDev>(S->meshes), n, P<float>(S->tlas_aabbs), ctx->stream);
@@ -840,7 +877,7 @@ int st_update_mesh_bvh(st_ctx *ctx, Mesh *mesh, int mode) {
 int st_build_bvh(st_ctx *ctx, int mode, const float *aabbs, uint32_t n, uint32_t max_leaf, uint32_t *codes,
                  uint32_t *order, BVHNode *nodes, uint32_t info[2]) {
     if (!ctx || !aabbs || !nodes || !order || !info || n == 0 || max_leaf == 0 || max_leaf > 0xFFFF ||
-        (mode != ST_BVH_LBVH30 && mode != ST_BVH_BINNED_SAH))
+        (mode != ST_BVH_LBVH30 && mode != ST_BVH_BINNED_SAH && mode != ST_BVH_REF_SAH))
         return ST_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
     if (lbvh_reserve(ctx->lbvh, n) != cudaSuccess) return ST_ERR_OUT_OF_MEMORY;
@@ -854,9 +891,10 @@ int st_build_bvh(st_ctx *ctx, int mode, const float *aabbs, uint32_t n, uint32_t
     u32t *d_codes = d_order + n;
     cudaMemcpyAsync(ctx->lbvh.aabbs, aabbs, sizeof(float) * 6 * (size_t)n, cudaMemcpyHostToDevice, st);
     u32t inf[2];
-    cudaError_t e = mode == ST_BVH_LBVH30 ? lbvh_build(ctx->lbvh, n, max_leaf, d_nodes, d_order, inf, st)
-                                          : sah_build(ctx->lbvh.aabbs, n, max_leaf, d_nodes, d_order, inf, st, ctx->sah_scratch.ptr,
-                                                    ctx->sah_scratch.bytes);
+    cudaError_t e = mode == ST_BVH_LBVH30     ? lbvh_build(ctx->lbvh, n, max_leaf, d_nodes, d_order, inf, st)
+                    : mode == ST_BVH_REF_SAH ? refsah_build(ctx->lbvh.aabbs, n, max_leaf, d_nodes, d_order, inf, st)
+                                             : sah_build(ctx->lbvh.aabbs, n, max_leaf, d_nodes, d_order, inf, st,
+                                                         ctx->sah_scratch.ptr, ctx->sah_scratch.bytes);
     if (e == cudaSuccess) {
         if (mode == ST_BVH_LBVH30) launch_codes_by_item(ctx->lbvh, n, d_codes, st);
         else codes = nullptr;
@@ -1164,8 +1202,8 @@ int plan_batch(st_ctx *ctx, const st_view *views, int n, int tile, const st_batc
 // (the persistent kernel over the group's tiles, or with kPerViewVariant one trace kernel per view
 // spread over the batch's aux streams), and the resolves of the views that want a frame.  The
 // set-up and resolve launches carry the group's view table as their kernel parameter.
-int launch_groups(st_ctx *ctx, BatchState &B, const BatchPlan &p, int tile, u32t chunk, unsigned *status,
-                  cudaStream_t st) {
+int launch_groups(st_ctx *ctx, BatchState &B, const BatchPlan &p, int tile, u32t chunk, u32t threshold,
+                  unsigned *status, cudaStream_t st) {
     const int n = (int)p.table.size();
     if (tile == kPerViewVariant) {
         // one per-frame trace kernel per view, the views spread over the auxiliary streams (the
@@ -1223,10 +1261,24 @@ int launch_groups(st_ctx *ctx, BatchState &B, const BatchPlan &p, int tile, u32t
                 max_h = std::max(max_h, b.view.grid_h - 1);
             }
         }
+        // the tile counter, and the parked-ray queue's reserved and drained counts
         ST_CUDA(cudaMemsetAsync(B.counter.ptr, 0, 16, st));
+        ParkQueue park;
+        if (threshold) {
+            park.rays = P<ParkedRay>(B.park);
+            park.reserved = P<u32t>(B.counter) + 1;
+            park.taken = P<u32t>(B.counter) + 2;
+            park.drained = P<u32t>(B.counter) + 4;
+            park.capacity = (u32t)(B.park.bytes / sizeof(ParkedRay));
+            park.threshold = threshold;
+        }
         launch_batch_setup(B.host_table, (u32t)gn, max_prims, max_rows, st);
         if (launch_batch(P<BatchView>(B.table) + g0, (u32t)gn, end - first, tile, chunk, blocks, P<u32t>(B.counter),
-                         status, P<unsigned long long>(ctx->counters), false, st) != 0)
+                         status, P<unsigned long long>(ctx->counters), false, st, park) != 0)
+            return ST_ERR_INVALID_ARG;
+        if (threshold &&
+            launch_drain(P<BatchView>(B.table) + g0, park, tile, blocks, status, P<unsigned long long>(ctx->counters),
+                         false, st) != 0)
             return ST_ERR_INVALID_ARG;
         if (max_w) launch_batch_resolve(B.host_table, (u32t)gn, max_w, max_h, st);
     }
@@ -1234,7 +1286,7 @@ int launch_groups(st_ctx *ctx, BatchState &B, const BatchPlan &p, int tile, u32t
 }
 
 int enqueue_batch(st_ctx *ctx, BatchState &B, unsigned *status, const st_view *views, int n, BatchPlan &p, int tile,
-                  u32t chunk, cudaStream_t st, const st_batch_options &o) {
+                  u32t chunk, u32t threshold, cudaStream_t st, const st_batch_options &o) {
     // per-view pointers into the arena (or the caller's device outputs)
     for (int i = 0; i < n; i++) {
         BatchView &b = p.table[i];
@@ -1246,7 +1298,8 @@ int enqueue_batch(st_ctx *ctx, BatchState &B, unsigned *status, const st_view *v
                    : o.device_outputs ? reinterpret_cast<uint32_t *>(views[i].out_u8) : P<uint32_t>(B.out_u8) + p.u8_off[i];
     }
     ST_CUDA(cudaMemsetAsync(status, 0, 16, st));
-    return launch_groups(ctx, B, p, tile, chunk, status, st);
+    ST_CUDA(cudaMemsetAsync(P<u32t>(B.counter) + 4, 0, 4, st));   // the batch's parked-path total
+    return launch_groups(ctx, B, p, tile, chunk, threshold, status, st);
 }
 
 // Device and pinned room for n views' table (grown geometrically: cudaFreeHost waits for the device).
@@ -1263,30 +1316,34 @@ int table_reserve(st_ctx *ctx, BatchState &B, int n) {
     return ST_OK;
 }
 
-int batch_reserve(st_ctx *ctx, BatchState &B, const BatchPlan &p, int n) {
+int batch_reserve(st_ctx *ctx, BatchState &B, const BatchPlan &p, int n, u32t threshold) {
     ST_TRY(table_reserve(ctx, B, n));
+    // the parked-ray queue: room for every ray of the batch, at most kParkCapacity (a launch group's
+    // parks beyond it are traced in place)
+    if (threshold) ST_TRY(reserve(ctx, B.park, sizeof(ParkedRay) * (size_t)std::min<uint64_t>(p.rays, kParkCapacity)));
     ST_TRY(reserve(ctx, B.ssb, sizeof(int4) * p.ssb_total));
     ST_TRY(reserve(ctx, B.seg, sizeof(float) * p.seg_total));
     ST_TRY(reserve(ctx, B.out_float, sizeof(FloatPixel) * std::max(p.float_total, (size_t)1)));
     ST_TRY(reserve(ctx, B.out_u8, sizeof(uint32_t) * std::max(p.u8_total, (size_t)1)));
-    ST_TRY(reserve(ctx, B.counter, 16));
+    ST_TRY(reserve(ctx, B.counter, 32));     // per group: tile counter, queue counts; then the parked total
     return ST_OK;
 }
 
 }  // namespace
 
-// One autotuning trial: the batch run twice with one kernel variant and chunk, the faster device
-// time kept (the first run also absorbs one-time costs such as the per-view streams' creation).
-static int time_batch(st_ctx *ctx, BatchState &B, const st_view *views, int n, int variant, u32t chunk, cudaStream_t st,
-                      const st_batch_options &o, float &best_ms) {
+// One autotuning trial: the batch run twice with one kernel variant, chunk and compaction threshold,
+// the faster device time kept (the first run also absorbs one-time costs such as the per-view
+// streams' creation).
+static int time_batch(st_ctx *ctx, BatchState &B, const st_view *views, int n, int variant, u32t chunk, u32t threshold,
+                      cudaStream_t st, const st_batch_options &o, float &best_ms) {
     BatchPlan q;
     ST_TRY(plan_batch(ctx, views, n, variant, o, q));
-    ST_TRY(batch_reserve(ctx, B, q, n));
+    ST_TRY(batch_reserve(ctx, B, q, n, threshold));
     if (variant == kPerViewVariant) ST_CUDA(ensure_aux(B));
     best_ms = INFINITY;
     for (int rep = 0; rep < 2; rep++) {
         ST_CUDA(cudaEventRecord(ctx->ev[0], st));
-        ST_TRY(enqueue_batch(ctx, B, P<unsigned>(ctx->status), views, n, q, variant, chunk, st, o));
+        ST_TRY(enqueue_batch(ctx, B, P<unsigned>(ctx->status), views, n, q, variant, chunk, threshold, st, o));
         ST_CUDA(cudaEventRecord(ctx->ev[1], st));
         ST_CUDA(cudaStreamSynchronize(st));
         float ms = 0;
@@ -1304,13 +1361,14 @@ int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *
     dflt.tile_shape = -1;
     dflt.stack_placement = -1;
     dflt.launch_mode = ST_LAUNCH_AUTOTUNED;
+    dflt.compaction_threshold = -1;
     st_batch_options &o = opt ? *opt : dflt;
     cudaStream_t st = o.stream ? (cudaStream_t)o.stream : ctx->stream;
     BatchState &B = ctx->batch;
     // the kernel variant (tile shape, stack placement) and queue chunk: given, cached for this scene
     // class, or tuned now
     if (o.tile_shape >= TILE_SHAPES || o.stack_placement >= STACK_PLACEMENTS || o.launch_mode < ST_LAUNCH_AUTOTUNED ||
-        o.launch_mode > ST_LAUNCH_PERSISTENT)
+        o.launch_mode > ST_LAUNCH_PERSISTENT || o.compaction_threshold < -1 || o.compaction_threshold > 32)
         return ST_ERR_INVALID_ARG;
     BatchPlan p;
     // one kernel per view has no tile shape, stack placement or chunk to choose; the persistent kernel
@@ -1319,55 +1377,73 @@ int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *
     int tile = o.launch_mode == ST_LAUNCH_PER_VIEW ? kPerViewVariant
                : (o.tile_shape >= 0 && o.stack_placement >= 0) ? o.tile_shape + TILE_SHAPES * o.stack_placement : -1;
     u32t chunk = o.launch_mode == ST_LAUNCH_PER_VIEW ? 1u : o.chunk > 0 ? (u32t)o.chunk : 0;
+    // the warp-vote compaction threshold applies to the persistent kernel only
+    int threshold = o.launch_mode == ST_LAUNCH_PER_VIEW ? 0 : o.compaction_threshold;
     ST_TRY(plan_batch(ctx, views, n, o.tile_shape >= 0 ? o.tile_shape : 0, o, p));
-    if (tile < 0 || chunk == 0) {
+    if (tile < 0 || chunk == 0 || threshold < 0) {
         auto it = B.tuned.find(p.class_key);
-        const bool per_view = it != B.tuned.end() && it->second.first == kPerViewVariant;
+        const bool per_view = it != B.tuned.end() && it->second.variant == kPerViewVariant;
         const bool fits = it != B.tuned.end() &&
-                          (per_view ? (o.launch_mode != ST_LAUNCH_PERSISTENT && !fixed_tile && !o.chunk)
+                          (per_view ? (o.launch_mode != ST_LAUNCH_PERSISTENT && !fixed_tile && !o.chunk &&
+                                       o.compaction_threshold < 0)
                                     : (o.launch_mode != ST_LAUNCH_PER_VIEW &&
-                                       (o.tile_shape < 0 || variant_tile(it->second.first) == o.tile_shape) &&
-                                       (o.stack_placement < 0 || variant_stack(it->second.first) == o.stack_placement)));
+                                       (o.tile_shape < 0 || variant_tile(it->second.variant) == o.tile_shape) &&
+                                       (o.stack_placement < 0 || variant_stack(it->second.variant) == o.stack_placement)));
         if (fits) {
-            if (tile < 0) tile = it->second.first;
-            if (!chunk) chunk = (u32t)it->second.second;
+            if (tile < 0) tile = it->second.variant;
+            if (!chunk) chunk = (u32t)it->second.chunk;
+            if (threshold < 0) threshold = tile == kPerViewVariant ? 0 : it->second.threshold;
         } else {
+            // the persistent kernel's variants and chunks without compaction, then compaction
+            // thresholds on the fastest of them, then one kernel per view
             const int shapes[4] = {TILE_8x4, TILE_16x2, TILE_4x8, TILE_32x1};
             const u32t chunks[2] = {1, 4};
+            const u32t thresholds[3] = {8, 16, 24};
+            const bool persistent = o.launch_mode != ST_LAUNCH_PER_VIEW;
             float best = INFINITY;
             int best_variant = TILE_8x4;
-            u32t best_chunk = 1;
-            for (int stack = 0; stack < STACK_PLACEMENTS; stack++) {
+            u32t best_chunk = 1, best_threshold = threshold > 0 ? (u32t)threshold : 0;
+            for (int stack = 0; persistent && stack < STACK_PLACEMENTS; stack++) {
                 if (o.stack_placement >= 0 && stack != o.stack_placement) continue;
                 for (int si = 0; si < 4; si++) {
                     if (o.tile_shape >= 0 && shapes[si] != o.tile_shape) continue;
                     const int variant = shapes[si] + TILE_SHAPES * stack;
+                    if (tile >= 0 && variant != tile) continue;
                     for (u32t c : chunks) {
                         if (chunk && c != chunk) continue;
                         float ms = 0;
-                        ST_TRY(time_batch(ctx, B, views, n, variant, c, st, o, ms));
+                        ST_TRY(time_batch(ctx, B, views, n, variant, c, best_threshold, st, o, ms));
                         if (ms < best) { best = ms; best_variant = variant; best_chunk = c; }
                     }
                 }
             }
-            if (o.launch_mode < 0 && !fixed_tile && !o.chunk) {   // one kernel per view
-                float ms = 0;
-                ST_TRY(time_batch(ctx, B, views, n, kPerViewVariant, 1, st, o, ms));
-                if (ms < best) { best = ms; best_variant = kPerViewVariant; best_chunk = 1; }
+            if (persistent && threshold < 0) {
+                for (u32t th : thresholds) {
+                    float ms = 0;
+                    ST_TRY(time_batch(ctx, B, views, n, best_variant, best_chunk, th, st, o, ms));
+                    if (ms < best) { best = ms; best_threshold = th; }
+                }
             }
-            if (o.tile_shape < 0 && o.stack_placement < 0 && !o.chunk && o.launch_mode < 0) {
-                B.tuned[p.class_key] = {best_variant, (int)best_chunk};
+            if (o.launch_mode < 0 && !fixed_tile && !o.chunk && o.compaction_threshold < 0) {   // one kernel per view
+                float ms = 0;
+                ST_TRY(time_batch(ctx, B, views, n, kPerViewVariant, 1, 0, st, o, ms));
+                if (ms < best) { best = ms; best_variant = kPerViewVariant; best_chunk = 1; best_threshold = 0; }
+            }
+            if (o.tile_shape < 0 && o.stack_placement < 0 && !o.chunk && o.launch_mode < 0 && o.compaction_threshold < 0) {
+                B.tuned[p.class_key] = Tuned{best_variant, (int)best_chunk, (int)best_threshold};
                 if (const char *path = getenv("ST_AUTOTUNE_CACHE")) {
                     std::ofstream f(path, std::ios::app);
-                    f << p.class_key << " " << best_variant << " " << best_chunk << "\n";
+                    f << p.class_key << " " << best_variant << " " << best_chunk << " " << best_threshold << "\n";
                 }
             }
             if (tile < 0) tile = best_variant;
             if (!chunk) chunk = best_chunk;
+            if (threshold < 0) threshold = (int)best_threshold;
         }
         ST_TRY(plan_batch(ctx, views, n, tile, o, p));
     }
-    ST_TRY(batch_reserve(ctx, B, p, n));
+    if (tile == kPerViewVariant) threshold = 0;
+    ST_TRY(batch_reserve(ctx, B, p, n, (u32t)threshold));
     o.graph_replayed = 0;
     ST_CUDA(cudaEventRecord(ctx->ev[0], st));
     if (o.use_graph) {
@@ -1375,7 +1451,7 @@ int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *
         // view groups and views wanting frames) is updated in place from the capture, so every kernel
         // parameter - view tables, cameras, arena and output pointers - is this call's.
         ST_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        int s = enqueue_batch(ctx, B, P<unsigned>(ctx->status), views, n, p, tile, chunk, st, o);
+        int s = enqueue_batch(ctx, B, P<unsigned>(ctx->status), views, n, p, tile, chunk, (u32t)threshold, st, o);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(st, &g);
         if (s != ST_OK) { if (g) cudaGraphDestroy(g); return s; }
@@ -1396,7 +1472,7 @@ int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *
         ST_CUDA(cudaGraphLaunch(B.exec, st));
         o.graph_replayed = updated ? 1 : 0;
     } else {
-        ST_TRY(enqueue_batch(ctx, B, P<unsigned>(ctx->status), views, n, p, tile, chunk, st, o));
+        ST_TRY(enqueue_batch(ctx, B, P<unsigned>(ctx->status), views, n, p, tile, chunk, (u32t)threshold, st, o));
     }
     ST_CUDA(cudaEventRecord(ctx->ev[1], st));
     if (!o.device_outputs) {
@@ -1413,14 +1489,18 @@ int st_render_batch(st_ctx *ctx, const st_view *views, int n, st_batch_options *
         }
     }
     unsigned status[4] = {0, 0, 0, 0};
+    u32t parked = 0;
     ST_CUDA(cudaMemcpyAsync(status, ctx->status.ptr, 16, cudaMemcpyDeviceToHost, st));
+    if (threshold) ST_CUDA(cudaMemcpyAsync(&parked, P<u32t>(B.counter) + 4, 4, cudaMemcpyDeviceToHost, st));
     ST_CUDA(cudaStreamSynchronize(st));
     cudaEventElapsedTime(&o.batch_ms, ctx->ev[0], ctx->ev[1]);
+    o.parked_rays = parked;
     o.rays = p.rays;
     o.launch_mode_used = tile == kPerViewVariant ? ST_LAUNCH_PER_VIEW : ST_LAUNCH_PERSISTENT;
     o.tile_shape_used = tile == kPerViewVariant ? -1 : variant_tile(tile);
     o.stack_placement_used = tile == kPerViewVariant ? -1 : variant_stack(tile);
     o.chunk_used = (int)chunk;
+    o.compaction_threshold_used = threshold;
     if (status[0] & S_STACK_OVERFLOW) return ST_ERR_STACK_OVERFLOW;
     return ST_OK;
 }
@@ -1741,7 +1821,7 @@ int enqueue_flight(st_ctx *ctx, InFlight &F, BatchPlan &p, std::vector<std::shar
         b.out_u8 = !r.out_u8 ? nullptr : r.mapped_u8 ? r.mapped_u8 : reinterpret_cast<uint32_t *>(arena + r.dev_u8);
     }
     ST_CUDA(cudaMemsetAsync(F.status.ptr, 0, 16, st));
-    ST_TRY(launch_groups(ctx, F.B, p, tile, chunk, P<unsigned>(F.status), st));
+    ST_TRY(launch_groups(ctx, F.B, p, tile, chunk, 0, P<unsigned>(F.status), st));
     for (int i = 0; i < n; i++) {
         const ServeReq &r = *reqs[i];
         const BatchView &b = p.table[i];
@@ -1797,9 +1877,9 @@ int launch_flight(st_ctx *ctx, int f, std::vector<std::shared_ptr<ServeReq>> &re
     }
     if (V.cfg.launch_mode == ST_LAUNCH_PERSISTENT && (V.cfg.tile_shape < 0 || V.cfg.chunk <= 0)) {
         auto it = ctx->batch.tuned.find(cls.str());
-        if (it != ctx->batch.tuned.end() && it->second.first != kPerViewVariant) {
-            if (V.cfg.tile_shape < 0) tile = it->second.first;
-            if (V.cfg.chunk <= 0) chunk = (u32t)it->second.second;
+        if (it != ctx->batch.tuned.end() && it->second.variant != kPerViewVariant) {
+            if (V.cfg.tile_shape < 0) tile = it->second.variant;
+            if (V.cfg.chunk <= 0) chunk = (u32t)it->second.chunk;
         }
     }
     tile_dims(tile, tw, th);

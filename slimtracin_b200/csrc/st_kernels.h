@@ -60,9 +60,39 @@ constexpr int kPerViewVariant = BATCH_VARIANTS;
 #endif
 constexpr int kAuxStreams = ST_AUX_STREAMS;
 
+// A grid point of a batch parked at a bounce: the persistent kernel's warp-vote compaction moves the
+// bounce rays of a warp that few lanes still trace into a queue, and drain_kernel traces them to the
+// end.  The record holds the whole path state carried across shadeSurface's bounce loop
+// (surface.h:180-239): the bounce ray, colour, throughput, the ray-cone footprints, the glow limit,
+// the bounces left and the primary hit's distance and depth.
+struct __align__(16) ParkedRay {
+    float4 origin_r;               // bounce ray origin xyz, colour r
+    float4 direction_g;            // bounce ray direction xyz, colour g
+    float4 throughput_b;           // throughput xyz, colour b
+    float4 carry;                  // du, dv, max_distance, closest_distance
+    uint4 where;                   // x, y, view in the launch group (kEmptySlot: nothing parked there),
+                                   // bounces << 2 | lights_shaded << 1 | hit_found
+    float4 depth;                  // z, unused x3
+};
+constexpr u32t kEmptySlot = 0xFFFFFFFFu;
+// The queue of one launch group: `threshold` is the warp-vote limit (a warp whose lanes still tracing
+// at a bounce number fewer than it parks them; 0: never), `reserved` counts slots handed out (parks
+// beyond `capacity` are refused and traced in place), `taken` the slots drained.
+struct ParkQueue {
+    ParkedRay *rays = nullptr;
+    u32t *reserved = nullptr, *taken = nullptr;
+    u32t *drained = nullptr;       // the batch's total of parked paths traced by the drain (all groups)
+    u32t capacity = 0, threshold = 0;
+};
+constexpr u32t kParkCapacity = 1u << 20;   // parked rays per launch group at most (96 MB)
+
 void launch_ssb(const SceneDev &S, const ViewDev &v, int4 *ssb, cudaStream_t st);
 int launch_batch(const BatchView *views, u32t n_views, u32t total_tiles, int variant, u32t chunk, u32t grid_blocks,
-                 u32t *tile_counter, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st);
+                 u32t *tile_counter, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st,
+                 const ParkQueue &park);
+// The parked rays of a launch group, traced to the end (a persistent grid of grid_blocks blocks).
+int launch_drain(const BatchView *views, const ParkQueue &park, int variant, u32t grid_blocks, unsigned *status,
+                 unsigned long long *counters, bool count, cudaStream_t st);
 void tile_dims(int variant, u32t &tw, u32t &th);
 int batch_blocks_per_sm(int variant);
 // Row-segment starts of the view's ray directions: (grid_h x ceil(grid_w / kSegment)) float3.
@@ -85,7 +115,11 @@ void launch_resolve(const FloatPixel *in, u32t grid_w, u32t width, u32t height, 
 void launch_batch_setup(const BatchTable &T, u32t n_views, u32t max_prims, u32t max_rows, cudaStream_t st);
 void launch_batch_resolve(const BatchTable &T, u32t n_views, u32t max_width, u32t max_height, cudaStream_t st);
 
-// ---- BVH builds (st_bvh.cu) ----
+// ---- BVH builds (st_bvh.cu, st_sah.cu, st_refsah.cu) ----
+// The reference's full-sweep SAH (buildBVH) over n device boxes: nodes and leaf ids as the reference
+// lays them out, info = {node_count, height}; synchronous on st.
+cudaError_t refsah_build(const float *boxes, u32t n, u32t max_leaf, BVHNode *nodes, u32t *leaf_ids, u32t info[2],
+                         cudaStream_t st);
 // Device scratch the LBVH build needs for n items (allocated once per context and grown).
 struct LbvhScratch {
     u32t capacity = 0;

@@ -7,31 +7,24 @@
 namespace st {
 
 // ---- triangles and the BLAS walk: intersection/mesh.h ----------------------------------------
+// hitTriangles (mesh.h:5) over the leaf's triangles: an accepted triangle (in front of the closest
+// so far, inside by its tangent-space UV) becomes the closest; only its distance and slot are kept
+// (finalize_hit rebuilds the rest of the record from them).
 template <bool CNT, int SHS>
-__device__ bool hit_triangles(TState<CNT, SHS> &t, const SceneDev &S, u32t base, u32t n, bool any_hit) {   // mesh.h:5
+__device__ bool hit_triangles(TState<CNT, SHS> &t, const SceneDev &S, u32t base, u32t slot0, u32t n, bool any_hit) {
     const RayD &ray = t.local;
-    Hit &hit = t.current;
-    Hit &closest = t.mesh_closest;
     bool found = false;
     for (u32t i = 0; i < n; i++) {
         const TriHot T = S.tri_hot[base + i];
         t.count(C_TRI);
         v3 pos = V(T.p.x, T.p.y, T.p.z), nrm = V(T.p.w, T.q.x, T.q.y);
-        if (hit_plane(pos, nrm, ray.origin, ray.direction, hit) && hit.distance < closest.distance) {
+        Hit hit;
+        if (hit_plane(pos, nrm, ray.origin, ray.direction, hit) && hit.distance < t.mesh_distance) {
             const float m[9] = {T.q.z, T.q.w, T.r.x, T.r.y, T.r.z, T.r.w, T.s.x, T.s.y, T.s.z};
             v3 UV = vmat3(hit.position - pos, m);
             if (UV.x < 0 || UV.y < 0 || (UV.x + UV.y) > 1) continue;
-            closest.NdotV = hit.NdotV;
-            closest.normal = hit.normal;
-            closest.u = UV.x;
-            closest.v = UV.y;
-            closest.object_id = i;
-            closest.from_behind = hit.from_behind;
-            closest.distance = hit.distance;
-            closest.position = hit.position;
-            const float2 areas = __ldg(reinterpret_cast<const float2 *>(&S.tri_full[base + i].area_of_parallelogram));
-            closest.area = areas.x;
-            closest.uv_area = areas.y;
+            t.mesh_distance = hit.distance;
+            t.mesh_tri = slot0 + i;
             found = true;
             if (any_hit) break;
         }
@@ -52,19 +45,19 @@ __device__ __forceinline__ NodePair load_pair(const NodePair *p) {
 template <bool CNT, int SHS>
 __device__ __forceinline__ bool trace_mesh(TState<CNT, SHS> &t, const SceneDev &S, const MeshDev &M, bool any_hit) {   // mesh.h:38
     const RayD &ray = t.local;
-    Hit &closest = t.mesh_closest;
     float ld, rd;
     t.count(C_MESH);
     t.count(C_AABB);
-    if (!hit_aabb(V(M.aabb[0], M.aabb[1], M.aabb[2]), V(M.aabb[3], M.aabb[4], M.aabb[5]), ray, closest.distance, ld))
+    if (!hit_aabb(V(M.aabb[0], M.aabb[1], M.aabb[2]), V(M.aabb[3], M.aabb[4], M.aabb[5]), ray, t.mesh_distance, ld))
         return false;
     // Leaves met at a node are tested (left, then right) before the walk moves on, as in the
     // reference; they are queued so that the triangle loop has a single call site.
-    u32t leaf_first[2], leaf_count[2];
+    // the queue is two named slots, not an indexed array, so that it stays in registers
+    u32t q0_first = 0, q0_count = 0, q1_first = 0, q1_count = 0;
     int leaves = 0;
     const NodePair *pairs = S.mesh_pairs + M.pair_offset;
     u32t pair = kNoPair;
-    if (M.root_count) { leaf_first[0] = 0; leaf_count[0] = M.triangle_count; leaves = 1; }
+    if (M.root_count) { q0_first = 0; q0_count = M.triangle_count; leaves = 1; }
     else pair = (M.root_first - 1) >> 1;
     u32t sp = 0;
     bool found = false;
@@ -74,11 +67,16 @@ __device__ __forceinline__ bool trace_mesh(TState<CNT, SHS> &t, const SceneDev &
         while (leaves == 0 && pair != kNoPair) {
             const NodePair P = load_pair(pairs + pair);
             t.count(C_AABB, 2);
-            bool hl = hit_aabb(V(P.a.x, P.a.y, P.a.z), V(P.a.w, P.b.x, P.b.y), ray, closest.distance, ld);
-            bool hr = hit_aabb(V(P.b.z, P.b.w, P.c.x), V(P.c.y, P.c.z, P.c.w), ray, closest.distance, rd);
+            bool hl = hit_aabb(V(P.a.x, P.a.y, P.a.z), V(P.a.w, P.b.x, P.b.y), ray, t.mesh_distance, ld);
+            bool hr = hit_aabb(V(P.b.z, P.b.w, P.c.x), V(P.c.y, P.c.z, P.c.w), ray, t.mesh_distance, rd);
             bool lgo = hl, rgo = hr;
-            if (hl && P.d.y) { leaf_first[leaves] = P.d.x; leaf_count[leaves] = P.d.y; leaves++; lgo = false; }
-            if (hr && P.d.w) { leaf_first[leaves] = P.d.z; leaf_count[leaves] = P.d.w; leaves++; rgo = false; }
+            if (hl && P.d.y) { q0_first = P.d.x; q0_count = P.d.y; leaves = 1; lgo = false; }
+            if (hr && P.d.w) {
+                if (leaves) { q1_first = P.d.z; q1_count = P.d.w; }
+                else { q0_first = P.d.z; q0_count = P.d.w; }
+                leaves++;
+                rgo = false;
+            }
             if (lgo) {
                 u32t near_pair = P.d.x, far_pair = P.d.z;
                 if (rgo) {
@@ -99,13 +97,15 @@ __device__ __forceinline__ bool trace_mesh(TState<CNT, SHS> &t, const SceneDev &
         }
         if (!leaves) break;
 #pragma unroll 1
-        for (int k = 0; k < leaves; k++)
-            if (hit_triangles(t, S, M.tri_offset + leaf_first[k], leaf_count[k], any_hit)) {
-                closest.object_id += leaf_first[k];
+        for (;;) {                       // the queued leaves in order: q0, then q1
+            if (hit_triangles(t, S, M.tri_offset + q0_first, q0_first, q0_count, any_hit)) {
                 found = true;
                 if (any_hit) return true;
             }
-        leaves = 0;
+            if (--leaves == 0) break;
+            q0_first = q1_first;
+            q0_count = q1_count;
+        }
         if (pair == kNoPair) break;
     }
     return found;
@@ -113,12 +113,15 @@ __device__ __forceinline__ bool trace_mesh(TState<CNT, SHS> &t, const SceneDev &
 
 // ---- hitPrimitives intersection/primitives.h:9 ----------------------------------------------------
 // ids == nullptr: the candidates are primitives first..first+count-1 in index order.
+// The candidate loop keeps the reference's order and comparisons; a winner updates t.best (the
+// hit test's distance, the world position and its squared distance, which the next candidates and
+// the walk read), and a call that found one ends with the world distance, as hitPrimitives' final
+// step leaves it (primitives.h:105).  The rest of that final step is finalize_hit's.
 template <bool CNT, int SHS>
 __device__ __forceinline__ bool hit_primitives(TState<CNT, SHS> &t, const SceneDev &S, const RayD &ray, const u32t *ids, u32t first,
-                               u32t count, bool any_hit, const int4 *ssb, int x, int y, float cone_angle) {
-    Hit &hit = t.current, &closest = t.closest;
+                               u32t count, bool any_hit, const int4 *ssb, int x, int y) {
+    Best &best = t.best;
     bool found = false;
-    u32t hid = 0;
     for (u32t i = 0; i < count; i++) {
         t.count(C_LEAF);
         const u32t pid = ids ? __ldg(ids + first + i) : first + i;
@@ -133,64 +136,118 @@ __device__ __forceinline__ bool hit_primitives(TState<CNT, SHS> &t, const SceneD
         to_object(ray.origin, ray.direction, P, t.local.origin, t.local.direction);
         t.local.origin = vsfma(t.local.direction, kTraceOffset, t.local.origin);
         bool cur;
-        switch (prim_type(P)) {
-            case PrimitiveType_Quad: cur = hit_quad(hit, t.local.origin, t.local.direction, flags); break;
-            case PrimitiveType_Box: cur = hit_box(hit, t.local.origin, t.local.direction, flags); break;
-            case PrimitiveType_Sphere: cur = hit_sphere(hit, t.local.origin, t.local.direction, flags); break;
-            case PrimitiveType_Tetrahedron: cur = hit_tetra(hit, t.local.origin, t.local.direction, flags); break;
-            case PrimitiveType_Mesh: {
-                t.local.rcp = rcp(t.local.direction);
-                t.mesh_closest.distance = closest.distance == INFINITY ? INFINITY :
-                    len(pos_to_object(closest.position, P) - t.local.origin);
-                pre_prep(t.local);
-                const MeshDev M = S.meshes[__float_as_uint(P.scale_id.w)];
-                cur = trace_mesh(t, S, M, any_hit);
-                if (cur) hit = t.mesh_closest;
-            } break;
-            default: continue;
+        float dist = 0.0f;
+        v3 pos = splat(0.0f);
+        u32t tri = 0;
+        const unsigned type = prim_type(P);
+        if (type == PrimitiveType_Mesh) {
+            t.local.rcp = rcp(t.local.direction);
+            t.mesh_distance = best.distance == INFINITY ? INFINITY :
+                len(pos_to_object(best.position, P) - t.local.origin);
+            pre_prep(t.local);
+            const u32t mesh = __float_as_uint(P.scale_id.w);
+            cur = trace_mesh(t, S, S.meshes[mesh], any_hit);
+            if (cur) {
+                // the accepted triangle's object-space hit point, recomputed exactly as
+                // hit_triangles computed it (same triangle, same ray, same operations)
+                const MeshDev &M = S.meshes[mesh];
+                tri = t.mesh_tri;
+                const float4 tp = __ldg(reinterpret_cast<const float4 *>(S.tri_hot + M.tri_offset + tri));
+                const float4 tq = __ldg(reinterpret_cast<const float4 *>(S.tri_hot + M.tri_offset + tri) + 1);
+                Hit h;
+                hit_plane(V(tp.x, tp.y, tp.z), V(tp.w, tq.x, tq.y), t.local.origin, t.local.direction, h);
+                pos = h.position;
+                dist = t.mesh_distance;
+            }
+        } else {
+            Hit hit;
+            switch (type) {
+                case PrimitiveType_Quad: cur = hit_quad(hit, t.local.origin, t.local.direction, flags); break;
+                case PrimitiveType_Box: cur = hit_box(hit, t.local.origin, t.local.direction, flags); break;
+                case PrimitiveType_Sphere: cur = hit_sphere(hit, t.local.origin, t.local.direction, flags); break;
+                case PrimitiveType_Tetrahedron: cur = hit_tetra(hit, t.local.origin, t.local.direction, flags); break;
+                default: continue;
+            }
+            pos = hit.position;
+            dist = hit.distance;
         }
         if (cur) {
-            hit.position = pos_to_world(hit.position, P);
-            hit.distance_squared = sqlen(hit.position - ray.origin);
-            if (hit.distance_squared < closest.distance_squared) {
-                closest = hit;
-                hid = pid;
-                closest.object_type = prim_type(P);
-                closest.material_id = prim_material(P);
+            pos = pos_to_world(pos, P);
+            const float dsq = sqlen(pos - ray.origin);
+            if (dsq < best.distance_squared) {
+                best.distance_squared = dsq;
+                best.distance = dist;
+                best.position = pos;
+                best.prim = pid;
+                best.tri = tri;
                 found = true;
                 if (any_hit) break;
             }
         }
     }
-    if (found) {
-        const PrimDev HP = S.prims[hid];
-        if (closest.object_type == PrimitiveType_Mesh) {
-            const MeshDev M = S.meshes[__float_as_uint(HP.scale_id.w)];
+    if (found) best.distance = sqrtf(best.distance_squared);
+    return found;
+}
+
+// The closest hit's full record (hitPrimitives' copy of the winner's RayHit and its final step,
+// primitives.h:63-108), rebuilt after a walk that found t.best: the winner's hit test runs again on
+// the same object-space ray (to_object and the offset as in the candidate loop), which gives the
+// record the candidate loop saw bit for bit; then the barycentric interpolation of mesh normals and
+// uvs, the primitive id, the world normal, distance, cone width and area.
+template <bool CNT, int SHS>
+__device__ __forceinline__ void finalize_hit(TState<CNT, SHS> &t, const SceneDev &S, const RayD &ray, float cone_angle) {
+    Hit &closest = t.closest;
+    const u32t hid = t.best.prim;
+    const PrimDev HP = S.prims[hid];
+    const unsigned flags = prim_flags(HP), type = prim_type(HP);
+    v3 lo, ld;
+    to_object(ray.origin, ray.direction, HP, lo, ld);
+    lo = vsfma(ld, kTraceOffset, lo);
+    switch (type) {
+        case PrimitiveType_Quad: hit_quad(closest, lo, ld, flags); break;
+        case PrimitiveType_Box: hit_box(closest, lo, ld, flags); break;
+        case PrimitiveType_Sphere: hit_sphere(closest, lo, ld, flags); break;
+        case PrimitiveType_Tetrahedron: hit_tetra(closest, lo, ld, flags); break;
+        default: {                                              // PrimitiveType_Mesh
+            const MeshDev &M = S.meshes[__float_as_uint(HP.scale_id.w)];
+            const u32t tri = t.best.tri;
+            const TriHot T = S.tri_hot[M.tri_offset + tri];
+            const v3 pos = V(T.p.x, T.p.y, T.p.z);
+            hit_plane(pos, V(T.p.w, T.q.x, T.q.y), lo, ld, closest);
+            const float m[9] = {T.q.z, T.q.w, T.r.x, T.r.y, T.r.z, T.r.w, T.s.x, T.s.y, T.s.z};
+            const v3 UV = vmat3(closest.position - pos, m);
+            closest.u = UV.x;
+            closest.v = UV.y;
+            const Triangle &TF = S.tri_full[M.tri_offset + tri];
+            closest.area = TF.area_of_parallelogram;
+            closest.uv_area = TF.area_of_uv;
             if (M.normals_count | M.uvs_count) {
-                const Triangle &T = S.tri_full[M.tri_offset + closest.object_id];
                 float u = closest.u, v = closest.v;
                 float w = 1 - u - v;
                 if (M.uvs_count) {
-                    closest.u = T.uvs[2].x * u + (T.uvs[1].x * v + T.uvs[0].x * w);
-                    closest.v = T.uvs[2].y * u + (T.uvs[1].y * v + T.uvs[0].y * w);
+                    closest.u = TF.uvs[2].x * u + (TF.uvs[1].x * v + TF.uvs[0].x * w);
+                    closest.v = TF.uvs[2].y * u + (TF.uvs[1].y * v + TF.uvs[0].y * w);
                 }
                 if (M.normals_count) {
-                    const vec3 *vn = T.vertex_normals;
+                    const vec3 *vn = TF.vertex_normals;
                     closest.normal.x = vn[2].x * u + (vn[1].x * v + vn[0].x * w);
                     closest.normal.y = vn[2].y * u + (vn[1].y * v + vn[0].y * w);
                     closest.normal.z = vn[2].z * u + (vn[1].z * v + vn[0].z * w);
                     closest.normal = norm(closest.normal);
                 }
             }
-        }
-        closest.object_id = hid;
-        closest.normal = norm(dir_to_world(closest.normal, HP));
-        closest.distance = sqrtf(closest.distance_squared);
-        closest.cone_width = 2.0f * cone_angle * closest.distance;
-        v3 rs = qrot(V(HP.scale_id.x, HP.scale_id.y, HP.scale_id.z), prim_rot(HP));
-        closest.area *= dot(one_minus(closest.normal), rs);
+        } break;
     }
-    return found;
+    closest.position = t.best.position;
+    closest.distance_squared = t.best.distance_squared;
+    closest.object_type = type;
+    closest.material_id = prim_material(HP);
+    closest.object_id = hid;
+    closest.normal = norm(dir_to_world(closest.normal, HP));
+    closest.distance = t.best.distance;
+    closest.cone_width = 2.0f * cone_angle * closest.distance;
+    v3 rs = qrot(V(HP.scale_id.x, HP.scale_id.y, HP.scale_id.z), prim_rot(HP));
+    closest.area *= dot(one_minus(closest.normal), rs);
 }
 
 // ---- traceScene shaders/trace.h:8 (TLAS walk); with ssb != null it also serves primary rays ----
@@ -200,22 +257,22 @@ __device__ __forceinline__ bool hit_primitives(TState<CNT, SHS> &t, const SceneD
 // scenes with few primitives, raytracer.h:100).
 template <bool CNT, int SHS>
 __device__ __forceinline__ bool trace_scene(TState<CNT, SHS> &t, const SceneDev &S, RayD &ray, bool any_hit, const int4 *ssb,
-                                            int x, int y, float cone_angle, bool prepped, bool all_prims) {
+                                            int x, int y, bool prepped, bool all_prims) {
     if (!prepped) {
         ray.rcp = rcp(ray.direction);
         pre_prep(ray);
     }
     float ld, rd;
-    u32t leaf_first[2], leaf_count[2];
+    u32t q0_first = 0, q0_count = 0, q1_first = 0, q1_count = 0;   // the leaf queue, as in trace_mesh
     int leaves = 0;
     u32t pair = kNoPair;
     if (!all_prims) {
         t.count(C_AABB);
         if (!hit_aabb(V(S.tlas_root_aabb[0], S.tlas_root_aabb[1], S.tlas_root_aabb[2]),
-                      V(S.tlas_root_aabb[3], S.tlas_root_aabb[4], S.tlas_root_aabb[5]), ray, t.closest.distance, ld))
+                      V(S.tlas_root_aabb[3], S.tlas_root_aabb[4], S.tlas_root_aabb[5]), ray, t.best.distance, ld))
             return false;
     }
-    if (all_prims || S.tlas_root_count) { leaf_first[0] = 0; leaf_count[0] = S.n_prims; leaves = 1; }
+    if (all_prims || S.tlas_root_count) { q0_first = 0; q0_count = S.n_prims; leaves = 1; }
     else pair = (S.tlas_root_first - 1) >> 1;
     u32t sp = 0;
     bool found = false;
@@ -223,11 +280,16 @@ __device__ __forceinline__ bool trace_scene(TState<CNT, SHS> &t, const SceneDev 
         while (leaves == 0 && pair != kNoPair) {      // inner nodes until leaves are queued
             const NodePair P = load_pair(S.tlas_pairs + pair);
             t.count(C_AABB, 2);
-            bool hl = hit_aabb(V(P.a.x, P.a.y, P.a.z), V(P.a.w, P.b.x, P.b.y), ray, t.closest.distance, ld);
-            bool hr = hit_aabb(V(P.b.z, P.b.w, P.c.x), V(P.c.y, P.c.z, P.c.w), ray, t.closest.distance, rd);
+            bool hl = hit_aabb(V(P.a.x, P.a.y, P.a.z), V(P.a.w, P.b.x, P.b.y), ray, t.best.distance, ld);
+            bool hr = hit_aabb(V(P.b.z, P.b.w, P.c.x), V(P.c.y, P.c.z, P.c.w), ray, t.best.distance, rd);
             bool lgo = hl, rgo = hr;
-            if (hl && P.d.y) { leaf_first[leaves] = P.d.x; leaf_count[leaves] = P.d.y; leaves++; lgo = false; }
-            if (hr && P.d.w) { leaf_first[leaves] = P.d.z; leaf_count[leaves] = P.d.w; leaves++; rgo = false; }
+            if (hl && P.d.y) { q0_first = P.d.x; q0_count = P.d.y; leaves = 1; lgo = false; }
+            if (hr && P.d.w) {
+                if (leaves) { q1_first = P.d.z; q1_count = P.d.w; }
+                else { q0_first = P.d.z; q0_count = P.d.w; }
+                leaves++;
+                rgo = false;
+            }
             if (lgo) {
                 u32t near_pair = P.d.x, far_pair = P.d.z;
                 if (rgo) {
@@ -248,12 +310,15 @@ __device__ __forceinline__ bool trace_scene(TState<CNT, SHS> &t, const SceneDev 
         }
         if (!leaves) break;
 #pragma unroll 1
-        for (int k = 0; k < leaves; k++)
-            if (hit_primitives(t, S, ray, S.tlas_leaf_ids, leaf_first[k], leaf_count[k], any_hit, ssb, x, y, cone_angle)) {
+        for (;;) {
+            if (hit_primitives(t, S, ray, S.tlas_leaf_ids, q0_first, q0_count, any_hit, ssb, x, y)) {
                 found = true;
                 if (any_hit) return true;
             }
-        leaves = 0;
+            if (--leaves == 0) break;
+            q0_first = q1_first;
+            q0_count = q1_count;
+        }
         if (pair == kNoPair) break;
     }
     return found;
@@ -262,29 +327,38 @@ __device__ __forceinline__ bool trace_scene(TState<CNT, SHS> &t, const SceneDev 
 // ---- closest_hit/surface.h, lights.h ------------------------------------------------------------
 template <bool CNT, int SHS>
 __device__ v3 shade_from_lights(TState<CNT, SHS> &t, const SceneDev &S, Shaded &s, RayD &ray, v3 color) {   // surface.h:9
-    Hit &hit = t.closest;
+    // The reference writes each light into trace->closest_hit (:14-17) and the shadow ray's walk
+    // reads it there (the occluder must be nearer than the light) or overwrites it with an
+    // occluder: the walk's record t.best plays that part, and closest_hit's position and distances
+    // are left as the last light's walk left them, because the emissive-quad test reads them (:55).
+    Best &b = t.best;
     for (u32t i = 0; i < S.n_lights; i++) {
         const Light &light = S.lights[i];
-        hit.position = from(light.position_or_direction);
-        s.light_direction = hit.position - s.position;
-        hit.distance_squared = sqlen(s.light_direction);
-        hit.distance = sqrtf(hit.distance_squared);
-        s.light_direction = vscale(s.light_direction, 1.0f / hit.distance);
+        b.position = from(light.position_or_direction);
+        s.light_direction = b.position - s.position;
+        b.distance_squared = sqlen(s.light_direction);
+        b.distance = sqrtf(b.distance_squared);
+        s.light_direction = vscale(s.light_direction, 1.0f / b.distance);
         float NdotL = dot(s.normal, s.light_direction);
         if (NdotL <= 0) continue;
-        float li = light.intensity / hit.distance_squared;
+        float li = light.intensity / b.distance_squared;
         ray.origin = s.position;
         ray.direction = s.light_direction;
         t.count(C_SHADOW);
-        if (trace_scene(t, S, ray, true, nullptr, 0, 0, 0.0f, false, false)) continue;       // inShadow trace.h:85
+        if (trace_scene(t, S, ray, true, nullptr, 0, 0, false, false)) continue;       // inShadow trace.h:85
         color = vvfma(shade_point(s, NdotL), vscale(from(light.color), li), color);
+    }
+    if (S.n_lights) {
+        t.closest.position = b.position;
+        t.closest.distance_squared = b.distance_squared;
+        t.closest.distance = b.distance;
     }
     return color;
 }
 
 template <bool CNT, int SHS>
 __device__ bool shade_from_emissive_quads(TState<CNT, SHS> &t, const SceneDev &S, Shaded &s, RayD &ray, v3 &color) {  // surface.h:37
-    Hit &hit = t.current;
+    Hit hit;                                    // the reference's trace->current_hit, scratch here
     bool found = false;
     for (u32t e = 0; e < S.n_emissive; e++) {
         const u32t qi = S.emissive_quads[e];
@@ -517,25 +591,23 @@ __device__ __forceinline__ v3 grid_direction(const ViewDev &v, const float *seg,
 // (black, 0, +inf).
 // ret_c / ret_d (optional): the point's FloatPixel (colour and opacity, depth) is returned there
 // instead of being written to out / out_host.
+// park (optional): at each bounce, a warp whose lanes still tracing number fewer than
+// park->threshold parks those lanes' paths in the queue (returns false: the point is not finished,
+// nothing is written); resume (optional): a parked path, continued from its bounce ray.  A path
+// runs the same steps whether it is parked or not, so the outputs and counters do not change.
 template <bool CNT, int SHS>
-__device__ __forceinline__ void trace_point(TState<CNT, SHS> &t, const SceneDev &S, const ViewDev &v, const int4 *ssb,
+__device__ __forceinline__ bool trace_point(TState<CNT, SHS> &t, const SceneDev &S, const ViewDev &v, const int4 *ssb,
                                             const float *dirs, u32t x, u32t y, FloatPixel *out, u32t *prim_ids,
                                             FloatPixel *out_host = nullptr, float4 *ret_c = nullptr,
-                                            double *ret_d = nullptr) {
+                                            double *ret_d = nullptr, const ParkQueue *park = nullptr,
+                                            u32t view_index = 0, const ParkedRay *resume = nullptr) {
     const size_t idx = (size_t)y * v.grid_w + x;
-    v3 current = grid_direction(v, dirs, x, y);
+    const v3 Ro = v.cam_pos, Rd = norm(grid_direction(v, dirs, x, y));
     RayD ray;
-    ray.origin = v.cam_pos;
-    ray.direction = norm(current);
-    ray.rcp = rcp(ray.direction);
-    pre_prep(ray);      // only the walk reads the prepared fields; every bounce ray prepares its own
     t.depth = v.depth;
     t.closest.distance = t.closest.distance_squared = INFINITY;
     t.closest.cone_width = 0;
-    t.mesh_closest.object_type = PrimitiveType_Mesh;
-    t.current.cone_width = 0;
-    t.count(C_PRIMARY);
-    const v3 Ro = ray.origin, Rd = ray.direction;
+    t.best.distance = t.best.distance_squared = INFINITY;
     v3 color = splat(0);
     bool lights_shaded = false, hit_found = false;
     float closest_distance = INFINITY, z = INFINITY;
@@ -547,11 +619,34 @@ __device__ __forceinline__ void trace_point(TState<CNT, SHS> &t, const SceneDev 
     v3 throughput = splat(1);
     u32t bounces = 0;                                       // shadeSurface's `depth`
     bool primary = true;
+    if (resume) {                                           // a parked path, at its bounce ray
+        const ParkedRay &P = *resume;
+        ray.origin = V(P.origin_r.x, P.origin_r.y, P.origin_r.z);
+        ray.direction = V(P.direction_g.x, P.direction_g.y, P.direction_g.z);
+        color = V(P.origin_r.w, P.direction_g.w, P.throughput_b.w);
+        throughput = V(P.throughput_b.x, P.throughput_b.y, P.throughput_b.z);
+        du = P.carry.x;
+        dv = P.carry.y;
+        max_distance = P.carry.z;
+        closest_distance = P.carry.w;
+        z = P.depth.x;
+        bounces = P.where.w >> 2;
+        lights_shaded = (P.where.w >> 1) & 1u;
+        hit_found = P.where.w & 1u;
+        primary = false;
+    } else {
+        ray.origin = Ro;
+        ray.direction = Rd;
+        ray.rcp = rcp(ray.direction);
+        pre_prep(ray);      // only the walk reads the prepared fields; every bounce ray prepares its own
+        t.count(C_PRIMARY);
+    }
     // The primary ray and every bounce ray of shadeSurface's loop share this one trace site, so the
     // kernel carries one inlined copy of the walk for both (shadow rays keep theirs).
     for (;;) {
-        const bool found = trace_scene(t, S, ray, false, primary ? ssb : nullptr, (int)x, (int)y,
-                                       primary ? v.cone_angle : 0.0f, primary, primary && !v.primary_tlas);
+        const bool found = trace_scene(t, S, ray, false, primary ? ssb : nullptr, (int)x, (int)y, primary,
+                                       primary && !v.primary_tlas);
+        if (found) finalize_hit(t, S, ray, primary ? v.cone_angle : 0.0f);
         if (primary) {                                      // rayTrace after the hit test (raytracer.h:89)
             primary = false;
             hit_found = found;
@@ -641,6 +736,32 @@ __device__ __forceinline__ void trace_point(TState<CNT, SHS> &t, const SceneDev 
         }
         t.count(C_BOUNCE);
         t.closest.distance = t.closest.distance_squared = INFINITY;           // traceRay trace.h:89
+        t.best.distance = t.best.distance_squared = INFINITY;
+        if (park && park->threshold) {
+            // warp-vote compaction: the lanes at this bounce are the warp's lanes still tracing
+            const unsigned mask = __activemask();
+            const u32t n = __popc(mask);
+            if (n < park->threshold) {
+                const u32t lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+                u32t base = 0;
+                if (lane == leader) base = atomicAdd(park->reserved, n);
+                base = __shfl_sync(mask, base, leader);
+                const u32t slot = base + __popc(mask & ((1u << lane) - 1u));
+                if (base + n <= park->capacity) {
+                    ParkedRay &P = park->rays[slot];
+                    P.origin_r = make_float4(ray.origin.x, ray.origin.y, ray.origin.z, color.x);
+                    P.direction_g = make_float4(ray.direction.x, ray.direction.y, ray.direction.z, color.y);
+                    P.throughput_b = make_float4(throughput.x, throughput.y, throughput.z, color.z);
+                    P.carry = make_float4(du, dv, max_distance, closest_distance);
+                    P.where = make_uint4(x, y, view_index, (bounces << 2) | ((u32t)lights_shaded << 1) | (u32t)hit_found);
+                    P.depth = make_float4(z, 0.0f, 0.0f, 0.0f);
+                    return false;
+                }
+                // the queue is full: these paths go on here; slots of the refused range that lie
+                // inside the queue are marked empty for the drain
+                if (slot < park->capacity) park->rays[slot].where = make_uint4(0, 0, kEmptySlot, 0);
+            }
+        }
     }
     if (v.mode == RenderMode_Beauty && S.lights && !lights_shaded) {
         if (shade_lights(t, S, Ro, Rd, closest_distance, color)) {
@@ -667,7 +788,7 @@ __device__ __forceinline__ void trace_point(TState<CNT, SHS> &t, const SceneDev 
     if (ret_c) {
         *ret_c = c01;
         *ret_d = depth;
-        return;
+        return true;
     }
     float2 *o = reinterpret_cast<float2 *>(out + idx);
     o[0] = make_float2(c01.x, c01.y);
@@ -679,6 +800,7 @@ __device__ __forceinline__ void trace_point(TState<CNT, SHS> &t, const SceneDev 
         h[1] = make_float2(c01.z, c01.w);
         reinterpret_cast<double *>(h)[2] = depth;
     }
+    return true;
 }
 
 template <bool CNT, int SHS>
@@ -765,14 +887,14 @@ __global__ void pick_kernel(SceneDev S, ViewDev v, const int4 *ssb, int x, int y
     t.status = 0;
     t.closest.distance = t.closest.distance_squared = INFINITY;       // MAX_DISTANCE base.h:164
     t.closest.cone_width = 0;
-    t.mesh_closest.object_type = PrimitiveType_Mesh;
-    t.current.cone_width = 0;
+    t.best.distance = t.best.distance_squared = INFINITY;
     RayD ray;
     ray.origin = v.cam_pos;
     ray.direction = norm(vsfma(v.pp_down, (float)y, vsfma(v.pp_right, (float)x, v.pp_start)));
     ray.rcp = rcp(ray.direction);
     bool found = hit_primitives(t, S, ray, S.tlas_leaf_ids, 0, S.n_prims, false, ssb, (int)(uint16_t)x,
-                                (int)(uint16_t)y, 0.0f);
+                                (int)(uint16_t)y);
+    if (found) finalize_hit(t, S, ray, 0.0f);
     Hit &hit = t.closest;
     for (u32t i = 0; S.lights && i < S.n_lights; i++) {
         const Light &L = S.lights[i];
@@ -804,7 +926,8 @@ __global__ void pick_kernel(SceneDev S, ViewDev v, const int4 *ssb, int x, int y
 // different sizes, scenes and bounce counts share the launch and no warp idles while work is left.
 template <bool CNT, int TW, int TH, int SHS>
 __global__ void ST_TRACE_BOUNDS batch_kernel(const BatchView *views, u32t n_views, u32t total_tiles, u32t chunk,
-                                                    u32t *tile_counter, unsigned *status, unsigned long long *counters) {
+                                                    u32t *tile_counter, unsigned *status, unsigned long long *counters,
+                                                    ParkQueue park) {
     static_assert(TW * TH == 32, "one warp per tile");
     const u32t lane = threadIdx.x & 31;
     __shared__ u32t stack_columns[SHS > 0 ? 2 * SHS * kTraceBlock : 1];
@@ -828,9 +951,44 @@ __global__ void ST_TRACE_BOUNDS batch_kernel(const BatchView *views, u32t n_view
             const u32t tx = 2 * (group % B.tiles_x) + (q & 1), ty = 2 * (group / B.tiles_x) + (q >> 1);
             const u32t x = tx * TW + (lane % TW), y = ty * TH + (lane / TW);
             if (x < B.view.grid_w && y < B.view.grid_h)
-                trace_point(t, B.scene, B.view, B.ssb, B.dirs, x, y, B.out, B.prim_ids);
+                trace_point(t, B.scene, B.view, B.ssb, B.dirs, x, y, B.out, B.prim_ids, nullptr, nullptr, nullptr,
+                            &park, vi);
         }
     }
+    flush_counters(t, status, counters);
+}
+
+// The paths batch_kernel parked, continued from their bounce rays to the end and written to their
+// views' outputs: a persistent grid whose warps take 32 queue slots at a time.
+template <bool CNT, int SHS>
+__global__ void ST_TRACE_BOUNDS drain_kernel(const BatchView *views, ParkQueue park, unsigned *status,
+                                                    unsigned long long *counters) {
+    const u32t lane = threadIdx.x & 31;
+    __shared__ u32t stack_columns[SHS > 0 ? 2 * SHS * kTraceBlock : 1];
+    TState<CNT, SHS> t;
+    t.sh = stack_columns + threadIdx.x;
+    t.status = 0;
+    if (CNT) for (int k = 0; k < C_COUNT; k++) t.cnt[k] = 0;
+    const u32t n = min(*park.reserved, park.capacity);
+    u32t drained = 0;
+    for (;;) {
+        u32t first = 0;
+        if (lane == 0) first = atomicAdd(park.taken, 32u);
+        first = __shfl_sync(0xFFFFFFFFu, first, 0);
+        if (first >= n) break;
+        const u32t i = first + lane;
+        if (i < n) {
+            const ParkedRay P = park.rays[i];
+            if (P.where.z != kEmptySlot) {
+                const BatchView &B = views[P.where.z];
+                trace_point(t, B.scene, B.view, B.ssb, B.dirs, P.where.x, P.where.y, B.out, nullptr, nullptr,
+                            nullptr, nullptr, nullptr, 0, &P);
+                drained++;
+            }
+        }
+    }
+    for (int off = 16; off; off >>= 1) drained += __shfl_down_sync(0xFFFFFFFFu, drained, off);
+    if (lane == 0 && drained) atomicAdd(park.drained, drained);
     flush_counters(t, status, counters);
 }
 
@@ -894,9 +1052,10 @@ void launch_trace(const SceneDev &S, const ViewDev &v, const int4 *ssb, const fl
     else trace_kernel<false><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, out_host);
 }
 int launch_batch(const BatchView *views, u32t n_views, u32t total_tiles, int variant, u32t chunk, u32t grid_blocks,
-                 u32t *tile_counter, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st) {
-#define ST_BATCH(TW, TH, SHS) (count ? (batch_kernel<true, TW, TH, SHS><<<grid_blocks, 128, 0, st>>>(views, n_views, total_tiles, chunk, tile_counter, status, counters), 0) \
-                                     : (batch_kernel<false, TW, TH, SHS><<<grid_blocks, 128, 0, st>>>(views, n_views, total_tiles, chunk, tile_counter, status, counters), 0))
+                 u32t *tile_counter, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st,
+                 const ParkQueue &park) {
+#define ST_BATCH(TW, TH, SHS) (count ? (batch_kernel<true, TW, TH, SHS><<<grid_blocks, 128, 0, st>>>(views, n_views, total_tiles, chunk, tile_counter, status, counters, park), 0) \
+                                     : (batch_kernel<false, TW, TH, SHS><<<grid_blocks, 128, 0, st>>>(views, n_views, total_tiles, chunk, tile_counter, status, counters, park), 0))
 #define ST_BATCH_STACKS(TW, TH) (variant_stack(variant) ? ST_BATCH(TW, TH, kSharedStackEntries) : ST_BATCH(TW, TH, 0))
     if (variant < 0 || variant >= BATCH_VARIANTS) return -1;
     switch (variant_tile(variant)) {
@@ -908,6 +1067,19 @@ int launch_batch(const BatchView *views, u32t n_views, u32t total_tiles, int var
 #undef ST_BATCH_STACKS
 #undef ST_BATCH
     return -1;
+}
+int launch_drain(const BatchView *views, const ParkQueue &park, int variant, u32t grid_blocks, unsigned *status,
+                 unsigned long long *counters, bool count, cudaStream_t st) {
+    if (variant < 0 || variant >= BATCH_VARIANTS) return -1;
+    const bool shared_stacks = variant_stack(variant) != 0;
+    if (count) {
+        if (shared_stacks) drain_kernel<true, kSharedStackEntries><<<grid_blocks, 128, 0, st>>>(views, park, status, counters);
+        else drain_kernel<true, 0><<<grid_blocks, 128, 0, st>>>(views, park, status, counters);
+    } else {
+        if (shared_stacks) drain_kernel<false, kSharedStackEntries><<<grid_blocks, 128, 0, st>>>(views, park, status, counters);
+        else drain_kernel<false, 0><<<grid_blocks, 128, 0, st>>>(views, park, status, counters);
+    }
+    return 0;
 }
 int batch_blocks_per_sm(int variant) {
     int n = 0;

@@ -39,12 +39,28 @@ struct SphereHitD { float b, c, t_near, t_far, furthest, closest_distance; };
 // Threads per block of the kernels that trace (the stride of the shared-memory stack columns).
 constexpr u32t kTraceBlock = 128;
 
+// What the walks read of the closest hit found so far (the reference's trace->closest_hit during
+// traceScene/hitPrimitives): its distance (the hit test's own distance until the hitPrimitives call
+// that found it ends, then the world distance), squared world distance and world position, and which
+// primitive and triangle it is.  The walks carry only these; the full record (normal, uv, areas ...)
+// is rebuilt once the walk is over (finalize_hit), from the same inputs and with the same arithmetic,
+// so that a lane's nested walks keep few values live.
+struct Best {
+    float distance, distance_squared;
+    v3 position;
+    u32t prim;                        // the winning primitive
+    u32t tri;                         // meshes: the winning triangle's slot in the mesh's leaf order
+};
+
 // SHS: entries of each traversal stack kept in shared memory (the block's stack columns, one per
 // thread, entry-major so that a warp's pushes hit distinct banks); the rest live in local memory.
 // Where the entries live changes no traversal step.
 template <bool CNT, int SHS = 0>
 struct TState {
-    Hit closest, mesh_closest, current;
+    Hit closest;                      // the finalized closest hit, as shading reads it
+    Best best;                        // the walk's view of it (above)
+    float mesh_distance;              // the BLAS walk's closest triangle so far (trace->closest_mesh_hit):
+    u32t mesh_tri;                    //   its distance along the object-space ray, and its slot
     SphereHitD sphere;
     RayD local;
     u32t depth;

@@ -139,7 +139,7 @@ class Batch:
     """The same views in one st_render_batch call (device outputs, autotuned, CUDA graph)."""
 
     def __init__(self, renderer, items, out_float_ptrs, out_u8_ptrs, use_graph=True, tile_shape=-1, chunk=0,
-                 stack_placement=-1, launch_mode=api.LAUNCH_AUTOTUNED):
+                 stack_placement=-1, launch_mode=api.LAUNCH_AUTOTUNED, compaction_threshold=-1):
         self.r = renderer
         self.views = (api.st_view * len(items))()
         self.keep = items
@@ -152,6 +152,7 @@ class Batch:
         self.opt.tile_shape, self.opt.chunk = tile_shape, chunk
         self.opt.stack_placement = stack_placement
         self.opt.launch_mode = launch_mode
+        self.opt.compaction_threshold = compaction_threshold
 
     def run(self):
         s = self.r.L.st_render_batch(self.r.ctx, self.views, len(self.views), C.byref(self.opt))

@@ -25,7 +25,10 @@ import oracle  # noqa: E402
 from slimtracin_b200 import scenes, structs as S  # noqa: E402
 from tests import helpers as H  # noqa: E402
 
-MONKEY = os.path.join(os.environ.get("ST_REFERENCE_SRC", "/root/reference/src"), "examples", "monkey.mesh")
+# the reference's src/ directory: $ST_REFERENCE_SRC, else a reference checkout beside this repository
+REF_SRC = os.environ.get("ST_REFERENCE_SRC") or os.path.join(
+    os.path.dirname(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))), "reference", "src")
+MONKEY = os.path.join(REF_SRC, "examples", "monkey.mesh")
 
 
 def sha(a):

@@ -119,7 +119,7 @@ def test_api_structs_and_enums_match_the_header(tmp_path):
           "ST_ERR_BAD_SCENE": api.ST_ERR_BAD_SCENE, "ST_ERR_IO": api.ST_ERR_IO,
           "ST_ERR_NOT_READY": api.ST_ERR_NOT_READY, "ST_ERR_TIMEOUT": api.ST_ERR_TIMEOUT,
           "ST_BVH_LBVH30": api.ST_BVH_LBVH30, "ST_BVH_BINNED_SAH": api.ST_BVH_BINNED_SAH,
-          "ST_BVH_REFIT": api.ST_BVH_REFIT, "ST_OVERLAY_BVH": api.OVERLAY_BVH, "ST_OVERLAY_SSB": api.OVERLAY_SSB,
+          "ST_BVH_REFIT": api.ST_BVH_REFIT, "ST_BVH_REF_SAH": api.ST_BVH_REF_SAH, "ST_OVERLAY_BVH": api.OVERLAY_BVH, "ST_OVERLAY_SSB": api.OVERLAY_SSB,
           "ST_LAUNCH_AUTOTUNED": api.LAUNCH_AUTOTUNED, "ST_LAUNCH_PER_VIEW": api.LAUNCH_PER_VIEW,
           "ST_LAUNCH_PERSISTENT": api.LAUNCH_PERSISTENT}
     for name, value in py.items():

@@ -56,6 +56,24 @@ def test_mesh_scene_small_reference_blas(renderer, mode):
     H.assert_parity(m, mode)
 
 
+@pytest.mark.parametrize("mode", [api.ST_BVH_LBVH30, api.ST_BVH_BINNED_SAH])
+def test_point_and_area_lights_device_tlas(renderer, mode):
+    """Point lights and emissive quads together under a TLAS built on the device: which occluder a
+    shadow ray finds first, and so the closest-hit record the emissive-quad test reads afterwards
+    (surface.h:14-17,55), depends on the tree's topology; given the same tree the oracle's frame and
+    work counters are the device's."""
+    sd, cam = scenes.example_area_lights()
+    renderer.upload(1, sd, tlas=None)
+    renderer.build_tlas(1, sd, mode)
+    for depth in (1, 3):
+        g = H.gpu_frame(renderer, 1, sd, cam, 320, 240, depth=depth, counters=True)
+        o = H.oracle_frame(sd, cam, 320, 240, depth=depth)
+        m = H.compare(g, o, S.RM_BEAUTY)
+        print("area, device TLAS", mode, depth, m)
+        assert np.array_equal(g.counters[:11], o.counters[:11]), (g.counters[:11], o.counters[:11])
+        H.assert_parity(m, S.RM_BEAUTY)
+
+
 def test_counters_match_oracle(renderer):
     """Same traversal, same work: every event counter equals the oracle's."""
     sd, cam = H.small_mesh_scene(subdivisions=2, texture_size=32, blas="orc")
@@ -441,3 +459,43 @@ def test_camera_facing_away_misses_everything(renderer):
     assert not np.isfinite(g.float_pixels["depth"]).any()
     assert g.float_pixels.tobytes() == o.float_pixels.tobytes()
     assert g.pixels.tobytes() == o.pixels.tobytes()
+
+
+@pytest.mark.parametrize("count", [2, 3, 16, 17, 64, 300, 1024, 4096])
+def test_ref_sah_tlas_equals_the_reference_builder(renderer, count):
+    """ST_BVH_REF_SAH: the device build of the reference's updateSceneBVH (full-sweep SAH, Lomuto
+    quicksort, right-first numbering) gives the oracle's node array, leaf ids and height byte for byte,
+    the oracle's own TLAS being pinned to the reference's (test_sah_tlas_matches_golden)."""
+    sd, cam = scenes.moving_scene(seed_offset=count, count=count)
+    if count == 300:
+        sd.primitives["position"][::7] = sd.primitives["position"][0]      # many equal sort keys
+    renderer.upload(6, sd, tlas=None)
+    renderer.build_tlas(6, sd, api.ST_BVH_REF_SAH)
+    ref = sd.copy()
+    H.tlas_sah(ref, "orc")
+    assert H.same_tlas(sd, ref)
+    boxes = np.zeros((count, 6), np.float32)
+    sc, keep = sd.to_ctypes()
+    oracle.restatement().orc_primitive_aabbs(C.byref(sc), boxes.ctypes.data)
+    _, order, nodes, node_count, height = renderer.build_lbvh(boxes, 2, api.ST_BVH_REF_SAH)
+    assert (node_count, height) == (ref.tlas_node_count, ref.tlas_height)
+    assert nodes.tobytes() == ref.tlas_nodes[:node_count].tobytes()
+    assert np.array_equal(order, ref.tlas_leaf_ids[:count])
+
+
+def test_point_and_area_lights_ref_sah_equal_the_reference(renderer):
+    """Point lights and emissive quads under the device REF_SAH TLAS: the frame equals the
+    reference's own render (with its own TLAS) within the stated tolerances, the non-libm bytes
+    exactly."""
+    sd, cam = scenes.example_area_lights()
+    renderer.upload(1, sd, tlas=None)
+    renderer.build_tlas(1, sd, api.ST_BVH_REF_SAH)
+    ref = sd.copy()
+    H.tlas_sah(ref, "ref" if oracle.reference_available() else "orc")
+    assert H.same_tlas(sd, ref)
+    for depth in (1, 3):
+        g = H.gpu_frame(renderer, 1, sd, cam, 320, 240, depth=depth)
+        r = (H.reference_frame if oracle.reference_available() else H.oracle_frame)(ref, cam, 320, 240, depth=depth)
+        m = H.compare(g, r, S.RM_BEAUTY)
+        print("area, REF_SAH TLAS vs reference", depth, m)
+        H.assert_parity(m, S.RM_BEAUTY)
