@@ -111,6 +111,22 @@ __device__ __forceinline__ bool trace_mesh(TState<CNT, SHS> &t, const SceneDev &
     return found;
 }
 
+// The primitive record again, by a load the compiler cannot merge with the first one: after a BLAS
+// walk the candidate's transform is reloaded (an L1 hit) instead of being held in registers, or
+// spilled, through the walk.
+__device__ __forceinline__ PrimDev load_prim_again(const PrimDev *p) {
+    PrimDev r;
+    asm volatile("ld.global.nc.v4.f32 {%0,%1,%2,%3}, [%4];"
+                 : "=f"(r.pos_bits.x), "=f"(r.pos_bits.y), "=f"(r.pos_bits.z), "=f"(r.pos_bits.w) : "l"(&p->pos_bits));
+    asm volatile("ld.global.nc.v4.f32 {%0,%1,%2,%3}, [%4];"
+                 : "=f"(r.rot.x), "=f"(r.rot.y), "=f"(r.rot.z), "=f"(r.rot.w) : "l"(&p->rot));
+    asm volatile("ld.global.nc.v4.f32 {%0,%1,%2,%3}, [%4];"
+                 : "=f"(r.scale_id.x), "=f"(r.scale_id.y), "=f"(r.scale_id.z), "=f"(r.scale_id.w) : "l"(&p->scale_id));
+    asm volatile("ld.global.nc.v4.f32 {%0,%1,%2,%3}, [%4];"
+                 : "=f"(r.inv_scale.x), "=f"(r.inv_scale.y), "=f"(r.inv_scale.z), "=f"(r.inv_scale.w) : "l"(&p->inv_scale));
+    return r;
+}
+
 // ---- hitPrimitives intersection/primitives.h:9 ----------------------------------------------------
 // ids == nullptr: the candidates are primitives first..first+count-1 in index order.
 // The candidate loop keeps the reference's order and comparisons; a winner updates t.best (the
@@ -172,7 +188,7 @@ __device__ __forceinline__ bool hit_primitives(TState<CNT, SHS> &t, const SceneD
             dist = hit.distance;
         }
         if (cur) {
-            pos = pos_to_world(pos, P);
+            pos = pos_to_world(pos, type == PrimitiveType_Mesh ? load_prim_again(S.prims + pid) : P);
             const float dsq = sqlen(pos - ray.origin);
             if (dsq < best.distance_squared) {
                 best.distance_squared = dsq;
@@ -829,9 +845,9 @@ __global__ void ST_TRACE_BOUNDS trace_kernel(SceneDev S, ViewDev v, const int4 *
                                                     FloatPixel *out, u32t *prim_ids, unsigned *status,
                                                     unsigned long long *counters, FloatPixel *out_host) {
     const u32t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // a block covers 16x8 grid points; each warp an 8x4 tile
-    const u32t x = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
-    const u32t y = blockIdx.y * 8 + (warp >> 1) * 4 + (lane >> 3);
+    // a block covers 8x16 grid points: four 8x4 warp tiles stacked vertically
+    const u32t x = blockIdx.x * 8 + (lane & 7);
+    const u32t y = blockIdx.y * 16 + warp * 4 + (lane >> 3);
     TState<CNT, 0> t;
     t.status = 0;
     if (CNT) for (int k = 0; k < C_COUNT; k++) t.cnt[k] = 0;
@@ -1047,7 +1063,7 @@ void launch_ray_rows(const ViewDev &v, float *dirs, cudaStream_t st) {
 void launch_trace(const SceneDev &S, const ViewDev &v, const int4 *ssb, const float *dirs, FloatPixel *out,
                   u32t *prim_ids, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st,
                   FloatPixel *out_host) {
-    dim3 grid((v.grid_w + 15) / 16, (v.grid_h + 7) / 8);
+    dim3 grid((v.grid_w + 7) / 8, (v.grid_h + 15) / 16);
     if (count) trace_kernel<true><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, out_host);
     else trace_kernel<false><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, out_host);
 }
