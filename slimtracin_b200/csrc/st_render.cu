@@ -843,11 +843,14 @@ __device__ __forceinline__ void flush_counters(TState<CNT, SHS> &t, unsigned *st
 template <bool CNT>
 __global__ void ST_TRACE_BOUNDS trace_kernel(SceneDev S, ViewDev v, const int4 *ssb, const float *dirs,
                                                     FloatPixel *out, u32t *prim_ids, unsigned *status,
-                                                    unsigned long long *counters, FloatPixel *out_host) {
+                                                    unsigned long long *counters, FloatPixel *out_host,
+                                                    int column_major) {
     const u32t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // a block covers 8x16 grid points: four 8x4 warp tiles stacked vertically
-    const u32t x = blockIdx.x * 8 + (lane & 7);
-    const u32t y = blockIdx.y * 16 + warp * 4 + (lane >> 3);
+    // a block covers 8x16 grid points: four 8x4 warp tiles stacked vertically; blocks are numbered
+    // down the columns (column_major) or along the rows
+    const u32t bx = column_major ? blockIdx.y : blockIdx.x, by = column_major ? blockIdx.x : blockIdx.y;
+    const u32t x = bx * 8 + (lane & 7);
+    const u32t y = by * 16 + warp * 4 + (lane >> 3);
     TState<CNT, 0> t;
     t.status = 0;
     if (CNT) for (int k = 0; k < C_COUNT; k++) t.cnt[k] = 0;
@@ -1063,9 +1066,15 @@ void launch_ray_rows(const ViewDev &v, float *dirs, cudaStream_t st) {
 void launch_trace(const SceneDev &S, const ViewDev &v, const int4 *ssb, const float *dirs, FloatPixel *out,
                   u32t *prim_ids, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st,
                   FloatPixel *out_host) {
-    dim3 grid((v.grid_w + 7) / 8, (v.grid_h + 15) / 16);
-    if (count) trace_kernel<true><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, out_host);
-    else trace_kernel<false><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, out_host);
+    // Blocks run in launch order, so the order decides which part of the frame is in flight at once:
+    // down the columns measured 3 % faster on the 1080p mesh frame with device outputs (2.16 against
+    // 2.24 ms), but 5 % slower when the kernel also writes the frame into page-locked host memory,
+    // whose bus writes are best issued along the rows.
+    const int column_major = out_host ? 0 : 1;
+    const u32t bw = (v.grid_w + 7) / 8, bh = (v.grid_h + 15) / 16;
+    dim3 grid = column_major ? dim3(bh, bw) : dim3(bw, bh);
+    if (count) trace_kernel<true><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, out_host, column_major);
+    else trace_kernel<false><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, out_host, column_major);
 }
 int launch_batch(const BatchView *views, u32t n_views, u32t total_tiles, int variant, u32t chunk, u32t grid_blocks,
                  u32t *tile_counter, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st,
