@@ -15,7 +15,14 @@ __device__ bool hit_triangles(TState<CNT, SHS> &t, const SceneDev &S, u32t base,
     const RayD &ray = t.local;
     bool found = false;
     for (u32t i = 0; i < n; i++) {
-        const TriHot T = S.tri_hot[base + i];
+        TriHot T;
+        {
+            const float4 *f = reinterpret_cast<const float4 *>(S.tri_hot + base + i);
+            asm("ld.global.nc.L1::evict_first.v4.f32 {%0,%1,%2,%3}, [%4];" : "=f"(T.p.x), "=f"(T.p.y), "=f"(T.p.z), "=f"(T.p.w) : "l"(f));
+            asm("ld.global.nc.L1::evict_first.v4.f32 {%0,%1,%2,%3}, [%4];" : "=f"(T.q.x), "=f"(T.q.y), "=f"(T.q.z), "=f"(T.q.w) : "l"(f + 1));
+            asm("ld.global.nc.L1::evict_first.v4.f32 {%0,%1,%2,%3}, [%4];" : "=f"(T.r.x), "=f"(T.r.y), "=f"(T.r.z), "=f"(T.r.w) : "l"(f + 2));
+            asm("ld.global.nc.L1::evict_first.v4.f32 {%0,%1,%2,%3}, [%4];" : "=f"(T.s.x), "=f"(T.s.y), "=f"(T.s.z), "=f"(T.s.w) : "l"(f + 3));
+        }
         t.count(C_TRI);
         v3 pos = V(T.p.x, T.p.y, T.p.z), nrm = V(T.p.w, T.q.x, T.q.y);
         Hit hit;
@@ -32,13 +39,17 @@ __device__ bool hit_triangles(TState<CNT, SHS> &t, const SceneDev &S, u32t base,
     return found;
 }
 
+// Cache hints: node pairs are marked to stay in L1 (evict_last; the top of every BLAS is read by
+// every ray that enters an instance), triangle records to leave first (evict_first; a triangle is
+// tested by the few neighbouring rays that reach its leaf).  Hints change no value read.  Measured on
+// the 1080p mesh frame: 2.15 against 2.18 ms, the triangle hint making the difference.
 __device__ __forceinline__ NodePair load_pair(const NodePair *p) {
     NodePair r;
     const float4 *f = reinterpret_cast<const float4 *>(p);
-    r.a = __ldg(f);
-    r.b = __ldg(f + 1);
-    r.c = __ldg(f + 2);
-    r.d = __ldg(reinterpret_cast<const uint4 *>(f + 3));
+    asm("ld.global.nc.L1::evict_last.v4.f32 {%0,%1,%2,%3}, [%4];" : "=f"(r.a.x), "=f"(r.a.y), "=f"(r.a.z), "=f"(r.a.w) : "l"(f));
+    asm("ld.global.nc.L1::evict_last.v4.f32 {%0,%1,%2,%3}, [%4];" : "=f"(r.b.x), "=f"(r.b.y), "=f"(r.b.z), "=f"(r.b.w) : "l"(f + 1));
+    asm("ld.global.nc.L1::evict_last.v4.f32 {%0,%1,%2,%3}, [%4];" : "=f"(r.c.x), "=f"(r.c.y), "=f"(r.c.z), "=f"(r.c.w) : "l"(f + 2));
+    asm("ld.global.nc.L1::evict_last.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(r.d.x), "=r"(r.d.y), "=r"(r.d.z), "=r"(r.d.w) : "l"(f + 3));
     return r;
 }
 
