@@ -16,18 +16,21 @@ roofline   the trace kernel: algorithmic bytes per frame (device event counters 
            traversal times the bytes per event of BYTES below: 32 per AABB test, 64 per triangle
            test, 72 per implicit-primitive test, 4 per leaf id, 148 per shaded hit, 12 per texel
            fetch, 24 per primary ray) / its CUDA-event time, against the measured HBM copy
-           bandwidth and an L2-resident read rate measured in the same run
+           bandwidth and the L2 read rate measured in the same run (csrc/st_peaks.cu); the
+           measured L2 and DRAM bytes of one launch come from the ncu capture in profiles/
 cpu_baseline / --impl reference
            the reference's own renderer (oracle/_ref, compiled from the reference sources) on the
            same scene bytes, all host threads, over a bounded sample of rows
 implicit16 16 implicit primitives, 3 point lights, 640x480, depth 2: the device frame beside
            the reference's CPU renderer (all host threads, and one thread)
-dynamic    4096 moving primitives, TLAS rebuilt (LBVH30, binned SAH) or refit every frame,
-           1280x720 depth 2, 300 frames: build ms (API wall time) and trace ms (device events)
+dynamic    4096 moving primitives, TLAS rebuilt (LBVH30, binned SAH, the reference's SAH) or refit
+           every frame, 1280x720 depth 2, 300 frames: build ms (API wall time) and trace ms (device
+           events)
 batched    64 views (resolutions from 256x256 to 1920x1080, 1-6 bounces) over 8 resident scenes:
-           one st_render_batch call (launch mode, tile shape, queue depth and stack placement
-           autotuned, CUDA graph) against one st_render_ex call per view, both timed with device
-           events around the whole sequence
+           one st_render_batch call (launch mode, tile shape, queue depth, stack placement and
+           compaction threshold autotuned, CUDA graph) against one st_render_ex call per view, both
+           timed with device events around the whole sequence, and how busy the device is during
+           the per-view loop
 served     Poisson request streams (--rates) over the same 8 scenes, each request a view plus a
            transform update of 0-64 primitives, u8 frames to host: the library's server against
            the same requests one at a time; p50/p99 latency from arrival to completion (library
@@ -295,8 +298,8 @@ def mixed_workloads(r, big_sd, stream, rates):
 
 
 def dynamic_tlas(r, frames, cpu_reference):
-    """The moving scene: 4096 implicit primitives, the TLAS rebuilt (LBVH30 or binned SAH) or refit
-    every frame, 1280x720 depth 2.  Per frame: the primitive records go up (whole array), the TLAS
+    """The moving scene: 4096 implicit primitives, the TLAS rebuilt (LBVH30, binned SAH, or the
+    reference's own SAH on the first 30 frames) or refit every frame, 1280x720 depth 2.  Per frame: the primitive records go up (whole array), the TLAS
     is updated through st_update_scene_bvh (wall time of the call, which includes its validity
     check of the new node array), and the frame is traced (device events)."""
     import torch
@@ -304,8 +307,9 @@ def dynamic_tlas(r, frames, cpu_reference):
     L = api.lib()
     out = {"primitives": 4096, "frames": frames, "width": 1280, "height": 720, "depth": 2}
     slot = 12
-    for name, mode in (("lbvh30", api.ST_BVH_LBVH30), ("binned_sah", api.ST_BVH_BINNED_SAH),
-                       ("refit", api.ST_BVH_REFIT)):
+    # the reference's own SAH (ST_BVH_REF_SAH) is a parity mode, timed on the first 30 frames
+    for name, mode, n_frames in (("lbvh30", api.ST_BVH_LBVH30, frames), ("binned_sah", api.ST_BVH_BINNED_SAH, frames),
+                                 ("refit", api.ST_BVH_REFIT, frames), ("ref_sah", api.ST_BVH_REF_SAH, min(frames, 30))):
         sd, cam = scenes.moving_scene()
         r.upload(slot, sd, tlas=None)
         r.build_tlas(slot, sd, api.ST_BVH_LBVH30)     # the topology a refit keeps
@@ -316,7 +320,7 @@ def dynamic_tlas(r, frames, cpu_reference):
         opt = api.st_render_options()
         opt.device_outputs, opt.out_float, opt.out_u8 = 1, dev_f.data_ptr(), dev_u.data_ptr()
         up_ms, build_ms, trace_ms = [], [], []
-        for _ in range(frames):
+        for _ in range(n_frames):
             scenes.advance_moving_scene(sd, 1)           # in place: sc.primitives sees the new records
             t0 = time.perf_counter()
             r._check(L.st_upload_primitives(r.ctx, slot, C.byref(sc)), "st_upload_primitives")
@@ -327,7 +331,8 @@ def dynamic_tlas(r, frames, cpu_reference):
             up_ms.append((t1 - t0) * 1e3)
             build_ms.append((t2 - t1) * 1e3)
             trace_ms.append(opt.trace_ms)
-        out[name] = {"build_ms_p50": float(np.median(build_ms)), "build_ms_p99": float(np.percentile(build_ms, 99)),
+        out[name] = {"frames": n_frames, "build_ms_p50": float(np.median(build_ms)),
+                     "build_ms_p99": float(np.percentile(build_ms, 99)),
                      "upload_ms_p50": float(np.median(up_ms)),
                      "trace_ms_p50": float(np.median(trace_ms)), "trace_ms_last": float(trace_ms[-1]),
                      "mrays_s": fr.rays / (float(np.median(trace_ms)) / 1e3) / 1e6}
