@@ -185,6 +185,9 @@ struct st_ctx {
     DevBuf overlay_scratch, overlay_frags;   // debug overlays: boxes/edges, and the plotted pixels
     char *upd_pinned = nullptr;          // ... and their pinned staging
     size_t upd_pinned_cap = 0;
+    // page-locked landing place of a render's status words and work counters, so that reading them
+    // back is an asynchronous copy rather than a staged one
+    unsigned long long *readback = nullptr;
     LbvhScratch lbvh;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     std::string cuda_error;
@@ -395,6 +398,10 @@ int st_init(st_ctx **out, const st_config *cfg) {
     }
     int s = reserve(ctx, ctx->status, 16);
     if (s == ST_OK) s = reserve(ctx, ctx->counters, sizeof(unsigned long long) * 16);
+    if (s == ST_OK && cudaMallocHost((void **)&ctx->readback, sizeof(unsigned long long) * 20) != cudaSuccess) {
+        ctx->readback = nullptr;
+        s = ST_ERR_OUT_OF_MEMORY;
+    }
     if (s != ST_OK) {
         st_shutdown(ctx);
         return s;
@@ -413,6 +420,7 @@ void st_shutdown(st_ctx *ctx) {
                       &ctx->upd_host_dev, &ctx->sah_scratch, &ctx->overlay_scratch, &ctx->overlay_frags})
         release(ctx, *b);
     if (ctx->upd_pinned) cudaFreeHost(ctx->upd_pinned);
+    if (ctx->readback) cudaFreeHost(ctx->readback);
     lbvh_release(ctx->lbvh);
     for (DevBuf *b : {&ctx->batch.table, &ctx->batch.ssb, &ctx->batch.seg, &ctx->batch.out_float, &ctx->batch.out_u8,
                       &ctx->batch.counter})
@@ -1112,15 +1120,13 @@ int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *view
         if (o->out_prim_id)
             ST_CUDA(cudaMemcpyAsync(o->out_prim_id, dev_ids, sizeof(u32t) * grid, cudaMemcpyDeviceToHost, st));
     }
-    unsigned status[4] = {0, 0, 0, 0};
+    unsigned *status = reinterpret_cast<unsigned *>(ctx->readback + 16);
+    unsigned long long *c = ctx->readback;
     ST_CUDA(cudaMemcpyAsync(status, ctx->status.ptr, 16, cudaMemcpyDeviceToHost, st));
-    if (o->count_work) {
-        unsigned long long c[16];
-        ST_CUDA(cudaMemcpyAsync(c, ctx->counters.ptr, sizeof(c), cudaMemcpyDeviceToHost, st));
-        ST_CUDA(cudaStreamSynchronize(st));
-        for (int k = 0; k < 16; k++) o->counters[k] = k < C_COUNT ? c[k] : 0;
-    }
+    if (o->count_work) ST_CUDA(cudaMemcpyAsync(c, ctx->counters.ptr, sizeof(unsigned long long) * 16, cudaMemcpyDeviceToHost, st));
     ST_CUDA(cudaStreamSynchronize(st));
+    if (o->count_work)
+        for (int k = 0; k < 16; k++) o->counters[k] = k < C_COUNT ? c[k] : 0;
     cudaEventElapsedTime(&o->trace_ms, ctx->ev[1], ctx->ev[2]);
     cudaEventElapsedTime(&o->total_ms, ctx->ev[0], ctx->ev[3]);
     if (status[0] & S_STACK_OVERFLOW) return ST_ERR_STACK_OVERFLOW;

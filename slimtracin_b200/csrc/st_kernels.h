@@ -95,7 +95,8 @@ int launch_drain(const BatchView *views, const ParkQueue &park, int variant, u32
                  unsigned long long *counters, bool count, cudaStream_t st);
 void tile_dims(int variant, u32t &tw, u32t &th);
 int batch_blocks_per_sm(int variant);
-// Row-segment starts of the view's ray directions: (grid_h x ceil(grid_w / kSegment)) float3.
+// Row-segment starts of the view's ray directions: ceil(grid_w / kSegment) x grid_h float3,
+// segment-major.
 void launch_ray_rows(const ViewDev &v, float *dirs, cudaStream_t st);
 inline size_t ray_rows_floats(const ViewDev &v) { return (size_t)v.grid_h * ((v.grid_w + kSegment - 1) / kSegment) * 3; }
 // out_host (optional): a device-accessible page-locked host copy of `out`, written by the kernel too

@@ -596,16 +596,18 @@ __global__ void ssb_kernel(SceneDev S, ViewDev v, int4 *ssb) {
 // row y starts at start + down added y times, pixel x at that plus right added x times.  That
 // sequence is kept exactly: one thread per row walks it and stores every kSegment-th value
 // ("segment starts", 3 MB at 1080p instead of a 25 MB direction table); the trace kernel adds
-// `right` the remaining x % kSegment times itself.
+// `right` the remaining x % kSegment times itself.  The starts are stored segment-major (segment k
+// of every row, row after row), so that the threads of a warp, one per row, write one contiguous
+// run per segment, and a warp tile's four rows read 48 contiguous bytes.
 __device__ __forceinline__ void row_segments_one(const ViewDev &v, float *seg, u32t row) {
     v3 cur = v.pp_start;
     for (u32t y = 0; y < row; y++) cur = cur + v.pp_down;
     const u32t nseg = (v.grid_w + kSegment - 1) / kSegment;
-    float *out = seg + (size_t)row * nseg * 3;
     for (u32t k = 0; k < nseg; k++) {
-        out[3 * k] = cur.x;
-        out[3 * k + 1] = cur.y;
-        out[3 * k + 2] = cur.z;
+        float *out = seg + ((size_t)k * v.grid_h + row) * 3;
+        out[0] = cur.x;
+        out[1] = cur.y;
+        out[2] = cur.z;
         for (int i = 0; i < kSegment; i++) cur = cur + v.pp_right;
     }
 }
@@ -615,8 +617,7 @@ __global__ void row_segments_kernel(ViewDev v, float *seg) {
 }
 
 __device__ __forceinline__ v3 grid_direction(const ViewDev &v, const float *seg, u32t x, u32t y) {
-    const u32t nseg = (v.grid_w + kSegment - 1) / kSegment;
-    const float *s = seg + ((size_t)y * nseg + x / kSegment) * 3;
+    const float *s = seg + ((size_t)(x / kSegment) * v.grid_h + y) * 3;
     v3 cur = V(__ldg(s), __ldg(s + 1), __ldg(s + 2));
     for (u32t i = 0; i < x % kSegment; i++) cur = cur + v.pp_right;
     return cur;
