@@ -170,6 +170,12 @@ struct Server {
     cudaMemPool_t pool = nullptr;       // per-batch arenas; keeps freed memory for the next batch
 };
 
+// A render into host memory is traced in up to this many column strips, so that each strip's float
+// grid is copied to the host while the other strips are traced.  All strips are in flight at once:
+// holding strip k back until strip k - 2 is done spreads their ends over the frame, but costs more
+// in the trace than it gains in the copies.
+constexpr int kRenderStrips = 8;
+
 struct st_ctx {
     int device = 0;
     Server server;
@@ -188,6 +194,11 @@ struct st_ctx {
     // page-locked landing place of a render's status words and work counters, so that reading them
     // back is an asynchronous copy rather than a staged one
     unsigned long long *readback = nullptr;
+    // renders into host memory, traced in column strips: one stream per strip (so that the strips
+    // run as one grid does, and each strip's copy and resolve follow its own trace), and the events
+    // that order them (created on first use)
+    cudaStream_t strip_trace[kRenderStrips] = {};
+    cudaEvent_t strip_ev[2 * kRenderStrips + 1] = {};
     LbvhScratch lbvh;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     std::string cuda_error;
@@ -421,6 +432,8 @@ void st_shutdown(st_ctx *ctx) {
         release(ctx, *b);
     if (ctx->upd_pinned) cudaFreeHost(ctx->upd_pinned);
     if (ctx->readback) cudaFreeHost(ctx->readback);
+    for (cudaEvent_t e : ctx->strip_ev) if (e) cudaEventDestroy(e);
+    for (cudaStream_t t : ctx->strip_trace) if (t) cudaStreamDestroy(t);
     lbvh_release(ctx->lbvh);
     for (DevBuf *b : {&ctx->batch.table, &ctx->batch.ssb, &ctx->batch.seg, &ctx->batch.out_float, &ctx->batch.out_u8,
                       &ctx->batch.counter})
@@ -1045,6 +1058,22 @@ static int draw_overlays(st_ctx *ctx, SceneSlot &S, const Viewport *vp, const Vi
     return ST_OK;
 }
 
+// The strips' streams get priorities falling with the strip's position, so that the block
+// scheduler starts a strip's blocks before the next strip's and the strips finish left to right,
+// each early enough for its copy to overlap the strips still being traced.
+static cudaError_t ensure_strips(st_ctx *ctx) {
+    cudaError_t e = cudaSuccess;
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    for (int k = 0; k < kRenderStrips && e == cudaSuccess; k++) {
+        const int prio = greatest + (int)((long)(least - greatest) * k / (kRenderStrips - 1));
+        if (!ctx->strip_trace[k]) e = cudaStreamCreateWithPriority(&ctx->strip_trace[k], cudaStreamNonBlocking, prio);
+    }
+    for (cudaEvent_t &ev : ctx->strip_ev)
+        if (e == cudaSuccess && !ev) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    return e;
+}
+
 int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *viewport, st_render_options *o) {
     SceneSlot *S = slot_of(ctx, slot);
     if (!S || !viewport) return ST_ERR_INVALID_ARG;
@@ -1094,27 +1123,74 @@ int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *view
     ST_CUDA(cudaEventRecord(ctx->ev[0], st));
     launch_ssb(sd, v, P<int4>(ctx->ssb), st);
     launch_ray_rows(v, P<float>(ctx->dirs), st);
-    // Page-locked host outputs are written by the kernels themselves (the float grid as it is traced,
-    // the resolved frame by the resolve kernel), so no copy follows the trace; pageable ones are
-    // copied at the end.
-    FloatPixel *mapped_float = nullptr;
-    uint32_t *mapped_u8 = nullptr;
-    if (!o->device_outputs) {
-        if (host_float && !o->skip_float_copy) mapped_float = static_cast<FloatPixel *>(device_view_of_host(host_float));
-        if (host_u8 && dev_u8) mapped_u8 = static_cast<uint32_t *>(device_view_of_host(host_u8));
-    }
+    // Host outputs.  A page-locked frame (pinned or registered) is written by the resolve kernel
+    // itself; a page-locked float grid is traced in column strips, one stream per strip, and each
+    // strip's columns are copied to the host by a 2-D DMA copy, and its pixels resolved, on its own
+    // stream as soon as it is traced, so that only the last strip's copy and resolve follow the
+    // trace.  Pageable buffers receive one copy at the end.
+    const bool host_out = !o->device_outputs;
+    const bool want_float = host_out && host_float && !o->skip_float_copy;
+    uint32_t *mapped_u8 = host_out && host_u8 && dev_u8 ? static_cast<uint32_t *>(device_view_of_host(host_u8)) : nullptr;
+    const bool float_pinned = want_float && device_view_of_host(host_float) != nullptr;
+    const bool overlays = (o->overlays & (ST_OVERLAY_BVH | ST_OVERLAY_SSB)) != 0;
+    const u32t bw = (v.grid_w + 7) / 8;
+    const int strips = (host_out && !overlays && (!want_float || float_pinned))
+                           ? (int)std::max(1u, std::min((u32t)kRenderStrips, bw / 24)) : 1;
+    uint32_t *u8_target = mapped_u8 ? mapped_u8 : dev_u8;
     ST_CUDA(cudaEventRecord(ctx->ev[1], st));
-    launch_trace(sd, v, P<int4>(ctx->ssb), P<float>(ctx->dirs), dev_float, dev_ids, P<unsigned>(ctx->status),
-                 P<unsigned long long>(ctx->counters), o->count_work != 0, st, mapped_float);
-    ST_CUDA(cudaGetLastError());
-    ST_CUDA(cudaEventRecord(ctx->ev[2], st));
-    if (o->overlays & (ST_OVERLAY_BVH | ST_OVERLAY_SSB))
-        ST_TRY(draw_overlays(ctx, *S, viewport, v, o->overlays, dev_float, mapped_float, st));
-    if (dev_u8) launch_resolve(dev_float, v.grid_w, W, H, mapped_u8 ? mapped_u8 : dev_u8, st);
-    ST_CUDA(cudaEventRecord(ctx->ev[3], st));
-    if (!o->device_outputs) {
-        if (host_float && !o->skip_float_copy && !mapped_float)
+    if (strips > 1) {
+        ST_CUDA(ensure_strips(ctx));
+        cudaEvent_t *done = ctx->strip_ev, *joined = ctx->strip_ev + kRenderStrips;   // per strip
+        cudaEvent_t fork = ctx->strip_ev[2 * kRenderStrips];
+        ST_CUDA(cudaEventRecord(fork, st));
+        const size_t pitch = sizeof(FloatPixel) * v.grid_w;
+        auto strip_cols = [&](int k, u32t &gx0, u32t &gx1) {
+            gx0 = (u32t)((uint64_t)bw * k / strips) * 8;
+            gx1 = std::min((u32t)((uint64_t)bw * (k + 1) / strips) * 8, v.grid_w);
+        };
+        // every trace is launched before any copy, so that a stream which shares a hardware queue
+        // with another never holds that stream's trace behind its own copy
+        for (int k = 0; k < strips; k++) {
+            u32t gx0, gx1;
+            strip_cols(k, gx0, gx1);
+            cudaStream_t ts = ctx->strip_trace[k];
+            ST_CUDA(cudaStreamWaitEvent(ts, fork, 0));
+            launch_trace(sd, v, P<int4>(ctx->ssb), P<float>(ctx->dirs), dev_float, dev_ids, P<unsigned>(ctx->status),
+                         P<unsigned long long>(ctx->counters), o->count_work != 0, ts, gx0 / 8, (gx1 - gx0 + 7) / 8);
+            ST_CUDA(cudaGetLastError());
+            ST_CUDA(cudaEventRecord(done[k], ts));
+        }
+        // each strip's columns are copied behind its own trace, whatever order the strips end in;
+        // pixel x reads grid columns x and x + 1, so a strip's pixels [gx0 - 1, gx1 - 1) are resolved
+        // once its left neighbour is traced too
+        for (int k = 0; k < strips; k++) {
+            u32t gx0, gx1;
+            strip_cols(k, gx0, gx1);
+            cudaStream_t ts = ctx->strip_trace[k];
+            if (want_float)
+                ST_CUDA(cudaMemcpy2DAsync(host_float + gx0, pitch, dev_float + gx0, pitch, sizeof(FloatPixel) * (gx1 - gx0),
+                                          v.grid_h, cudaMemcpyDeviceToHost, ts));
+            if (u8_target) {
+                if (k > 0) ST_CUDA(cudaStreamWaitEvent(ts, done[k - 1], 0));
+                launch_resolve(dev_float, v.grid_w, W, H, u8_target, ts, k > 0 ? gx0 - 1 : 0, k + 1 == strips ? W : gx1 - 1);
+            }
+            ST_CUDA(cudaEventRecord(joined[k], ts));
+        }
+        for (int k = 0; k < strips; k++) ST_CUDA(cudaStreamWaitEvent(st, done[k], 0));
+        ST_CUDA(cudaEventRecord(ctx->ev[2], st));
+        for (int k = 0; k < strips; k++) ST_CUDA(cudaStreamWaitEvent(st, joined[k], 0));
+    } else {
+        launch_trace(sd, v, P<int4>(ctx->ssb), P<float>(ctx->dirs), dev_float, dev_ids, P<unsigned>(ctx->status),
+                     P<unsigned long long>(ctx->counters), o->count_work != 0, st);
+        ST_CUDA(cudaGetLastError());
+        ST_CUDA(cudaEventRecord(ctx->ev[2], st));
+        if (overlays) ST_TRY(draw_overlays(ctx, *S, viewport, v, o->overlays, dev_float, nullptr, st));
+        if (u8_target) launch_resolve(dev_float, v.grid_w, W, H, u8_target, st);
+        if (want_float)
             ST_CUDA(cudaMemcpyAsync(host_float, dev_float, sizeof(FloatPixel) * grid, cudaMemcpyDeviceToHost, st));
+    }
+    ST_CUDA(cudaEventRecord(ctx->ev[3], st));
+    if (host_out) {
         if (host_u8 && dev_u8 && !mapped_u8)
             ST_CUDA(cudaMemcpyAsync(host_u8, dev_u8, sizeof(uint32_t) * (size_t)W * H, cudaMemcpyDeviceToHost, st));
         if (o->out_prim_id)

@@ -99,10 +99,11 @@ int batch_blocks_per_sm(int variant);
 // segment-major.
 void launch_ray_rows(const ViewDev &v, float *dirs, cudaStream_t st);
 inline size_t ray_rows_floats(const ViewDev &v) { return (size_t)v.grid_h * ((v.grid_w + kSegment - 1) / kSegment) * 3; }
-// out_host (optional): a device-accessible page-locked host copy of `out`, written by the kernel too
+// Block columns [bx_first, bx_first + bx_count) of the grid (8 grid points wide each; bx_count 0:
+// to the last column).
 void launch_trace(const SceneDev &S, const ViewDev &v, const int4 *ssb, const float *dirs, FloatPixel *out,
                   u32t *prim_ids, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st,
-                  FloatPixel *out_host = nullptr);
+                  u32t bx_first = 0, u32t bx_count = 0);
 // The result of a pick (layout of st_pick_result)
 struct PickDev {
     int found, object_type;
@@ -111,7 +112,9 @@ struct PickDev {
     float distance, object_distance;
 };
 void launch_pick(const SceneDev &S, const ViewDev &v, const int4 *ssb, int x, int y, PickDev *out, cudaStream_t st);
-void launch_resolve(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out, cudaStream_t st);
+// Pixel columns [x0, x1) of the QCAA resolve (all of them by default).
+void launch_resolve(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out, cudaStream_t st,
+                    u32t x0 = 0, u32t x1 = 0xFFFFFFFFu);
 // A batch's SSBs and ray-row starts (every view of the table), and its resolves (views with out_u8).
 void launch_batch_setup(const BatchTable &T, u32t n_views, u32t max_prims, u32t max_rows, cudaStream_t st);
 void launch_batch_resolve(const BatchTable &T, u32t n_views, u32t max_width, u32t max_height, cudaStream_t st);

@@ -864,55 +864,18 @@ __device__ __forceinline__ void flush_counters(TState<CNT, SHS> &t, unsigned *st
 template <bool CNT>
 __global__ void ST_TRACE_BOUNDS trace_kernel(SceneDev S, ViewDev v, const int4 *ssb, const float *dirs,
                                                     FloatPixel *out, u32t *prim_ids, unsigned *status,
-                                                    unsigned long long *counters, FloatPixel *out_host,
-                                                    int column_major) {
+                                                    unsigned long long *counters, u32t bx_first) {
     const u32t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // a block covers 8x16 grid points: four 8x4 warp tiles stacked vertically; blocks are numbered
-    // down the columns (column_major) or along the rows
-    const u32t bx = column_major ? blockIdx.y : blockIdx.x, by = column_major ? blockIdx.x : blockIdx.y;
-    const u32t x = bx * 8 + (lane & 7);
-    const u32t y = by * 16 + warp * 4 + (lane >> 3);
+    // A block covers 8x16 grid points: four 8x4 warp tiles stacked vertically.  Blocks are numbered
+    // down the columns, starting at block column bx_first: blocks start in launch order, so this
+    // decides which part of the frame is in flight at once (down the columns measured 3 % faster on
+    // the 1080p mesh frame than along the rows).
+    const u32t x = (blockIdx.y + bx_first) * 8 + (lane & 7);
+    const u32t y = blockIdx.x * 16 + warp * 4 + (lane >> 3);
     TState<CNT, 0> t;
     t.status = 0;
     if (CNT) for (int k = 0; k < C_COUNT; k++) t.cnt[k] = 0;
-    const bool active = x < v.grid_w && y < v.grid_h;
-    float4 c = make_float4(0, 0, 0, 0);
-    double d = 0;
-    if (active) trace_point(t, S, v, ssb, dirs, x, y, out, prim_ids, out_host, &c, &d);
-    if (active) {
-        const size_t idx = (size_t)y * v.grid_w + x;
-        float2 *o = reinterpret_cast<float2 *>(out + idx);
-        o[0] = make_float2(c.x, c.y);
-        o[1] = make_float2(c.z, c.w);
-        reinterpret_cast<double *>(o)[2] = d;
-    }
-    // A page-locked host copy is written over the bus as the frame is traced.  The warp's 8x4
-    // FloatPixels go out as contiguous 8-byte runs, each store instruction covering 256 bytes of
-    // whole grid rows instead of one 8-byte part of 32 pixels 24 bytes apart, so that the bus
-    // writes carry full lines.
-    if (out_host) {
-        const u32t x0 = x - (lane & 7), y0 = y - (lane >> 3);
-        if (x0 + 8 <= v.grid_w && y0 + 4 <= v.grid_h) {          // warp-uniform: the whole tile is inside
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                const u32t chunk = 32 * k + lane, row = chunk / 24, j = chunk % 24, src = row * 8 + j / 3, part = j % 3;
-                const float a0 = __shfl_sync(0xFFFFFFFFu, c.x, src), a1 = __shfl_sync(0xFFFFFFFFu, c.y, src);
-                const float b0 = __shfl_sync(0xFFFFFFFFu, c.z, src), b1 = __shfl_sync(0xFFFFFFFFu, c.w, src);
-                const double dd = __shfl_sync(0xFFFFFFFFu, d, src);
-                const unsigned long long bits =
-                    part == 0 ? ((unsigned long long)__float_as_uint(a1) << 32) | __float_as_uint(a0)
-                    : part == 1 ? ((unsigned long long)__float_as_uint(b1) << 32) | __float_as_uint(b0)
-                                : (unsigned long long)__double_as_longlong(dd);
-                const size_t byte = ((size_t)(y0 + row) * v.grid_w + x0) * sizeof(FloatPixel) + 8 * j;
-                *reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(out_host) + byte) = bits;
-            }
-        } else if (active) {
-            float2 *h = reinterpret_cast<float2 *>(out_host + (size_t)y * v.grid_w + x);
-            h[0] = make_float2(c.x, c.y);
-            h[1] = make_float2(c.z, c.w);
-            reinterpret_cast<double *>(h)[2] = d;
-        }
-    }
+    if (x < v.grid_w && y < v.grid_h) trace_point(t, S, v, ssb, dirs, x, y, out, prim_ids);
     flush_counters(t, status, counters);
 }
 
@@ -1050,9 +1013,11 @@ __device__ __forceinline__ void resolve_one(const FloatPixel *in, u32t grid_w, u
     }
     out[(size_t)y * width + x] = px;
 }
-__global__ void resolve_kernel(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out) {
-    const u32t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x < width && y < height) resolve_one(in, grid_w, width, out, x, y);
+// Pixel columns [x0, x1) of the frame (pixel x reads grid columns x and x + 1).
+__global__ void resolve_kernel(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out, u32t x0,
+                               u32t x1) {
+    const u32t x = x0 + blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x < x1 && x < width && y < height) resolve_one(in, grid_w, width, out, x, y);
 }
 
 // ---- a batch's per-view set-up and resolve, driven by the view table (one launch each) ----------
@@ -1086,16 +1051,13 @@ void launch_ray_rows(const ViewDev &v, float *dirs, cudaStream_t st) {
 }
 void launch_trace(const SceneDev &S, const ViewDev &v, const int4 *ssb, const float *dirs, FloatPixel *out,
                   u32t *prim_ids, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st,
-                  FloatPixel *out_host) {
-    // Blocks run in launch order, so the order decides which part of the frame is in flight at once:
-    // down the columns measured 3 % faster on the 1080p mesh frame with device outputs (2.16 against
-    // 2.24 ms), but 5 % slower when the kernel also writes the frame into page-locked host memory,
-    // whose bus writes are best issued along the rows.
-    const int column_major = out_host ? 0 : 1;
+                  u32t bx_first, u32t bx_count) {
     const u32t bw = (v.grid_w + 7) / 8, bh = (v.grid_h + 15) / 16;
-    dim3 grid = column_major ? dim3(bh, bw) : dim3(bw, bh);
-    if (count) trace_kernel<true><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, out_host, column_major);
-    else trace_kernel<false><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, out_host, column_major);
+    if (bx_first >= bw) return;
+    if (!bx_count || bx_first + bx_count > bw) bx_count = bw - bx_first;
+    const dim3 grid(bh, bx_count);
+    if (count) trace_kernel<true><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, bx_first);
+    else trace_kernel<false><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, bx_first);
 }
 int launch_batch(const BatchView *views, u32t n_views, u32t total_tiles, int variant, u32t chunk, u32t grid_blocks,
                  u32t *tile_counter, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st,
@@ -1159,9 +1121,12 @@ void launch_batch_setup(const BatchTable &T, u32t n_views, u32t max_prims, u32t 
 void launch_batch_resolve(const BatchTable &T, u32t n_views, u32t max_width, u32t max_height, cudaStream_t st) {
     batch_resolve_kernel<<<dim3((max_width + 127) / 128, max_height, n_views), 128, 0, st>>>(T, n_views);
 }
-void launch_resolve(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out, cudaStream_t st) {
-    dim3 grid((width + 127) / 128, height);
-    resolve_kernel<<<grid, 128, 0, st>>>(in, grid_w, width, height, out);
+void launch_resolve(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out, cudaStream_t st,
+                    u32t x0, u32t x1) {
+    if (x1 > width) x1 = width;
+    if (x0 >= x1) return;
+    dim3 grid((x1 - x0 + 127) / 128, height);
+    resolve_kernel<<<grid, 128, 0, st>>>(in, grid_w, width, height, out, x0, x1);
 }
 
 }  // namespace st

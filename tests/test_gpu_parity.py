@@ -318,6 +318,31 @@ def test_pinned_host_outputs_written_by_the_kernels(renderer):
     assert np.array_equal(pu.numpy(), pageable.pixels.view(np.uint8))
 
 
+@pytest.mark.parametrize("w,h", [(1920, 1080), (1283, 721)])
+def test_pinned_outputs_traced_in_strips(renderer, w, h):
+    """Page-locked outputs at frame sizes that are traced in column strips (each strip's grid copied
+    to the host while later strips trace, its pixels resolved as soon as their columns are done):
+    float grid and frame byte-identical to the same view rendered into pageable buffers, also with
+    the frame alone (no float grid)."""
+    import torch
+    c1, cam1 = H.small_mesh_scene(subdivisions=3, texture_size=64, blas="orc")
+    H.tlas_sah(c1)
+    renderer.upload(14, c1, tlas="host")
+    pageable = scenes.Frame(w, h, cam1, depth=4)
+    renderer.render(14, c1, pageable)
+    sc, keep = c1.to_ctypes()
+    for with_float in (True, False):
+        pinned = scenes.Frame(w, h, cam1, depth=4, with_pixels=False, with_float=False)
+        pf = torch.zeros(pinned.rays * 24, dtype=torch.uint8, pin_memory=True)
+        pu = torch.zeros(w * h * 4, dtype=torch.uint8, pin_memory=True)
+        pinned.grid.float_pixels = pf.data_ptr() if with_float else None
+        pinned.grid.pixels = pu.data_ptr()
+        assert api.lib().st_render_scene(renderer.ctx, 14, C.byref(sc), C.byref(pinned.viewport)) == 0
+        if with_float:
+            assert np.array_equal(pf.numpy(), pageable.float_pixels.view(np.uint8))
+        assert np.array_equal(pu.numpy(), pageable.pixels.view(np.uint8)), with_float
+
+
 @pytest.mark.parametrize("which", ["implicit16", "mesh"])
 def test_pick_equals_oracle(renderer, which):
     """st_pick (manipulateSelection's picking ray on the device) equals the oracle's pick bit for bit
