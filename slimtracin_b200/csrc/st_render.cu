@@ -626,8 +626,6 @@ __device__ __forceinline__ v3 grid_direction(const ViewDev &v, const float *seg,
 // rayTrace render/raytracer.h:81 for one QCAA grid point, writing the FloatPixel the reference's
 // setPixel leaves after beginDrawing's clear (viewport.h:88): hit -> (color, 1, z), miss ->
 // (black, 0, +inf).
-// ret_c / ret_d (optional): the point's FloatPixel (colour and opacity, depth) is returned there
-// instead of being written to out / out_host.
 // park (optional): at each bounce, a warp whose lanes still tracing number fewer than
 // park->threshold parks those lanes' paths in the queue (returns false: the point is not finished,
 // nothing is written); resume (optional): a parked path, continued from its bounce ray.  A path
@@ -635,8 +633,7 @@ __device__ __forceinline__ v3 grid_direction(const ViewDev &v, const float *seg,
 template <bool CNT, int SHS>
 __device__ __forceinline__ bool trace_point(TState<CNT, SHS> &t, const SceneDev &S, const ViewDev &v, const int4 *ssb,
                                             const float *dirs, u32t x, u32t y, FloatPixel *out, u32t *prim_ids,
-                                            FloatPixel *out_host = nullptr, float4 *ret_c = nullptr,
-                                            double *ret_d = nullptr, const ParkQueue *park = nullptr,
+                                            const ParkQueue *park = nullptr,
                                             u32t view_index = 0, const ParkedRay *resume = nullptr) {
     const size_t idx = (size_t)y * v.grid_w + x;
     const v3 Ro = v.cam_pos, Rd = norm(grid_direction(v, dirs, x, y));
@@ -687,7 +684,7 @@ __device__ __forceinline__ bool trace_point(TState<CNT, SHS> &t, const SceneDev 
         if (primary) {                                      // rayTrace after the hit test (raytracer.h:89)
             primary = false;
             hit_found = found;
-            if (prim_ids) prim_ids[idx] = found ? hit.object_id : 0xFFFFFFFFu;
+            if (prim_ids) __stcs(prim_ids + idx, found ? hit.object_id : 0xFFFFFFFFu);
             closest_distance = found ? hit.distance : INFINITY;
             if (!found) break;
             z = qrot(hit.position - v.cam_pos, v.cam_rot_inv).z;
@@ -822,21 +819,12 @@ __device__ __forceinline__ bool trace_point(TState<CNT, SHS> &t, const SceneDev 
         c01 = make_float4(0, 0, 0, 0);
         depth = (double)INFINITY;
     }
-    if (ret_c) {
-        *ret_c = c01;
-        *ret_d = depth;
-        return true;
-    }
+    // streaming stores: the grid is written once and read back by a copy or the resolve, so its
+    // lines go first from L2 rather than the scene's nodes (0.5 % off the 1080p mesh frame)
     float2 *o = reinterpret_cast<float2 *>(out + idx);
-    o[0] = make_float2(c01.x, c01.y);
-    o[1] = make_float2(c01.z, c01.w);
-    reinterpret_cast<double *>(o)[2] = depth;
-    if (out_host) {        // the caller's page-locked host buffer, written over the bus as the frame is traced
-        float2 *h = reinterpret_cast<float2 *>(out_host + idx);
-        h[0] = make_float2(c01.x, c01.y);
-        h[1] = make_float2(c01.z, c01.w);
-        reinterpret_cast<double *>(h)[2] = depth;
-    }
+    __stcs(o, make_float2(c01.x, c01.y));
+    __stcs(o + 1, make_float2(c01.z, c01.w));
+    __stcs(reinterpret_cast<double *>(o) + 2, depth);
     return true;
 }
 
@@ -954,8 +942,7 @@ __global__ void ST_TRACE_BOUNDS batch_kernel(const BatchView *views, u32t n_view
             const u32t tx = 2 * (group % B.tiles_x) + (q & 1), ty = 2 * (group / B.tiles_x) + (q >> 1);
             const u32t x = tx * TW + (lane % TW), y = ty * TH + (lane / TW);
             if (x < B.view.grid_w && y < B.view.grid_h)
-                trace_point(t, B.scene, B.view, B.ssb, B.dirs, x, y, B.out, B.prim_ids, nullptr, nullptr, nullptr,
-                            &park, vi);
+                trace_point(t, B.scene, B.view, B.ssb, B.dirs, x, y, B.out, B.prim_ids, &park, vi);
         }
     }
     flush_counters(t, status, counters);
@@ -984,8 +971,7 @@ __global__ void ST_TRACE_BOUNDS drain_kernel(const BatchView *views, ParkQueue p
             const ParkedRay P = park.rays[i];
             if (P.where.z != kEmptySlot) {
                 const BatchView &B = views[P.where.z];
-                trace_point(t, B.scene, B.view, B.ssb, B.dirs, P.where.x, P.where.y, B.out, nullptr, nullptr,
-                            nullptr, nullptr, nullptr, 0, &P);
+                trace_point(t, B.scene, B.view, B.ssb, B.dirs, P.where.x, P.where.y, B.out, nullptr, nullptr, 0, &P);
                 drained++;
             }
         }
@@ -1013,11 +999,14 @@ __device__ __forceinline__ void resolve_one(const FloatPixel *in, u32t grid_w, u
     }
     out[(size_t)y * width + x] = px;
 }
-// Pixel columns [x0, x1) of the frame (pixel x reads grid columns x and x + 1).
+// Pixel columns [x0, x1) of the frame (pixel x reads grid columns x and x + 1), one thread per
+// pixel along the rows of the range, so that a narrow range leaves no block mostly idle.
 __global__ void resolve_kernel(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out, u32t x0,
                                u32t x1) {
-    const u32t x = x0 + blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x < x1 && x < width && y < height) resolve_one(in, grid_w, width, out, x, y);
+    const u32t n = x1 - x0;
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const u32t y = (u32t)(i / n), x = x0 + (u32t)(i % n);
+    if (y < height) resolve_one(in, grid_w, width, out, x, y);
 }
 
 // ---- a batch's per-view set-up and resolve, driven by the view table (one launch each) ----------
@@ -1124,9 +1113,9 @@ void launch_batch_resolve(const BatchTable &T, u32t n_views, u32t max_width, u32
 void launch_resolve(const FloatPixel *in, u32t grid_w, u32t width, u32t height, uint32_t *out, cudaStream_t st,
                     u32t x0, u32t x1) {
     if (x1 > width) x1 = width;
-    if (x0 >= x1) return;
-    dim3 grid((x1 - x0 + 127) / 128, height);
-    resolve_kernel<<<grid, 128, 0, st>>>(in, grid_w, width, height, out, x0, x1);
+    if (x0 >= x1 || !height) return;
+    const size_t pixels = (size_t)(x1 - x0) * height;
+    resolve_kernel<<<(unsigned)((pixels + 255) / 256), 256, 0, st>>>(in, grid_w, width, height, out, x0, x1);
 }
 
 }  // namespace st

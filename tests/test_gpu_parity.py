@@ -318,12 +318,13 @@ def test_pinned_host_outputs_written_by_the_kernels(renderer):
     assert np.array_equal(pu.numpy(), pageable.pixels.view(np.uint8))
 
 
-@pytest.mark.parametrize("w,h", [(1920, 1080), (1283, 721)])
+@pytest.mark.parametrize("w,h", [(1920, 1080), (1283, 721), (4000, 300), (400, 200), (135, 130)])
 def test_pinned_outputs_traced_in_strips(renderer, w, h):
     """Page-locked outputs at frame sizes that are traced in column strips (each strip's grid copied
-    to the host while later strips trace, its pixels resolved as soon as their columns are done):
-    float grid and frame byte-identical to the same view rendered into pageable buffers, also with
-    the frame alone (no float grid)."""
+    to the host while later strips trace, its pixels resolved as soon as their columns are done;
+    1920 and 4000 wide make eight strips, 1283 six of unequal widths, 400 two, 135 one): float grid
+    and frame byte-identical to the same view rendered into pageable buffers, also with the frame
+    alone (no float grid)."""
     import torch
     c1, cam1 = H.small_mesh_scene(subdivisions=3, texture_size=64, blas="orc")
     H.tlas_sah(c1)
