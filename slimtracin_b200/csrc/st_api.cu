@@ -1156,7 +1156,8 @@ int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *view
             cudaStream_t ts = ctx->strip_trace[k];
             ST_CUDA(cudaStreamWaitEvent(ts, fork, 0));
             launch_trace(sd, v, P<int4>(ctx->ssb), P<float>(ctx->dirs), dev_float, dev_ids, P<unsigned>(ctx->status),
-                         P<unsigned long long>(ctx->counters), o->count_work != 0, ts, gx0 / 8, (gx1 - gx0 + 7) / 8);
+                         P<unsigned long long>(ctx->counters), o->count_work != 0, ts, gx0 / 8, (gx1 - gx0 + 7) / 8,
+                         want_float);
             ST_CUDA(cudaGetLastError());
             ST_CUDA(cudaEventRecord(done[k], ts));
         }

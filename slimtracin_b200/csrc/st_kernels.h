@@ -100,10 +100,11 @@ int batch_blocks_per_sm(int variant);
 void launch_ray_rows(const ViewDev &v, float *dirs, cudaStream_t st);
 inline size_t ray_rows_floats(const ViewDev &v) { return (size_t)v.grid_h * ((v.grid_w + kSegment - 1) / kSegment) * 3; }
 // Block columns [bx_first, bx_first + bx_count) of the grid (8 grid points wide each; bx_count 0:
-// to the last column).
+// to the last column).  overlapped: the grid is copied to the host while it is traced (the kernel
+// then runs with fewer blocks per SM).
 void launch_trace(const SceneDev &S, const ViewDev &v, const int4 *ssb, const float *dirs, FloatPixel *out,
                   u32t *prim_ids, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st,
-                  u32t bx_first = 0, u32t bx_count = 0);
+                  u32t bx_first = 0, u32t bx_count = 0, bool overlapped = false);
 // The result of a pick (layout of st_pick_result)
 struct PickDev {
     int found, object_type;

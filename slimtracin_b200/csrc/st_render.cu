@@ -845,14 +845,20 @@ __device__ __forceinline__ void flush_counters(TState<CNT, SHS> &t, unsigned *st
 // spills) beat the compiler's own choice of 128 registers (four blocks) on the 1080p mesh frame
 // (2.38 vs 2.62 ms), and six and seven blocks (2.42, 2.40 ms) there, on the 64-view mixed batch and
 // on the served stream; 5 blocks measured 2.52 ms, 2 blocks 5.6 ms.
+// A frame whose float grid is copied to the host while it is traced runs with fewer blocks (more
+// registers, fewer spills): its spill traffic and the copies slow each other, and on the 1080p mesh
+// frame six blocks measured 2.19 ms alone but 798-803 Mrays/s end to end against 776 at eight.
 #ifndef ST_TRACE_MIN_BLOCKS
 #define ST_TRACE_MIN_BLOCKS 8
 #endif
+#ifndef ST_TRACE_OVERLAP_MIN_BLOCKS
+#define ST_TRACE_OVERLAP_MIN_BLOCKS 6
+#endif
 #define ST_TRACE_BOUNDS __launch_bounds__(128, ST_TRACE_MIN_BLOCKS)
-template <bool CNT>
-__global__ void ST_TRACE_BOUNDS trace_kernel(SceneDev S, ViewDev v, const int4 *ssb, const float *dirs,
-                                                    FloatPixel *out, u32t *prim_ids, unsigned *status,
-                                                    unsigned long long *counters, u32t bx_first) {
+template <bool CNT, int MINB>
+__global__ void __launch_bounds__(128, MINB) trace_kernel(SceneDev S, ViewDev v, const int4 *ssb, const float *dirs,
+                                                          FloatPixel *out, u32t *prim_ids, unsigned *status,
+                                                          unsigned long long *counters, u32t bx_first) {
     const u32t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // A block covers 8x16 grid points: four 8x4 warp tiles stacked vertically.  Blocks are numbered
     // down the columns, starting at block column bx_first: blocks start in launch order, so this
@@ -1040,13 +1046,20 @@ void launch_ray_rows(const ViewDev &v, float *dirs, cudaStream_t st) {
 }
 void launch_trace(const SceneDev &S, const ViewDev &v, const int4 *ssb, const float *dirs, FloatPixel *out,
                   u32t *prim_ids, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st,
-                  u32t bx_first, u32t bx_count) {
+                  u32t bx_first, u32t bx_count, bool overlapped) {
     const u32t bw = (v.grid_w + 7) / 8, bh = (v.grid_h + 15) / 16;
     if (bx_first >= bw) return;
     if (!bx_count || bx_first + bx_count > bw) bx_count = bw - bx_first;
     const dim3 grid(bh, bx_count);
-    if (count) trace_kernel<true><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, bx_first);
-    else trace_kernel<false><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, bx_first);
+    constexpr int A = ST_TRACE_MIN_BLOCKS, B = ST_TRACE_OVERLAP_MIN_BLOCKS;
+    if (count && overlapped)
+        trace_kernel<true, B><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, bx_first);
+    else if (count)
+        trace_kernel<true, A><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, bx_first);
+    else if (overlapped)
+        trace_kernel<false, B><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, bx_first);
+    else
+        trace_kernel<false, A><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, bx_first);
 }
 int launch_batch(const BatchView *views, u32t n_views, u32t total_tiles, int variant, u32t chunk, u32t grid_blocks,
                  u32t *tile_counter, unsigned *status, unsigned long long *counters, bool count, cudaStream_t st,
