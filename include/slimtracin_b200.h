@@ -207,7 +207,7 @@ typedef struct st_batch_options {
     void *stream;               /* cudaStream_t; NULL -> the context's stream */
     int device_outputs;         /* 1: out_* are device pointers */
     int tile_shape;             /* -1: autotuned; 0: 8x4, 1: 16x2, 2: 32x1, 3: 4x8 grid points per warp */
-    int chunk;                  /* tiles a warp takes per queue fetch; 0: autotuned */
+    int chunk;                  /* groups of four tiles a block takes per queue fetch (a tile per warp); 0: autotuned */
     int use_graph;              /* 1: launch through a CUDA graph: the batch's launches are captured and an
                                    instantiated graph of the same topology is updated in place */
     float batch_ms;             /* out: CUDA-event time of the batch on the launch stream */

@@ -1223,14 +1223,15 @@ struct BatchPlan {
     std::string shape_key, class_key;
 };
 
-// A view's tiles are numbered in 2x2 groups of warp tiles, so that the four warps of a block, which
-// fetch consecutive tiles, trace one compact region as the per-frame kernel's blocks do.  Sets
-// b.tiles_x (groups per row) and returns the number of tile slots (4 per group; slots of a group
-// that fall outside the view have no grid points).
+// A view's tiles are numbered in groups of four warp tiles (group_tiles_w across), groups down
+// the view's columns, so that the four warps of a block, which take one group, trace one compact
+// region as the per-frame kernel's blocks do.  Sets b.groups_y and returns the number of tile
+// slots (4 per group; slots of a group that fall outside the view have no grid points).
 u32t view_tiles(BatchView &b, u32t tw, u32t th) {
+    const u32t gw = group_tiles_w((int)tw), gh = 4 / gw;
     const u32t tx = (b.view.grid_w + tw - 1) / tw, ty = (b.view.grid_h + th - 1) / th;
-    b.tiles_x = (tx + 1) / 2;
-    return 4 * b.tiles_x * ((ty + 1) / 2);
+    b.groups_y = (ty + gh - 1) / gh;
+    return 4 * ((tx + gw - 1) / gw) * b.groups_y;
 }
 
 int plan_batch(st_ctx *ctx, const st_view *views, int n, int tile, const st_batch_options &o, BatchPlan &p) {

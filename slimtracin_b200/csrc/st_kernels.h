@@ -34,8 +34,12 @@ struct BatchView {
     FloatPixel *out;
     u32t *prim_ids;
     uint32_t *out_u8;              // resolved frame (device), or null
-    u32t tile_begin, tiles_x;      // first tile slot; 2x2 groups of warp tiles per row
+    u32t tile_begin;               // first tile slot (4 per group of warp tiles)
+    u32t groups_y;                 // groups of warp tiles per column of groups
 };
+// Warp tiles across one group of four: groups cover about 8x16 grid points (four 8x4 tiles
+// stacked, 2x2 tiles of 4x8, four 16x2 or 32x1 tiles stacked).
+__host__ __device__ constexpr u32t group_tiles_w(int tile_w) { return tile_w >= 8 ? 1u : 2u; }
 // A batch's views as a kernel parameter of its set-up and resolve kernels: one launch group takes at
 // most kTableViews views.  (The trace kernel reads the same views from device memory: indexed by a
 // tile's view, kernel-parameter memory measured slower there than an L1-cached table.)
