@@ -845,11 +845,16 @@ __device__ __forceinline__ void flush_counters(TState<CNT, SHS> &t, unsigned *st
 // spills) beat the compiler's own choice of 128 registers (four blocks) on the 1080p mesh frame
 // (2.38 vs 2.62 ms), and six and seven blocks (2.42, 2.40 ms) there, on the 64-view mixed batch and
 // on the served stream; 5 blocks measured 2.52 ms, 2 blocks 5.6 ms.
-// A frame whose float grid is copied to the host while it is traced runs with fewer blocks (more
-// registers, fewer spills): its spill traffic and the copies slow each other, and on the 1080p mesh
-// frame six blocks measured 2.19 ms alone but 798-803 Mrays/s end to end against 776 at eight.
+// The per-frame trace kernel with device outputs runs nine blocks (56 registers): 2.101 ms against
+// 2.110 at eight and 2.176 at ten on the 1080p mesh frame.  A frame whose float grid is copied to
+// the host while it is traced runs with fewer blocks (more registers, fewer spills): its spill
+// traffic and the copies slow each other, and on the 1080p mesh frame six blocks measured 2.19 ms
+// alone but 798-803 Mrays/s end to end against 776 at eight.
 #ifndef ST_TRACE_MIN_BLOCKS
 #define ST_TRACE_MIN_BLOCKS 8
+#endif
+#ifndef ST_TRACE_DEVICE_MIN_BLOCKS
+#define ST_TRACE_DEVICE_MIN_BLOCKS 9
 #endif
 #ifndef ST_TRACE_OVERLAP_MIN_BLOCKS
 #define ST_TRACE_OVERLAP_MIN_BLOCKS 6
@@ -1057,7 +1062,7 @@ void launch_trace(const SceneDev &S, const ViewDev &v, const int4 *ssb, const fl
     if (bx_first >= bw) return;
     if (!bx_count || bx_first + bx_count > bw) bx_count = bw - bx_first;
     const dim3 grid(bh, bx_count);
-    constexpr int A = ST_TRACE_MIN_BLOCKS, B = ST_TRACE_OVERLAP_MIN_BLOCKS;
+    constexpr int A = ST_TRACE_DEVICE_MIN_BLOCKS, B = ST_TRACE_OVERLAP_MIN_BLOCKS;
     if (count && overlapped)
         trace_kernel<true, B><<<grid, 128, 0, st>>>(S, v, ssb, dirs, out, prim_ids, status, counters, bx_first);
     else if (count)
