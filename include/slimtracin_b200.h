@@ -178,8 +178,9 @@ ST_API int st_validate_bvh(const BVHNode *nodes, uint32_t node_count, uint32_t i
  * frame_buffer->pixels is non-null, the resolved W x H BGRA pixels.  `scene` supplies the per-frame
  * values the reference passes by value to its kernel (counts, ambient light); the arrays come from
  * the device copy.  viewport->trace.depth is the bounce count.  Page-locked host buffers (pinned
- * or registered) are written by the kernels while the frame is traced; pageable ones receive a
- * copy once it is done.  viewport->settings.show_BVH / show_SSB draw the drawBVH / drawSSB overlays
+ * or registered) are filled while the frame is traced: it is traced in column strips, and each
+ * strip's float_pixels are copied and its pixels resolved into them as soon as the strip is done;
+ * pageable ones receive a copy once the whole frame is done.  viewport->settings.show_BVH / show_SSB draw the drawBVH / drawSSB overlays
  * into the frame before the resolve (a host that binds renderScene here drops its own drawBVH and
  * drawSSB calls). */
 ST_API int st_render_scene(st_ctx *ctx, int slot, const Scene *scene, Viewport *viewport);
