@@ -436,7 +436,7 @@ void st_shutdown(st_ctx *ctx) {
     for (cudaStream_t t : ctx->strip_trace) if (t) cudaStreamDestroy(t);
     lbvh_release(ctx->lbvh);
     for (DevBuf *b : {&ctx->batch.table, &ctx->batch.ssb, &ctx->batch.seg, &ctx->batch.out_float, &ctx->batch.out_u8,
-                      &ctx->batch.counter})
+                      &ctx->batch.counter, &ctx->batch.park})
         release(ctx, *b);
     if (ctx->batch.exec) cudaGraphExecDestroy(ctx->batch.exec);
     if (ctx->batch.graph) cudaGraphDestroy(ctx->batch.graph);

@@ -54,3 +54,24 @@ def test_compacted_batch_equals_per_frame_renders(renderer):
     assert opt.compaction_threshold_used in (0, 8, 16, 24)
     for a, b in zip(frames, singles):
         assert np.array_equal(a.float_pixels.view(np.uint8), b.float_pixels.view(np.uint8))
+
+
+def test_context_shutdown_returns_the_ray_queue():
+    """A compacting batch reserves the parked-ray queue (96 MB for a launch group of a million rays or
+    more); shutting the context down gives it back with everything else the context holds."""
+    import torch
+    c0, cam0 = scenes.implicit16_scene()
+    H.tlas_sah(c0)
+    warm = api.Renderer(device=0)          # the library's modules load once, outside the measurement
+    warm.close()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    r = api.Renderer(device=0)
+    r.upload(3, c0, tlas="host")
+    fr = scenes.Frame(1920, 1080, cam0, depth=3, mode=S.RM_BEAUTY)
+    opt = api.render_batch(r, [(3, c0, fr)], tile_shape=0, stack_placement=0, chunk=1,
+                           launch_mode=api.LAUNCH_PERSISTENT, compaction_threshold=32)
+    assert opt.compaction_threshold_used == 32
+    r.close()
+    torch.cuda.synchronize()
+    assert free0 - torch.cuda.mem_get_info()[0] < (16 << 20)
