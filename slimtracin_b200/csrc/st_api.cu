@@ -195,10 +195,10 @@ struct st_ctx {
     // back is an asynchronous copy rather than a staged one
     unsigned long long *readback = nullptr;
     // renders into host memory, traced in column strips: one stream per strip (so that the strips
-    // run as one grid does, and each strip's copy and resolve follow its own trace), and the events
-    // that order them (created on first use)
-    cudaStream_t strip_trace[kRenderStrips] = {};
-    cudaEvent_t strip_ev[2 * kRenderStrips + 1] = {};
+    // run as one grid does, and each strip's copy follows its own trace), a stream for the strips'
+    // resolves, and the events that order them (created on first use)
+    cudaStream_t strip_trace[kRenderStrips] = {}, strip_resolve = nullptr;
+    cudaEvent_t strip_ev[2 * kRenderStrips + 2] = {};
     LbvhScratch lbvh;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     std::string cuda_error;
@@ -434,6 +434,7 @@ void st_shutdown(st_ctx *ctx) {
     if (ctx->readback) cudaFreeHost(ctx->readback);
     for (cudaEvent_t e : ctx->strip_ev) if (e) cudaEventDestroy(e);
     for (cudaStream_t t : ctx->strip_trace) if (t) cudaStreamDestroy(t);
+    if (ctx->strip_resolve) cudaStreamDestroy(ctx->strip_resolve);
     lbvh_release(ctx->lbvh);
     for (DevBuf *b : {&ctx->batch.table, &ctx->batch.ssb, &ctx->batch.seg, &ctx->batch.out_float, &ctx->batch.out_u8,
                       &ctx->batch.counter, &ctx->batch.park})
@@ -1069,6 +1070,9 @@ static cudaError_t ensure_strips(st_ctx *ctx) {
         const int prio = greatest + (int)((long)(least - greatest) * k / (kRenderStrips - 1));
         if (!ctx->strip_trace[k]) e = cudaStreamCreateWithPriority(&ctx->strip_trace[k], cudaStreamNonBlocking, prio);
     }
+    // the resolves go ahead of the trace blocks still waiting to start
+    if (e == cudaSuccess && !ctx->strip_resolve)
+        e = cudaStreamCreateWithPriority(&ctx->strip_resolve, cudaStreamNonBlocking, greatest);
     for (cudaEvent_t &ev : ctx->strip_ev)
         if (e == cudaSuccess && !ev) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
     return e;
@@ -1125,9 +1129,9 @@ int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *view
     launch_ray_rows(v, P<float>(ctx->dirs), st);
     // Host outputs.  A page-locked frame (pinned or registered) is written by the resolve kernel
     // itself; a page-locked float grid is traced in column strips, one stream per strip, and each
-    // strip's columns are copied to the host by a 2-D DMA copy, and its pixels resolved, on its own
-    // stream as soon as it is traced, so that only the last strip's copy and resolve follow the
-    // trace.  Pageable buffers receive one copy at the end.
+    // strip's columns are copied to the host by a 2-D DMA copy on its own stream, and its pixels
+    // resolved on the resolve stream, as soon as it is traced, so that only the last strip's copy
+    // and resolve follow the trace.  Pageable buffers receive one copy at the end.
     const bool host_out = !o->device_outputs;
     const bool want_float = host_out && host_float && !o->skip_float_copy;
     uint32_t *mapped_u8 = host_out && host_u8 && dev_u8 ? static_cast<uint32_t *>(device_view_of_host(host_u8)) : nullptr;
@@ -1141,7 +1145,7 @@ int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *view
     if (strips > 1) {
         ST_CUDA(ensure_strips(ctx));
         cudaEvent_t *done = ctx->strip_ev, *joined = ctx->strip_ev + kRenderStrips;   // per strip
-        cudaEvent_t fork = ctx->strip_ev[2 * kRenderStrips];
+        cudaEvent_t fork = ctx->strip_ev[2 * kRenderStrips], resolved_ev = ctx->strip_ev[2 * kRenderStrips + 1];
         ST_CUDA(cudaEventRecord(fork, st));
         const size_t pitch = sizeof(FloatPixel) * v.grid_w;
         auto strip_cols = [&](int k, u32t &gx0, u32t &gx1) {
@@ -1162,8 +1166,9 @@ int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *view
             ST_CUDA(cudaEventRecord(done[k], ts));
         }
         // each strip's columns are copied behind its own trace, whatever order the strips end in;
-        // pixel x reads grid columns x and x + 1, so a strip's pixels [gx0 - 1, gx1 - 1) are resolved
-        // once its left neighbour is traced too
+        // the resolve stream takes the strips in order: pixel x reads grid columns x and x + 1, so a
+        // strip's pixels [gx0 - 1, gx1 - 1) are resolved once it and the strips left of it are
+        // traced, on their own stream so that the last strip's resolve overlaps its copy
         for (int k = 0; k < strips; k++) {
             u32t gx0, gx1;
             strip_cols(k, gx0, gx1);
@@ -1171,15 +1176,20 @@ int st_render_ex(st_ctx *ctx, int slot, const Scene *scene, const Viewport *view
             if (want_float)
                 ST_CUDA(cudaMemcpy2DAsync(host_float + gx0, pitch, dev_float + gx0, pitch, sizeof(FloatPixel) * (gx1 - gx0),
                                           v.grid_h, cudaMemcpyDeviceToHost, ts));
-            if (u8_target) {
-                if (k > 0) ST_CUDA(cudaStreamWaitEvent(ts, done[k - 1], 0));
-                launch_resolve(dev_float, v.grid_w, W, H, u8_target, ts, k > 0 ? gx0 - 1 : 0, k + 1 == strips ? W : gx1 - 1);
-            }
             ST_CUDA(cudaEventRecord(joined[k], ts));
+            if (u8_target) {
+                ST_CUDA(cudaStreamWaitEvent(ctx->strip_resolve, done[k], 0));
+                launch_resolve(dev_float, v.grid_w, W, H, u8_target, ctx->strip_resolve, k > 0 ? gx0 - 1 : 0,
+                               k + 1 == strips ? W : gx1 - 1);
+            }
         }
         for (int k = 0; k < strips; k++) ST_CUDA(cudaStreamWaitEvent(st, done[k], 0));
         ST_CUDA(cudaEventRecord(ctx->ev[2], st));
         for (int k = 0; k < strips; k++) ST_CUDA(cudaStreamWaitEvent(st, joined[k], 0));
+        if (u8_target) {
+            ST_CUDA(cudaEventRecord(resolved_ev, ctx->strip_resolve));
+            ST_CUDA(cudaStreamWaitEvent(st, resolved_ev, 0));
+        }
     } else {
         launch_trace(sd, v, P<int4>(ctx->ssb), P<float>(ctx->dirs), dev_float, dev_ids, P<unsigned>(ctx->status),
                      P<unsigned long long>(ctx->counters), o->count_work != 0, st);
