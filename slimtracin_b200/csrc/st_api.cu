@@ -190,6 +190,11 @@ struct st_ctx {
     DevBuf sah_scratch;                  // binned-SAH builds (kept between builds)
     DevBuf overlay_scratch, overlay_frags;   // debug overlays: boxes/edges, and the plotted pixels
     char *upd_pinned = nullptr;          // ... and their pinned staging
+    char *bvh_pinned = nullptr;          // a TLAS build's counts, nodes and leaf order, read back at once
+    size_t bvh_pinned_cap = 0;
+    // an LBVH30 TLAS build as a graph, replayed while its operands are those of `lbvh_key`
+    cudaGraphExec_t lbvh_exec = nullptr;
+    const void *lbvh_key[9] = {};
     size_t upd_pinned_cap = 0;
     // page-locked landing place of a render's status words and work counters, so that reading them
     // back is an asynchronous copy rather than a staged one
@@ -431,6 +436,8 @@ void st_shutdown(st_ctx *ctx) {
                       &ctx->upd_host_dev, &ctx->sah_scratch, &ctx->overlay_scratch, &ctx->overlay_frags})
         release(ctx, *b);
     if (ctx->upd_pinned) cudaFreeHost(ctx->upd_pinned);
+    if (ctx->bvh_pinned) cudaFreeHost(ctx->bvh_pinned);
+    if (ctx->lbvh_exec) cudaGraphExecDestroy(ctx->lbvh_exec);
     if (ctx->readback) cudaFreeHost(ctx->readback);
     for (cudaEvent_t e : ctx->strip_ev) if (e) cudaEventDestroy(e);
     for (cudaStream_t t : ctx->strip_trace) if (t) cudaStreamDestroy(t);
@@ -765,18 +772,97 @@ int st_update_scene_bvh(st_ctx *ctx, int slot, Scene *scene, int mode) {
     return status;
 }
 
+// An LBVH30 TLAS update waits once: the build's counts, its nodes (at most 2n - 1) and its leaf order
+// come back together into page-locked staging, are checked there and, when the host scene has BVH
+// arrays, copied into them from there (the other modes wait for the build, the check and the copy
+// one after another).  The build's thirty-odd launches and the copies back run as one CUDA graph,
+// captured once and replayed while the scene's arrays, the count and the scratch stay the same, as
+// they do for a scene that moves every frame.
+static int update_scene_lbvh(st_ctx *ctx, SceneSlot *S, Scene *scene) {
+    const u32t n = S->n_prims;
+    cudaStream_t st = ctx->stream;
+    if (lbvh_reserve(ctx->lbvh, n) != cudaSuccess) return ST_ERR_OUT_OF_MEMORY;
+    const size_t node_bytes = sizeof(BVHNode) * 2 * (size_t)n, need = 64 + node_bytes + sizeof(u32t) * (size_t)n;
+    if (need > ctx->bvh_pinned_cap) {
+        if (ctx->bvh_pinned) cudaFreeHost(ctx->bvh_pinned);
+        ctx->bvh_pinned = nullptr;
+        ctx->bvh_pinned_cap = 0;
+        ST_CUDA(cudaHostAlloc((void **)&ctx->bvh_pinned, need, cudaHostAllocDefault));
+        ctx->bvh_pinned_cap = need;
+    }
+    u32t *counts = reinterpret_cast<u32t *>(ctx->bvh_pinned);
+    BVHNode *nodes = reinterpret_cast<BVHNode *>(ctx->bvh_pinned + 64);
+    u32t *ids = reinterpret_cast<u32t *>(ctx->bvh_pinned + 64 + node_bytes);
+    auto enqueue = [&]() {
+        launch_prim_aabbs(P<Primitive>(S->prims_raw), P<MeshDev>(S->meshes), n, ctx->lbvh.aabbs, st);
+        lbvh_enqueue(ctx->lbvh, n, MAX_OBJS_PER_SCENE_BVH_NODE, P<BVHNode>(S->tlas_nodes), P<u32t>(S->tlas_leaf_ids),
+                     counts, st);
+        cudaMemcpyAsync(nodes, S->tlas_nodes.ptr, node_bytes - sizeof(BVHNode), cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(ids, S->tlas_leaf_ids.ptr, sizeof(u32t) * n, cudaMemcpyDeviceToHost, st);
+    };
+    // the graph: captured and instantiated anew when the key changes (updated in place across a
+    // change of count, it reported success and then failed to launch), else replayed; any failure
+    // drops it and the build is launched directly (a failed graph launch enqueues nothing)
+    bool graphed = false;
+    if (n > MAX_OBJS_PER_SCENE_BVH_NODE) {         // (a one-leaf build writes its counts on the host)
+        const void *key[9] = {(const void *)(uintptr_t)n, (const void *)(uintptr_t)ctx->lbvh.capacity,
+                              ctx->lbvh.aabbs, ctx->lbvh.codes, S->prims_raw.ptr, S->meshes.ptr, S->tlas_nodes.ptr,
+                              S->tlas_leaf_ids.ptr, ctx->bvh_pinned};
+        cudaError_t e = cudaSuccess;
+        if (!ctx->lbvh_exec || memcmp(key, ctx->lbvh_key, sizeof(key)) != 0) {
+            cudaGraph_t g = nullptr;
+            e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                enqueue();
+                e = cudaStreamEndCapture(st, &g);
+            }
+            if (ctx->lbvh_exec) cudaGraphExecDestroy(ctx->lbvh_exec);
+            ctx->lbvh_exec = nullptr;
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&ctx->lbvh_exec, g, 0);
+            if (e != cudaSuccess) ctx->lbvh_exec = nullptr;
+            if (g) cudaGraphDestroy(g);
+            if (e == cudaSuccess) memcpy(ctx->lbvh_key, key, sizeof(key));
+        }
+        if (e == cudaSuccess) e = cudaGraphLaunch(ctx->lbvh_exec, st);
+        graphed = e == cudaSuccess;
+        if (!graphed) {
+            cudaGetLastError();
+            if (ctx->lbvh_exec) cudaGraphExecDestroy(ctx->lbvh_exec);
+            ctx->lbvh_exec = nullptr;
+        }
+    }
+    if (!graphed) {
+        enqueue();
+        ST_CUDA(cudaGetLastError());
+    }
+    ST_TRY(ST_CUDA_SYNC(ctx));
+    const u32t count = 1 + 2 * counts[2], height = counts[1];
+    // the walk trusts every index it reads: check the new arrays before first use
+    if (count > 2 * n - 1 || height + 2 > (u32t)kStack) return ST_ERR_BAD_SCENE;
+    if (!check_bvh(nodes, count, n, height)) return ST_ERR_BAD_SCENE;
+    for (u32t i = 0; i < n; i++) if (ids[i] >= n) return ST_ERR_BAD_SCENE;
+    S->tlas_node_count = count;
+    S->tlas_height = height;
+    if (count > 1) {
+        launch_make_pairs(P<BVHNode>(S->tlas_nodes), count, P<NodePair>(S->tlas_pairs), st);
+        ST_CUDA(cudaGetLastError());
+    }
+    S->tlas_root = nodes[0];
+    S->tlas_valid = true;
+    S->moved_since_build = 0;
+    if (scene && scene->bvh.nodes && scene->bvh.leaf_ids) {
+        memcpy(scene->bvh.nodes, nodes, sizeof(BVHNode) * count);
+        memcpy(scene->bvh.leaf_ids, ids, sizeof(u32t) * n);
+        scene->bvh.node_count = count;
+        scene->bvh.height = height;
+    }
+    return ST_OK;
+}
+
 static int update_scene_bvh(st_ctx *ctx, SceneSlot *S, Scene *scene, int mode) {
     const u32t n = S->n_prims;
     if (mode == ST_BVH_LBVH30) {
-        if (lbvh_reserve(ctx->lbvh, n) != cudaSuccess) return ST_ERR_OUT_OF_MEMORY;
-        launch_prim_aabbs(P<Primitive>(S->prims_raw), P<MeshDev>(S->meshes), n, ctx->lbvh.aabbs, ctx->stream);
-        u32t info[2];
-        cudaError_t e = lbvh_build(ctx->lbvh, n, MAX_OBJS_PER_SCENE_BVH_NODE, P<BVHNode>(S->tlas_nodes),
-                                   P<u32t>(S->tlas_leaf_ids), info, ctx->stream);
-        if (e != cudaSuccess) return fail_cuda(ctx, e);
-        S->tlas_node_count = info[0];
-        S->tlas_height = info[1];
-        if (S->tlas_height + 2 > (u32t)kStack) return ST_ERR_BAD_SCENE;
+        return update_scene_lbvh(ctx, S, scene);
     } else if (mode == ST_BVH_BINNED_SAH) {
         if (lbvh_reserve(ctx->lbvh, n) != cudaSuccess) return ST_ERR_OUT_OF_MEMORY;
         launch_prim_aabbs(P<Primitive>(S->prims_raw), P<MeshDev>(S->meshes), n, ctx->lbvh.aabbs, ctx->stream);

@@ -449,6 +449,16 @@ void lbvh_release(LbvhScratch &s) {
 cudaError_t lbvh_build(LbvhScratch &s, u32t n, u32t max_leaf, BVHNode *out_nodes, u32t *out_order, u32t info[2],
                        cudaStream_t st) {
     if (n == 0) { info[0] = 0; info[1] = 0; return cudaSuccess; }
+    u32t h[3];
+    lbvh_enqueue(s, n, max_leaf, out_nodes, out_order, h, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    info[0] = 1 + 2 * h[2];
+    info[1] = h[1];
+    return e;
+}
+
+void lbvh_enqueue(LbvhScratch &s, u32t n, u32t max_leaf, BVHNode *out_nodes, u32t *out_order, u32t *counts,
+                  cudaStream_t st) {
     const u32t T = 256;
     bounds_init_kernel<<<1, 32, 0, st>>>(s.bounds);
     bounds_kernel<<<min((n + T - 1) / T, 1184u), T, 0, st>>>(s.aabbs, n, s.bounds);
@@ -468,9 +478,10 @@ cudaError_t lbvh_build(LbvhScratch &s, u32t n, u32t max_leaf, BVHNode *out_nodes
     if (n <= max_leaf) {
         single_leaf_kernel<<<1, 1, 0, st>>>(s.aabbs, s.order, n, out_nodes);
         cudaMemcpyAsync(out_order, s.order, sizeof(u32t) * n, cudaMemcpyDeviceToDevice, st);
-        info[0] = 1;
-        info[1] = 1;
-        return cudaStreamSynchronize(st);
+        counts[0] = 0;                     // one node (1 + 2 * 0 kept internal nodes), height 1
+        counts[1] = 1;
+        counts[2] = 0;
+        return;
     }
     const u32t ni = n - 1;
     karras_kernel<<<(ni + T - 1) / T, T, 0, st>>>(s.codes, s.order, n, s.first, s.last, s.lchild, s.rchild, s.parent,
@@ -485,12 +496,7 @@ cudaError_t lbvh_build(LbvhScratch &s, u32t n, u32t max_leaf, BVHNode *out_nodes
     layout_kernel<<<(ni + T - 1) / T, T, 0, st>>>(s.aabbs, s.order, ni, s.first, s.last, s.lchild, s.rchild, s.parent,
                                                   s.flags, s.rank, s.kbox, out_nodes, s.info + 1);
     cudaMemcpyAsync(out_order, s.order, sizeof(u32t) * n, cudaMemcpyDeviceToDevice, st);
-    u32t h[3];
-    cudaMemcpyAsync(h, s.info, sizeof(u32t) * 3, cudaMemcpyDeviceToHost, st);
-    cudaError_t e = cudaStreamSynchronize(st);
-    info[0] = 1 + 2 * h[2];
-    info[1] = h[1];
-    return e;
+    cudaMemcpyAsync(counts, s.info, sizeof(u32t) * 3, cudaMemcpyDeviceToHost, st);
 }
 
 // ---- refit of a reference-layout BVH ------------------------------------------------------------

@@ -160,6 +160,10 @@ void lbvh_carve(LbvhScratch &s, void *base, u32t cap);
 // out_nodes must hold 2n nodes; out_order n ids.  info (host) receives node_count, height.
 cudaError_t lbvh_build(LbvhScratch &s, u32t n, u32t max_leaf, BVHNode *out_nodes, u32t *out_order,
                        u32t info[2], cudaStream_t st);
+// The same build (n > 0) without waiting: counts[3] (page-locked host memory, filled once `st`
+// reaches it) receive the words from which node_count = 1 + 2 * counts[2] and height = counts[1].
+void lbvh_enqueue(LbvhScratch &s, u32t n, u32t max_leaf, BVHNode *out_nodes, u32t *out_order, u32t *counts,
+                  cudaStream_t st);
 // Binned SAH over n device boxes (st_sah.cu): reference-layout nodes (2n capacity) + leaf order.
 // scratch (optional, sah_scratch_bytes(n) bytes): used instead of a stream-ordered allocation
 cudaError_t sah_build(const float *aabbs, u32t n, u32t max_leaf, BVHNode *out_nodes, u32t *out_order, u32t info[2],
