@@ -344,6 +344,29 @@ def test_pinned_outputs_traced_in_strips(renderer, w, h):
         assert np.array_equal(pu.numpy(), pageable.pixels.view(np.uint8)), with_float
 
 
+def test_strip_traced_render_counts_the_same_work(renderer):
+    """A render into page-locked buffers traces the frame in column strips (eight at 1920 wide), each
+    strip a launch of its own: the work counters summed over the strips equal those of the same view
+    traced in one launch (pageable buffers), which the oracle pins, and the frames are identical."""
+    import torch
+    c1, cam1 = H.small_mesh_scene(subdivisions=3, texture_size=64, blas="orc")
+    H.tlas_sah(c1)
+    renderer.upload(15, c1, tlas="host")
+    w, h = 1920, 1080
+    one = H.gpu_frame(renderer, 15, c1, cam1, w, h, depth=4, counters=True)
+    strips = scenes.Frame(w, h, cam1, depth=4, with_pixels=False, with_float=False)
+    pf = torch.zeros(strips.rays * 24, dtype=torch.uint8, pin_memory=True)
+    pu = torch.zeros(w * h * 4, dtype=torch.uint8, pin_memory=True)
+    strips.grid.float_pixels = pf.data_ptr()
+    strips.grid.pixels = pu.data_ptr()
+    opt = renderer.render(15, c1, strips, count_work=True)
+    counted = np.array([opt.counters[k] for k in range(16)], dtype=np.uint64)
+    assert np.array_equal(counted, one.counters)
+    assert counted[0] == strips.rays                     # every grid point traced once
+    assert np.array_equal(pf.numpy(), one.float_pixels.view(np.uint8))
+    assert np.array_equal(pu.numpy(), one.pixels.view(np.uint8))
+
+
 @pytest.mark.parametrize("which", ["implicit16", "mesh"])
 def test_pick_equals_oracle(renderer, which):
     """st_pick (manipulateSelection's picking ray on the device) equals the oracle's pick bit for bit
