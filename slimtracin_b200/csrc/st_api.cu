@@ -192,9 +192,6 @@ struct st_ctx {
     char *upd_pinned = nullptr;          // ... and their pinned staging
     char *bvh_pinned = nullptr;          // a TLAS build's counts, nodes and leaf order, read back at once
     size_t bvh_pinned_cap = 0;
-    // an LBVH30 TLAS build as a graph, replayed while its operands are those of `lbvh_key`
-    cudaGraphExec_t lbvh_exec = nullptr;
-    const void *lbvh_key[9] = {};
     size_t upd_pinned_cap = 0;
     // page-locked landing place of a render's status words and work counters, so that reading them
     // back is an asynchronous copy rather than a staged one
@@ -437,7 +434,6 @@ void st_shutdown(st_ctx *ctx) {
         release(ctx, *b);
     if (ctx->upd_pinned) cudaFreeHost(ctx->upd_pinned);
     if (ctx->bvh_pinned) cudaFreeHost(ctx->bvh_pinned);
-    if (ctx->lbvh_exec) cudaGraphExecDestroy(ctx->lbvh_exec);
     if (ctx->readback) cudaFreeHost(ctx->readback);
     for (cudaEvent_t e : ctx->strip_ev) if (e) cudaEventDestroy(e);
     for (cudaStream_t t : ctx->strip_trace) if (t) cudaStreamDestroy(t);
@@ -775,9 +771,7 @@ int st_update_scene_bvh(st_ctx *ctx, int slot, Scene *scene, int mode) {
 // An LBVH30 TLAS update waits once: the build's counts, its nodes (at most 2n - 1) and its leaf order
 // come back together into page-locked staging, are checked there and, when the host scene has BVH
 // arrays, copied into them from there (the other modes wait for the build, the check and the copy
-// one after another).  The build's thirty-odd launches and the copies back run as one CUDA graph,
-// captured once and replayed while the scene's arrays, the count and the scratch stay the same, as
-// they do for a scene that moves every frame.
+// one after another).
 static int update_scene_lbvh(st_ctx *ctx, SceneSlot *S, Scene *scene) {
     const u32t n = S->n_prims;
     cudaStream_t st = ctx->stream;
@@ -793,48 +787,12 @@ static int update_scene_lbvh(st_ctx *ctx, SceneSlot *S, Scene *scene) {
     u32t *counts = reinterpret_cast<u32t *>(ctx->bvh_pinned);
     BVHNode *nodes = reinterpret_cast<BVHNode *>(ctx->bvh_pinned + 64);
     u32t *ids = reinterpret_cast<u32t *>(ctx->bvh_pinned + 64 + node_bytes);
-    auto enqueue = [&]() {
-        launch_prim_aabbs(P<Primitive>(S->prims_raw), P<MeshDev>(S->meshes), n, ctx->lbvh.aabbs, st);
-        lbvh_enqueue(ctx->lbvh, n, MAX_OBJS_PER_SCENE_BVH_NODE, P<BVHNode>(S->tlas_nodes), P<u32t>(S->tlas_leaf_ids),
-                     counts, st);
-        cudaMemcpyAsync(nodes, S->tlas_nodes.ptr, node_bytes - sizeof(BVHNode), cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(ids, S->tlas_leaf_ids.ptr, sizeof(u32t) * n, cudaMemcpyDeviceToHost, st);
-    };
-    // the graph: captured and instantiated anew when the key changes (updated in place across a
-    // change of count, it reported success and then failed to launch), else replayed; any failure
-    // drops it and the build is launched directly (a failed graph launch enqueues nothing)
-    bool graphed = false;
-    if (n > MAX_OBJS_PER_SCENE_BVH_NODE) {         // (a one-leaf build writes its counts on the host)
-        const void *key[9] = {(const void *)(uintptr_t)n, (const void *)(uintptr_t)ctx->lbvh.capacity,
-                              ctx->lbvh.aabbs, ctx->lbvh.codes, S->prims_raw.ptr, S->meshes.ptr, S->tlas_nodes.ptr,
-                              S->tlas_leaf_ids.ptr, ctx->bvh_pinned};
-        cudaError_t e = cudaSuccess;
-        if (!ctx->lbvh_exec || memcmp(key, ctx->lbvh_key, sizeof(key)) != 0) {
-            cudaGraph_t g = nullptr;
-            e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
-            if (e == cudaSuccess) {
-                enqueue();
-                e = cudaStreamEndCapture(st, &g);
-            }
-            if (ctx->lbvh_exec) cudaGraphExecDestroy(ctx->lbvh_exec);
-            ctx->lbvh_exec = nullptr;
-            if (e == cudaSuccess) e = cudaGraphInstantiate(&ctx->lbvh_exec, g, 0);
-            if (e != cudaSuccess) ctx->lbvh_exec = nullptr;
-            if (g) cudaGraphDestroy(g);
-            if (e == cudaSuccess) memcpy(ctx->lbvh_key, key, sizeof(key));
-        }
-        if (e == cudaSuccess) e = cudaGraphLaunch(ctx->lbvh_exec, st);
-        graphed = e == cudaSuccess;
-        if (!graphed) {
-            cudaGetLastError();
-            if (ctx->lbvh_exec) cudaGraphExecDestroy(ctx->lbvh_exec);
-            ctx->lbvh_exec = nullptr;
-        }
-    }
-    if (!graphed) {
-        enqueue();
-        ST_CUDA(cudaGetLastError());
-    }
+    launch_prim_aabbs(P<Primitive>(S->prims_raw), P<MeshDev>(S->meshes), n, ctx->lbvh.aabbs, st);
+    lbvh_enqueue(ctx->lbvh, n, MAX_OBJS_PER_SCENE_BVH_NODE, P<BVHNode>(S->tlas_nodes), P<u32t>(S->tlas_leaf_ids),
+                 counts, st);
+    ST_CUDA(cudaGetLastError());
+    ST_CUDA(cudaMemcpyAsync(nodes, S->tlas_nodes.ptr, node_bytes - sizeof(BVHNode), cudaMemcpyDeviceToHost, st));
+    ST_CUDA(cudaMemcpyAsync(ids, S->tlas_leaf_ids.ptr, sizeof(u32t) * n, cudaMemcpyDeviceToHost, st));
     ST_TRY(ST_CUDA_SYNC(ctx));
     const u32t count = 1 + 2 * counts[2], height = counts[1];
     // the walk trusts every index it reads: check the new arrays before first use
