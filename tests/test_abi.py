@@ -182,6 +182,12 @@ def test_validate_bvh(L):
     assert L.st_validate_bvh(deep.ctypes.data, len(deep), n_items, 3) == ok
     deeper, n_items = _chain(63)
     assert L.st_validate_bvh(deeper.ctypes.data, len(deeper), n_items, 3) == bad
+    # words that are no tree at all (a node array read back before anything wrote it): refused
+    rng = np.random.default_rng(7)
+    for _ in range(4):
+        junk = np.frombuffer(rng.integers(0, 2**32, size=len(nodes) * 8, dtype=np.uint32).tobytes(),
+                             dtype=S.BVHNODE_DT).copy()
+        assert L.st_validate_bvh(junk.ctypes.data, len(junk), items, 5) == bad
     # a root leaf
     leaf = np.zeros(1, dtype=S.BVHNODE_DT)
     leaf[0]["child_count"] = 2
